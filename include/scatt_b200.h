@@ -1,0 +1,182 @@
+/* scatt_b200.h -- C ABI of the B200 static-exchange scattering library.
+ *
+ * Drop-in boundary for the per-energy hot path of static-exchangeHF
+ * (SchurInverter -> ForwardRPropagator -> KMatrixExtractor ->
+ *  BackPropagator -> AsymptoticAmplitudes -> DipoleMatrixElement).
+ *
+ * Conventions
+ *   - every function returns an int status (SCATT_OK = 0); the message of
+ *     the last failure on the calling thread is scatt_last_error();
+ *   - no exceptions cross this boundary; no C++ or torch types appear in it;
+ *   - matrices are FP64, column-major, with explicit leading dimensions
+ *     (Eigen's default layout, as in src/scatt/GpuPropagate.hpp:188-193);
+ *   - all host arrays are caller-owned; the library owns device memory;
+ *   - there is no CPU fallback: without a CUDA device every compute entry
+ *     point returns SCATT_ERR_NO_DEVICE.
+ */
+#ifndef SCATT_B200_H
+#define SCATT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SCATT_OK                 0
+#define SCATT_ERR_ARG            1   /* bad argument / shape                        */
+#define SCATT_ERR_CUDA           2   /* CUDA runtime error                          */
+#define SCATT_ERR_SIZE           3   /* size beyond a kernel limit                  */
+#define SCATT_ERR_SINGULAR       4   /* zero pivot (LapackInverse.hpp:73-86 throws)  */
+#define SCATT_ERR_NONFINITE      5   /* NaN / Inf pivot                             */
+#define SCATT_ERR_CLOSED_CHANNEL 6   /* AsymptoticAmplitudes.cpp:177-186 abort      */
+#define SCATT_ERR_NO_DEVICE      7   /* no CUDA device visible                      */
+#define SCATT_ERR_STATE          8   /* call order (e.g. solve before upload)       */
+#define SCATT_ERR_OOM            9   /* device allocation failed                    */
+#define SCATT_ERR_FIT_WINDOW    10   /* AsymptoticAmplitudes.cpp:85-91 abort        */
+
+/* ------------------------------------------------------------------ misc */
+const char* scatt_version(void);
+const char* scatt_last_error(void);
+/* Number of visible CUDA devices (0 without a GPU; never fails on a CPU host). */
+int scatt_device_count(int* count);
+
+/* ------------------------------------------------------- angular algebra
+ * Host-side precompute shared with the device tables.
+ * Replace src/angular/Gaunt.hpp:65-135 (gaunt_real over GSL 3j) and
+ * src/scatt/DipoleMatrixElement.cpp:80-95 (angular_dipole, velocity_coef). */
+double scatt_wigner3j(int j1, int j2, int j3, int m1, int m2, int m3);
+double scatt_gaunt_real(int l1, int m1, int l2, int m2, int l3, int m3);
+double scatt_angular_dipole(int l_mu, int m_mu, int q, int l_nu, int m_nu);
+double scatt_velocity_coef(int l_mu, int l_nu);
+/* Riccati-Bessel x j_l(x) and Riccati-Neumann x y_l(x) (the same routine the
+ * kernels use).  Replace the GSL calls of ForwardRPropagator.cpp:64-75,
+ * KMatrixExtractor.cpp:50-73, AsymptoticAmplitudes.cpp:39-62. */
+double scatt_riccati_j(int l, double x);
+double scatt_riccati_y(int l, double x);
+
+/* ------------------------------------------------ dense device building blocks
+ * Batched inverse of `count` n x n matrices (contiguous, ld = n) with partial
+ * pivoting; symmetrize != 0 returns 0.5 (X + X^T).  status (may be NULL)
+ * receives 2 ints per matrix: device status code, first failing column.
+ * Replaces inverse_general / inverse_symmetric_indefinite
+ * (src/scatt/LapackInverse.hpp:53-178). */
+int scatt_inverse_batched(int n, int count, const double* A, double* out,
+                          int symmetrize, int* status);
+
+/* C = alpha op(A) op(B) + beta C on the device, host buffers (op: 0 = N, 1 = T). */
+int scatt_dgemm(int opA, int opB, int M, int N, int K, double alpha,
+                const double* A, int lda, const double* B, int ldb,
+                double beta, double* C, int ldc);
+
+/* Device-resident timing of scatt_inverse_batched's kernels on seeded
+ * matrices (CUDA events around the kernels only); used by the tile autotuner
+ * and the benchmark. */
+int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call);
+
+/* ------------------------------------------------------ per-scan solver
+ * The reference runs one energy at a time through run_one_energy
+ * (src/main.cpp:1081-1623); here a batch of energies is solved together,
+ * lock-step over the radial grid, with every intermediate (Sinv, R^-1, the
+ * dipole sweeps) resident in HBM.  Stage order and policies follow the
+ * reference classes (SchurInverter, ForwardRPropagator, KMatrixExtractor,
+ * BackPropagator, AsymptoticAmplitudes, DipoleMatrixElement). */
+typedef struct scatt_ctx scatt_ctx;
+
+/* Energy-independent inputs of one scan: the content of the preprocessing
+ * file the reference reads (src/io/HDF5Reader.hpp:42-86). */
+typedef struct {
+    int    Nr;            /* radial points (SolverParams::n_grid)                        */
+    double dr;            /* step; the preprocessing grid is r = ir * dr                 */
+    int    l_cont_max;    /* largest continuum l of any energy in the scan               */
+    int    n_occ;         /* occupied orbitals in the exchange sum and orthogonalisation */
+    int    n_orb;         /* orbitals stored in psi_lm (>= n_occ)                        */
+    int    Nlm_store;     /* angular channels stored per orbital                         */
+    int    Nr_store;      /* radial points stored per orbital (<= Nr)                    */
+    const double* psi_lm; /* [n_orb][Nlm_store][Nr_store] C order: F_{i,lambda}(ir dr)    */
+    int    init_state;    /* orbital used as dipole initial state; -1 = n_occ - 1 (HOMO)  */
+    int    n_H;           /* rows of V_H supplied                                        */
+    const double* V_H;    /* [n_H][Nr] C order: Hartree multipoles V_H,sigma(ir dr)       */
+    int    n_atoms;
+    const double* atoms;  /* [n_atoms][4]: Z, x, y, z (bohr)                              */
+    double alpha_pol;     /* polarisability; 0 = no polarisation potential              */
+    int    pol_form;      /* 0: -a/2 (1-exp(-(r/r_c)^6))^2 / r^4 (Potentials.cpp:111-129)
+                             1: -a / (2 (r^2 + r_c^2)^2)                                  */
+    double r_c;           /* cutoff radius (the reference fixes 1.5 for form 0)           */
+    int    n_transition;  /* > 0: explicit; 0: chi_cutoff rule (WavefunctionSetup.cpp:278-324) */
+    double chi_cutoff;    /* 1e-15 in the reference                                       */
+} scatt_scan_desc;
+
+/* Policies (defaults in parentheses are the reference's). */
+typedef struct {
+    double W_min;                 /* (0.001) SchurInverter.hpp:74                     */
+    int    stab_n_max;            /* (60)    SchurInverter.hpp:75                     */
+    double shift_margin;          /* (0.01)  SchurInverter.hpp:76                     */
+    int    n_asym;                /* (300)   main.cpp:1335                            */
+    int    allow_closed_channels; /* (0)     AsymptoticAmplitudes.hpp:72-102          */
+    int    orthogonalize;         /* (1)     DipoleMatrixElement.hpp:104-148          */
+    int    max_batch;             /* energies per device batch; 0 = as many as fit    */
+    int    use_graphs;            /* 1: replay the radial step as a CUDA graph        */
+    int    diagnostics;           /* 1: S-matrix unitarity and eigenphases            */
+} scatt_solve_opts;
+
+/* Diagnostics per energy (index into scatt_outputs.diag). */
+#define SCATT_DIAG_FIT_RESIDUAL_MAX    0
+#define SCATT_DIAG_FIT_RESIDUAL_REL    1
+#define SCATT_DIAG_A_MINUS_I_MAX       2
+#define SCATT_DIAG_K_SYMMETRY_ERR_AA   3
+#define SCATT_DIAG_S_UNITARITY_ERR_AA  4
+#define SCATT_DIAG_K_SYMMETRY_ERR_KME  5
+#define SCATT_DIAG_UNITARITY_ERR_KME   6
+#define SCATT_DIAG_N_FIT_START         7
+#define SCATT_DIAG_N_FIT_END           8
+#define SCATT_DIAG_N_TRANSITION        9
+#define SCATT_DIAG_SHIFTS_A           10
+#define SCATT_DIAG_SHIFTS_S           11
+#define SCATT_DIAG_N_CLOSED_L         12
+#define SCATT_DIAG_SCHUR_COUPLING_0   13
+#define SCATT_NDIAG                   16
+
+/* Caller-owned host outputs; any pointer may be NULL.  Np = (l_cont_max+1)^2.
+ * For energy e, a matrix output starts at e * Np * Np and is column-major
+ * with ld = Np; an energy whose l_cont is smaller fills the leading block.
+ * Slot order of the six dipole slices is (L,x) (L,y) (L,z) (V,x) (V,y) (V,z)
+ * (DipoleWriter::slice_index). */
+typedef struct {
+    double* K_kme;       /* [E][Np*Np]  KMatrixExtractor::extract K                    */
+    double* A;           /* [E][Np*Np]  AsymptoticAmplitudes A                         */
+    double* B;           /* [E][Np*Np]  AsymptoticAmplitudes B                         */
+    double* K_aa;        /* [E][Np*Np]  B A^-1                                         */
+    double* b_overlap;   /* [E][Np*n_occ]  <phi_alpha | psi_beta>, Np x n_occ          */
+    double* D_re;        /* [E][6][Np]  D_reduced                                      */
+    double* D_im;
+    double* Draw_re;     /* [E][6][Np]  D_reduced_raw                                  */
+    double* Draw_im;
+    double* d_raw;       /* [E][6][Np]                                                 */
+    double* d_corr;      /* [E][6][n_occ]                                              */
+    double* partial_sigma; /* [E][6]                                                   */
+    double* eig_kme;     /* [E][Np]  eigenphases atan(eig K) (diagnostics = 1)         */
+    double* eig_aa;      /* [E][Np]                                                    */
+    double* diag;        /* [E][SCATT_NDIAG]                                           */
+    int*    status;      /* [E]      per-energy SCATT_* status                         */
+} scatt_outputs;
+
+int scatt_ctx_create(int device, scatt_ctx** out);
+int scatt_ctx_destroy(scatt_ctx* ctx);
+/* Builds every energy-independent table on the device (potential Gaunt
+ * pairs, exchange coupling CSR, chi, dipole rows, stability spectra). */
+int scatt_upload_static(scatt_ctx* ctx, const scatt_scan_desc* desc);
+/* n_transition and channel sizes of the uploaded scan: out[0] = n_transition,
+ * out[1] = Np_max, out[2] = N_f, out[3] = n_lambda, out[4] = n_sigma. */
+int scatt_scan_info(scatt_ctx* ctx, int* out5);
+/* Solves n_energy energies E_e = energies[e] (Hartree) with continuum cutoffs
+ * l_cont[e] (NULL: all l_cont_max).  Returns SCATT_OK or the first failing
+ * energy's status; outputs->status has every energy's status. */
+int scatt_solve_batch(scatt_ctx* ctx, int n_energy, const double* energies, const int* l_cont,
+                      const scatt_solve_opts* opts, const scatt_outputs* outputs);
+/* Default policies (the reference's). */
+void scatt_default_opts(scatt_solve_opts* opts);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCATT_B200_H */

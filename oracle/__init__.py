@@ -1,0 +1,26 @@
+"""CPU oracle for the static-exchange per-energy scattering path.
+
+TEST INFRASTRUCTURE ONLY.  This package is a plain numpy/scipy restatement
+of the reference C++ hot path (SchurInverter -> ForwardRPropagator ->
+KMatrixExtractor -> BackPropagator -> AsymptoticAmplitudes ->
+DipoleMatrixElement) used as the checker for the CUDA library.  Only the
+test suite, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import it.  The product path never calls into it and
+fails loudly when the CUDA extension is missing.
+
+Each function cites the reference file:line it restates (paths relative to
+the reference project root).  Dense linear algebra goes through the same
+LAPACK routines the reference's MKL build calls (dgetrf/dgetri for the
+general inverse, dsytrf/dsytri on the LOWER triangle for the Schur
+inverse), here via scipy's bundled OpenBLAS.
+
+Parity pinning: the angular algebra (3j / Gaunt / real-Y dipole table),
+Simpson quadrature and the free-particle dipole are pinned to the golden
+vectors of the reference's own unit tests (tests/golden/); the Riccati
+functions are pinned to mpmath.  The end-to-end K / A / B / dipole values
+cannot be pinned to the reference binary (it needs Eigen, HDF5 and GSL,
+none of which exist in this image), so the end-to-end restatement is
+"parity unpinned" against the reference binary and pinned only through
+the property tests (Schur gold standard, Numerov identity, symmetry,
+unitarity, gauge identity, compute_six == 6 x compute).
+"""

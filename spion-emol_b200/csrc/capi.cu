@@ -1,0 +1,190 @@
+// capi.cu -- extern "C" entry points: error handling, angular algebra,
+// device building blocks.  The per-energy-batch solver entry points live in
+// scan.cu, the per-step compatibility seam in steppers.cu.
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "angular.hpp"
+#include "common.cuh"
+#include "devbuf.cuh"
+#include "riccati.cuh"
+
+namespace scatt {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+int require_device() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        (void)cudaGetLastError();
+        set_last_error("no CUDA device visible (the library has no CPU fallback)");
+        return SCATT_ERR_NO_DEVICE;
+    }
+    return SCATT_OK;
+}
+
+__global__ void fill_test_matrices(double* A, int n, int count, unsigned seed) {
+    const size_t total = (size_t)n * n * count;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        unsigned h = (unsigned)(idx * 2654435761u) ^ seed;
+        h ^= h >> 13; h *= 0x5bd1e995u; h ^= h >> 15;
+        const size_t within = idx % ((size_t)n * n);
+        const int i = (int)(within % n), j = (int)(within / n);
+        A[idx] = (double)(h & 0xffffff) / 16777216.0 - 0.5 + (i == j ? 2.0 : 0.0);
+    }
+}
+
+}  // namespace scatt
+
+using namespace scatt;
+
+extern "C" {
+
+const char* scatt_version(void) { return "spion-emol_b200 0.1 (sm_100a, FP64 DMMA)"; }
+
+const char* scatt_last_error(void) { return g_last_error.c_str(); }
+
+int scatt_device_count(int* count) {
+    if (!count) return SCATT_ERR_ARG;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        (void)cudaGetLastError();
+        n = 0;
+    }
+    *count = n;
+    return SCATT_OK;
+}
+
+double scatt_wigner3j(int j1, int j2, int j3, int m1, int m2, int m3) {
+    return wigner3j(j1, j2, j3, m1, m2, m3);
+}
+double scatt_gaunt_real(int l1, int m1, int l2, int m2, int l3, int m3) {
+    return gaunt_real(l1, m1, l2, m2, l3, m3);
+}
+double scatt_angular_dipole(int l_mu, int m_mu, int q, int l_nu, int m_nu) {
+    return angular_dipole(l_mu, m_mu, q, l_nu, m_nu);
+}
+double scatt_velocity_coef(int l_mu, int l_nu) { return velocity_coef(l_mu, l_nu); }
+double scatt_riccati_j(int l, double x) { return scatt::riccati_j(l, x); }
+double scatt_riccati_y(int l, double x) { return scatt::riccati_y(l, x); }
+
+int scatt_inverse_batched(int n, int count, const double* A, double* out, int symmetrize,
+                          int* status) {
+    if (n <= 0 || count <= 0 || !A || !out) {
+        set_last_error("scatt_inverse_batched: bad arguments");
+        return SCATT_ERR_ARG;
+    }
+    SCATT_TRY(require_device());
+    const size_t nn = (size_t)n * n;
+    DevBuf<double> dA, dW, dO;
+    DevBuf<int> dsig, drid, dst;
+    SCATT_TRY(dA.alloc(nn * count));
+    SCATT_TRY(dW.alloc(nn * count));
+    SCATT_TRY(dO.alloc(nn * count));
+    SCATT_TRY(dsig.alloc((size_t)n * count));
+    SCATT_TRY(drid.alloc((size_t)n * count));
+    SCATT_TRY(dst.alloc(2 * (size_t)count));
+    SCATT_CUDA_TRY(cudaMemcpy(dA.p, A, nn * count * sizeof(double), cudaMemcpyHostToDevice));
+    SCATT_CUDA_TRY(cudaMemset(dst.p, 0, 2 * count * sizeof(int)));
+    std::vector<GjEntry> ent(count);
+    for (int b = 0; b < count; ++b) {
+        ent[b] = GjEntry{dA.p + nn * b, dW.p + nn * b, dO.p + nn * b, dsig.p + (size_t)n * b,
+                         drid.p + (size_t)n * b, dst.p + 2 * b, n, n, n};
+    }
+    DevBuf<GjEntry> dent;
+    SCATT_TRY(dent.upload(ent));
+    SCATT_TRY(gj_inverse_batched(dent.p, count, n, symmetrize != 0, 0));
+    SCATT_CUDA_TRY(cudaDeviceSynchronize());
+    SCATT_CUDA_TRY(cudaMemcpy(out, dO.p, nn * count * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<int> st(2 * count);
+    SCATT_CUDA_TRY(cudaMemcpy(st.data(), dst.p, st.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    if (status) std::memcpy(status, st.data(), st.size() * sizeof(int));
+    for (int b = 0; b < count; ++b) {
+        if (st[2 * b] == DEV_SINGULAR) {
+            set_last_error("scatt_inverse_batched: singular pivot in matrix " + std::to_string(b) +
+                           " at column " + std::to_string(st[2 * b + 1]));
+            return SCATT_ERR_SINGULAR;
+        }
+        if (st[2 * b] == DEV_NONFINITE) {
+            set_last_error("scatt_inverse_batched: non-finite pivot in matrix " + std::to_string(b) +
+                           " at column " + std::to_string(st[2 * b + 1]));
+            return SCATT_ERR_NONFINITE;
+        }
+    }
+    return SCATT_OK;
+}
+
+int scatt_dgemm(int opA, int opB, int M, int N, int K, double alpha, const double* A, int lda,
+                const double* B, int ldb, double beta, double* C, int ldc) {
+    if (M <= 0 || N <= 0 || K < 0 || !A || !B || !C) {
+        set_last_error("scatt_dgemm: bad arguments");
+        return SCATT_ERR_ARG;
+    }
+    SCATT_TRY(require_device());
+    const size_t sa = (size_t)lda * (opA ? M : K), sb = (size_t)ldb * (opB ? K : N);
+    const size_t sc = (size_t)ldc * N;
+    DevBuf<double> dA, dB, dC;
+    SCATT_TRY(dA.alloc(sa ? sa : 1));
+    SCATT_TRY(dB.alloc(sb ? sb : 1));
+    SCATT_TRY(dC.alloc(sc));
+    SCATT_CUDA_TRY(cudaMemcpy(dA.p, A, sa * sizeof(double), cudaMemcpyHostToDevice));
+    SCATT_CUDA_TRY(cudaMemcpy(dB.p, B, sb * sizeof(double), cudaMemcpyHostToDevice));
+    SCATT_CUDA_TRY(cudaMemcpy(dC.p, C, sc * sizeof(double), cudaMemcpyHostToDevice));
+    GemmEntry e{dA.p, dB.p, dC.p, M, N, K, lda, ldb, ldc, alpha, beta};
+    DevBuf<GemmEntry> de;
+    SCATT_TRY(de.upload(std::vector<GemmEntry>{e}));
+    SCATT_TRY(gemm_batched(de.p, 1, M, N, opA, opB, 0));
+    SCATT_CUDA_TRY(cudaDeviceSynchronize());
+    SCATT_CUDA_TRY(cudaMemcpy(C, dC.p, sc * sizeof(double), cudaMemcpyDeviceToHost));
+    return SCATT_OK;
+}
+
+
+int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call) {
+    if (n <= 0 || count <= 0 || reps <= 0 || !ms_per_call) return SCATT_ERR_ARG;
+    SCATT_TRY(require_device());
+    const size_t nn = (size_t)n * n;
+    DevBuf<double> dA, dW, dO, dS;
+    DevBuf<int> dsig, drid, dst;
+    SCATT_TRY(dA.alloc(nn * count));
+    SCATT_TRY(dS.alloc(nn * count));
+    SCATT_TRY(dW.alloc(nn * count));
+    SCATT_TRY(dO.alloc(nn * count));
+    SCATT_TRY(dsig.alloc((size_t)n * count));
+    SCATT_TRY(drid.alloc((size_t)n * count));
+    SCATT_TRY(dst.alloc(2 * (size_t)count));
+    fill_test_matrices<<<1024, 256>>>(dS.p, n, count, 12345u);
+    std::vector<GjEntry> ent(count);
+    for (int b = 0; b < count; ++b)
+        ent[b] = GjEntry{dA.p + nn * b, dW.p + nn * b, dO.p + nn * b, dsig.p + (size_t)n * b,
+                         drid.p + (size_t)n * b, dst.p + 2 * b, n, n, n};
+    DevBuf<GjEntry> dent;
+    SCATT_TRY(dent.upload(ent));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float total = 0.f;
+    for (int r = 0; r < reps + 1; ++r) {
+        SCATT_CUDA_TRY(cudaMemcpyAsync(dA.p, dS.p, nn * count * sizeof(double), cudaMemcpyDeviceToDevice));
+        cudaEventRecord(e0);
+        SCATT_TRY(gj_inverse_batched(dent.p, count, n, true, 0));
+        cudaEventRecord(e1);
+        SCATT_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (r > 0) total += ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms_per_call = total / reps;
+    return SCATT_OK;
+}
+
+}  // extern "C"

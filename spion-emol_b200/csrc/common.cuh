@@ -1,0 +1,92 @@
+// common.cuh -- shared definitions for the sm_100a scattering library.
+//
+// All matrices are FP64, column-major (element (i, j) at p[i + j * ld]),
+// matching the Eigen default layout the reference interfaces use.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "scatt_b200.h"
+
+namespace scatt {
+
+// Error bookkeeping: every host entry point returns an int status; the last
+// error message is kept per thread (see capi.cu).
+void set_last_error(const std::string& msg);
+
+#define SCATT_CUDA_TRY(expr)                                                    \
+    do {                                                                        \
+        cudaError_t _e = (expr);                                                \
+        if (_e != cudaSuccess) {                                                \
+            ::scatt::set_last_error(std::string(#expr) + ": " +                 \
+                                    cudaGetErrorString(_e));                    \
+            return SCATT_ERR_CUDA;                                              \
+        }                                                                       \
+    } while (0)
+
+inline int cuda_status(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+        return SCATT_ERR_CUDA;
+    }
+    return SCATT_OK;
+}
+#define SCATT_CUDA_TRY_RET(expr) ::scatt::cuda_status((expr), #expr)
+
+#define SCATT_TRY(expr)                                                         \
+    do {                                                                        \
+        int _s = (expr);                                                        \
+        if (_s != SCATT_OK) return _s;                                          \
+    } while (0)
+
+// Device-side status codes written into per-matrix status words.
+enum DeviceStatus : int {
+    DEV_OK = 0,
+    DEV_SINGULAR = 1,      // zero pivot encountered
+    DEV_NONFINITE = 2,     // NaN / Inf pivot
+};
+
+// ---------------------------------------------------------------- GEMM
+// One entry of a batched GEMM:  C = alpha * op(A) * op(B) + beta * C.
+// op(A) is M x K, op(B) is K x N.  Entries with M, N or K <= 0 are skipped
+// (K <= 0 with beta != 1 still scales C).
+struct GemmEntry {
+    const double* A;
+    const double* B;
+    double*       C;
+    int M, N, K;
+    int lda, ldb, ldc;
+    double alpha, beta;
+};
+
+// opA / opB: 0 = no transpose, 1 = transpose.  `entries` is a DEVICE array.
+int gemm_batched(const GemmEntry* entries_dev, int count, int maxM, int maxN,
+                 int opA, int opB, cudaStream_t stream);
+
+// ---------------------------------------------------------------- GJ inverse
+// Batched in-place Gauss-Jordan inversion with partial (row) pivoting,
+// blocked by GJ_NB columns.  Each matrix has its own order n (<= nmax).
+struct GjEntry {
+    double* A;        // input matrix (n x n, ld), destroyed
+    double* W;        // workspace of the same shape (ping-pong buffer)
+    double* out;      // output (n x n, ldo): inverse (optionally symmetrised)
+    int*    sigma;    // n ints: row map of the current block step
+    int*    rowid;    // n ints: original row index at each position
+    int*    status;   // 1 int: DeviceStatus (first failing column in status[1])
+    int n, ld, ldo;
+};
+
+constexpr int GJ_NB = 16;
+
+// Largest n the single-CTA panel factorisation holds in shared memory.
+int gj_max_order();
+
+// Runs the whole inversion (ceil(nmax / GJ_NB) block steps).  `entries_dev`
+// is a DEVICE array; `symmetrize` writes 0.5 * (X + X^T) into `out`.
+int gj_inverse_batched(const GjEntry* entries_dev, int count, int nmax,
+                       bool symmetrize, cudaStream_t stream);
+
+}  // namespace scatt

@@ -1,0 +1,496 @@
+// gj_inverse.cu -- batched FP64 matrix inversion, blocked Gauss-Jordan with
+// partial (row) pivoting, for the per-step dense inverses of the Numerov
+// R-ratio recurrence (R = 12 W^-1 - 10 I - Rinv_prev, N_total x N_total),
+// the Schur inverses Sinv(n) and the small per-energy solves.
+//
+// The reference inverts with LU + partial pivoting (dgetrf + dgetri, or
+// Eigen partialPivLu) and symmetrises with 0.5 (M + M^T)
+// (src/scatt/LapackInverse.hpp:53-92, ForwardRPropagator.cpp:357-358).
+// Gauss-Jordan with the same pivot rule (largest |entry| among rows not yet
+// pivoted, first index on ties) computes the same inverse to rounding and
+// is a better fit for the GPU: every block step is one uniform rank-16
+// update of the whole matrix instead of a shrinking trailing matrix.
+//
+// Block step kb (columns K = [k0, k0 + 16)):
+//   panel  : one CTA per matrix loads the n x 16 panel into shared memory,
+//            runs 16 pivoted GJ eliminations on it (pivot search by warp
+//            shuffles + one block reduction per column) and writes the
+//            transformed panel M, the row map sigma of this step and the
+//            running row identity.
+//   update : a DMMA tile kernel applies the deferred update to every other
+//            column:  new[i, c] = (i in K ? 0 : old[sigma(i), c])
+//                                  + sum_j M[i, j] * old[sigma(k0 + j), c].
+//            It reads the previous buffer and writes the other one
+//            (ping-pong), so the row interchanges need no separate pass
+//            and no CTA ever reads a value another CTA is writing.
+// finalize: out[:, j] = X[:, pi(j)] with pi the inverse of the composite
+//            row permutation (LAPACK getri's column interchanges), and
+//            optionally 0.5 (X + X^T) in the same pass.
+#include "common.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace scatt {
+
+namespace {
+
+constexpr int NB = GJ_NB;
+constexpr int PANEL_THREADS = 512;
+constexpr int PANEL_WARPS = PANEL_THREADS / 32;
+constexpr size_t PANEL_SMEM_LIMIT = 227 * 1024 - 1024;   // dynamic part; static scratch stays below 1 KB
+
+size_t panel_smem_bytes(int nmax) {
+    return (size_t)nmax * NB * sizeof(double) + 2 * (size_t)nmax * sizeof(int)
+           + PANEL_WARPS * (sizeof(double) + sizeof(int)) + 64;
+}
+
+__device__ __forceinline__ double* buf_of(const GjEntry& e, int which) {
+    return which == 0 ? e.A : e.W;
+}
+
+__device__ __forceinline__ void better(double& v, int& i, double v2, int i2) {
+    // larger magnitude wins; ties go to the smaller row index
+    if (v2 > v || (v2 == v && i2 >= 0 && (i < 0 || i2 < i))) { v = v2; i = i2; }
+}
+
+__global__ void __launch_bounds__(PANEL_THREADS)
+gj_panel_kernel(const GjEntry* __restrict__ entries, int kb) {
+    const GjEntry e = entries[blockIdx.x];
+    const int n = e.n;
+    const int k0 = kb * NB;
+    if (k0 >= n) return;
+    const int nb = min(NB, n - k0);
+    const double* src = buf_of(e, kb & 1);
+    double* dst = buf_of(e, (kb + 1) & 1);
+
+    // panel held column-major in shared memory: P[j * n + i] (consecutive
+    // rows -> consecutive banks, so row-parallel sweeps are conflict-free)
+    extern __shared__ double smem[];
+    double* P = smem;
+    int* loc = reinterpret_cast<int*>(P + (size_t)n * NB);
+    int* rid = loc + n;
+    double* red_v = reinterpret_cast<double*>(rid + n);
+    int* red_i = reinterpret_cast<int*>(red_v + PANEL_WARPS);
+    __shared__ int s_piv;
+    __shared__ int s_status;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    if (tid == 0) s_status = (kb == 0) ? 0 : e.status[0];
+    for (int j = 0; j < nb; ++j)
+        for (int i = tid; i < n; i += PANEL_THREADS)
+            P[j * n + i] = src[i + (size_t)(k0 + j) * e.ld];
+    for (int i = tid; i < n; i += PANEL_THREADS) {
+        loc[i] = i;
+        rid[i] = (kb == 0) ? i : e.rowid[i];
+    }
+    __syncthreads();
+
+    for (int j = 0; j < nb; ++j) {
+        const int k = k0 + j;
+        const double* Pj = P + j * n;
+        // ---- pivot search over rows [k, n): largest |P|, first index on ties
+        double bv = -1.0;
+        int bi = -1;
+        for (int i = k + tid; i < n; i += PANEL_THREADS) {
+            const double v = fabs(Pj[i]);
+            if (v > bv) { bv = v; bi = i; }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double ov = __shfl_down_sync(0xffffffffu, bv, off);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+            better(bv, bi, ov, oi);
+        }
+        if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
+        __syncthreads();
+        if (warp == 0) {
+            bv = lane < PANEL_WARPS ? red_v[lane] : -1.0;
+            bi = lane < PANEL_WARPS ? red_i[lane] : -1;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const double ov = __shfl_down_sync(0xffffffffu, bv, off);
+                const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+                better(bv, bi, ov, oi);
+            }
+            if (lane == 0) {
+                int p = bi;
+                if (p < 0) {               // every candidate NaN
+                    p = k;
+                    if (s_status == 0) { s_status = DEV_NONFINITE; e.status[1] = k; }
+                } else if (!(bv < INFINITY)) {
+                    if (s_status == 0) { s_status = DEV_NONFINITE; e.status[1] = k; }
+                } else if (bv == 0.0) {
+                    if (s_status == 0) { s_status = DEV_SINGULAR; e.status[1] = k; }
+                }
+                s_piv = p;
+            }
+        }
+        __syncthreads();
+        const int p = s_piv;
+        // ---- interchange rows k <-> p and scale the new pivot row (one phase)
+        if (tid < nb) {
+            double piv = P[j * n + p];
+            if (piv == 0.0) piv = 1.0;             // status already records the failure
+            const double inv = 1.0 / piv;
+            const double a = P[tid * n + k];
+            const double b = P[tid * n + p];
+            P[tid * n + p] = a;
+            P[tid * n + k] = (tid == j) ? inv : b * inv;
+        } else if (tid == NB && p != k) {
+            const int a = loc[k]; loc[k] = loc[p]; loc[p] = a;
+            const int b = rid[k]; rid[k] = rid[p]; rid[p] = b;
+        }
+        __syncthreads();
+        // ---- eliminate column j from every other row
+        const double inv = P[j * n + k];
+        for (int i = tid; i < n; i += PANEL_THREADS) {
+            if (i == k) continue;
+            const double f = P[j * n + i];
+            if (f != 0.0) {
+#pragma unroll
+                for (int jj = 0; jj < NB; ++jj) {
+                    if (jj < nb && jj != j) P[jj * n + i] -= f * P[jj * n + k];
+                }
+            }
+            P[j * n + i] = -f * inv;
+        }
+        __syncthreads();
+    }
+
+    for (int j = 0; j < nb; ++j)
+        for (int i = tid; i < n; i += PANEL_THREADS)
+            dst[i + (size_t)(k0 + j) * e.ld] = P[j * n + i];
+    for (int i = tid; i < n; i += PANEL_THREADS) {
+        e.sigma[i] = loc[i];
+        e.rowid[i] = rid[i];
+    }
+    if (tid == 0) e.status[0] = s_status;
+}
+
+// Register-resident panel: thread t owns rows t, t + 512, ... (R rows) and
+// keeps their 16 panel entries in registers; only the pivot row travels
+// through shared memory.  Two barriers per pivot.
+template <int R>
+__global__ void __launch_bounds__(PANEL_THREADS)
+gj_panel_reg_kernel(const GjEntry* __restrict__ entries, int kb) {
+    const GjEntry e = entries[blockIdx.x];
+    const int n = e.n;
+    const int k0 = kb * NB;
+    if (k0 >= n) return;
+    const int nb = min(NB, n - k0);
+    const double* src = buf_of(e, kb & 1);
+    double* dst = buf_of(e, (kb + 1) & 1);
+
+    extern __shared__ double smem[];
+    int* loc = reinterpret_cast<int*>(smem);
+    int* rid = loc + n;
+    __shared__ double red_v[2][PANEL_WARPS];
+    __shared__ int red_i[2][PANEL_WARPS];
+    __shared__ double prow[2][NB];     // pivot row p before the interchange
+    __shared__ double krow[2][NB];     // row k before the interchange
+    __shared__ int s_status;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double v[R][NB];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = tid + r * PANEL_THREADS;
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+            v[r][j] = (i < n && j < nb) ? src[i + (size_t)(k0 + j) * e.ld] : 0.0;
+    }
+    for (int i = tid; i < n; i += PANEL_THREADS) {
+        loc[i] = i;
+        rid[i] = (kb == 0) ? i : e.rowid[i];
+    }
+    if (tid == 0) s_status = (kb == 0) ? 0 : e.status[0];
+    __syncthreads();
+
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        if (j < nb) {
+            const int k = k0 + j;
+            const int par = j & 1;
+            double bv = -1.0;
+            int bi = -1;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = tid + r * PANEL_THREADS;
+                if (i >= k && i < n) {
+                    const double a = fabs(v[r][j]);
+                    if (a > bv) { bv = a; bi = i; }
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const double ov = __shfl_down_sync(0xffffffffu, bv, off);
+                const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+                better(bv, bi, ov, oi);
+            }
+            if (lane == 0) { red_v[par][warp] = bv; red_i[par][warp] = bi; }
+            __syncthreads();
+            // every thread reduces the 16 warp winners itself (no second round trip)
+            bv = -1.0;
+            bi = -1;
+#pragma unroll
+            for (int w = 0; w < PANEL_WARPS; ++w) better(bv, bi, red_v[par][w], red_i[par][w]);
+            int p = bi;
+            if (p < 0) p = k;
+            if (tid == 0) {
+                int st = 0;
+                if (bi < 0 || !(bv < INFINITY)) st = DEV_NONFINITE;
+                else if (bv == 0.0) st = DEV_SINGULAR;
+                if (st && s_status == 0) { s_status = st; e.status[1] = k; }
+                if (p != k) {
+                    const int a = loc[k]; loc[k] = loc[p]; loc[p] = a;
+                    const int b = rid[k]; rid[k] = rid[p]; rid[p] = b;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = tid + r * PANEL_THREADS;
+                if (i == p) {
+#pragma unroll
+                    for (int jj = 0; jj < NB; ++jj) prow[par][jj] = v[r][jj];
+                }
+                if (i == k) {
+#pragma unroll
+                    for (int jj = 0; jj < NB; ++jj) krow[par][jj] = v[r][jj];
+                }
+            }
+            __syncthreads();
+            double piv = prow[par][j];
+            if (piv == 0.0) piv = 1.0;             // the status word records the failure
+            const double inv = 1.0 / piv;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = tid + r * PANEL_THREADS;
+                if (i >= n) continue;
+                if (i == k) {
+#pragma unroll
+                    for (int jj = 0; jj < NB; ++jj) v[r][jj] = (jj == j) ? inv : prow[par][jj] * inv;
+                    continue;
+                }
+                if (i == p) {
+#pragma unroll
+                    for (int jj = 0; jj < NB; ++jj) v[r][jj] = krow[par][jj];
+                }
+                const double f = v[r][j];
+#pragma unroll
+                for (int jj = 0; jj < NB; ++jj)
+                    if (jj != j) v[r][jj] -= f * (prow[par][jj] * inv);
+                v[r][j] = -f * inv;
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = tid + r * PANEL_THREADS;
+        if (i < n) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+                if (j < nb) dst[i + (size_t)(k0 + j) * e.ld] = v[r][j];
+        }
+    }
+    for (int i = tid; i < n; i += PANEL_THREADS) {
+        e.sigma[i] = loc[i];
+        e.rowid[i] = rid[i];
+    }
+    if (tid == 0) e.status[0] = s_status;
+}
+
+constexpr int UBM = 64, UBN = 64, UPAD = 4, UTHREADS = 128;
+
+__device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1, double b0) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 "
+        "{%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a0), "d"(a1), "d"(b0));
+}
+
+__global__ void __launch_bounds__(UTHREADS)
+gj_update_kernel(const GjEntry* __restrict__ entries, int kb) {
+    const GjEntry e = entries[blockIdx.z];
+    const int n = e.n;
+    const int k0 = kb * NB;
+    if (k0 >= n) return;
+    const int nb = min(NB, n - k0);
+    const int r0 = blockIdx.x * UBM, c0 = blockIdx.y * UBN;
+    if (r0 >= n || c0 >= n) return;
+    // tiles fully inside the panel columns have nothing to do
+    if (c0 >= k0 && c0 + UBN <= k0 + nb) return;
+    const double* src = buf_of(e, kb & 1);
+    double* dst = buf_of(e, (kb + 1) & 1);
+
+    __shared__ double Ms[NB][UBM + UPAD];     // M[r0 + m][k0 + j]  -> Ms[j][m]
+    __shared__ double Xs[NB][UBN + UPAD];     // old[sigma(k0 + j)][c0 + c] -> Xs[j][c]
+    __shared__ int srow[UBM];
+    __shared__ int xrow[NB];
+
+    const int tid = threadIdx.x;
+    if (tid < UBM) {
+        const int i = r0 + tid;
+        srow[tid] = (i < n) ? e.sigma[i] : 0;
+    }
+    if (tid < NB) xrow[tid] = (tid < nb) ? e.sigma[k0 + tid] : 0;
+    __syncthreads();
+    for (int idx = tid; idx < NB * UBM; idx += UTHREADS) {
+        const int m = idx % UBM, j = idx / UBM;
+        const int i = r0 + m;
+        Ms[j][m] = (j < nb && i < n) ? dst[i + (size_t)(k0 + j) * e.ld] : 0.0;
+    }
+    for (int idx = tid; idx < NB * UBN; idx += UTHREADS) {
+        const int j = idx % NB, c = idx / NB;
+        const int col = c0 + c;
+        Xs[j][c] = (j < nb && col < n) ? src[xrow[j] + (size_t)col * e.ld] : 0.0;
+    }
+    __syncthreads();
+
+    const int lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+
+    double acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int jn = 0; jn < 4; ++jn)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int rl = wm + i * 16 + g + ((v >> 1) << 3);
+                const int row = r0 + rl;
+                const int col = c0 + wn + jn * 8 + 2 * t + (v & 1);
+                double old = 0.0;
+                if (row < n && col < n && !(row >= k0 && row < k0 + nb))
+                    old = src[srow[rl] + (size_t)col * e.ld];
+                acc[i][jn][v] = old;
+            }
+
+#pragma unroll
+    for (int kk = 0; kk < NB; kk += 4) {
+        double a[2][2], b[4];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            a[i][0] = Ms[kk + t][wm + i * 16 + g];
+            a[i][1] = Ms[kk + t][wm + i * 16 + g + 8];
+        }
+#pragma unroll
+        for (int jn = 0; jn < 4; ++jn) b[jn] = Xs[kk + t][wn + jn * 8 + g];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int jn = 0; jn < 4; ++jn) dmma_16x8x4(acc[i][jn], a[i][0], a[i][1], b[jn]);
+    }
+
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int jn = 0; jn < 4; ++jn)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int row = r0 + wm + i * 16 + g + ((v >> 1) << 3);
+                const int col = c0 + wn + jn * 8 + 2 * t + (v & 1);
+                if (row < n && col < n && !(col >= k0 && col < k0 + nb))
+                    dst[row + (size_t)col * e.ld] = acc[i][jn][v];
+            }
+}
+
+constexpr int FT = 32;
+
+__global__ void __launch_bounds__(FT * 8)
+gj_finalize_kernel(const GjEntry* __restrict__ entries, int nsteps_parity, int symmetrize) {
+    const GjEntry e = entries[blockIdx.z];
+    const int n = e.n;
+    const int i0 = blockIdx.x * FT, j0 = blockIdx.y * FT;
+    if (i0 >= n || j0 >= n) return;
+    // the result of the last block step lives in buffer (number of steps of this matrix) % 2
+    const int steps = (n + NB - 1) / NB;
+    (void)nsteps_parity;
+    const double* X = buf_of(e, steps & 1);
+
+    __shared__ int pi_i[FT], pi_j[FT];
+    __shared__ double T1[FT][FT + 1];
+    __shared__ double T2[FT][FT + 1];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
+    // pi = inverse of rowid: pi[rowid[r]] = r.  Scan for the 32 + 32 labels we need.
+    if (threadIdx.x < 64) {
+        // filled below by the scan
+    }
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        const int id = e.rowid[r];
+        if (id >= i0 && id < i0 + FT) pi_i[id - i0] = r;
+        if (id >= j0 && id < j0 + FT) pi_j[id - j0] = r;
+    }
+    __syncthreads();
+    // T1[a][b] = X[i0 + a][pi(j0 + b)],  T2[a][b] = X[j0 + a][pi(i0 + b)]
+    for (int b = ty; b < FT; b += 8) {
+        const int a = tx;
+        if (j0 + b < n && i0 + a < n) T1[a][b] = X[(i0 + a) + (size_t)pi_j[b] * e.ld];
+        if (symmetrize && i0 + b < n && j0 + a < n) T2[a][b] = X[(j0 + a) + (size_t)pi_i[b] * e.ld];
+    }
+    __syncthreads();
+    for (int b = ty; b < FT; b += 8) {
+        const int a = tx;
+        const int i = i0 + a, j = j0 + b;
+        if (i < n && j < n) {
+            double v = T1[a][b];
+            if (symmetrize) v = 0.5 * (v + T2[b][a]);
+            e.out[i + (size_t)j * e.ldo] = v;
+        }
+    }
+}
+
+}  // namespace
+
+int gj_max_order() {
+    // shared memory per panel: n * (NB doubles + 2 ints) + reduction scratch
+    int lo = 1, hi = 1 << 16;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (panel_smem_bytes(mid) <= PANEL_SMEM_LIMIT) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+int gj_inverse_batched(const GjEntry* entries_dev, int count, int nmax,
+                       bool symmetrize, cudaStream_t stream) {
+    if (count <= 0 || nmax <= 0) return SCATT_OK;
+    if (nmax > gj_max_order()) {
+        set_last_error("gj_inverse_batched: order " + std::to_string(nmax) +
+                       " exceeds the single-CTA panel limit " + std::to_string(gj_max_order()));
+        return SCATT_ERR_SIZE;
+    }
+    const size_t smem = panel_smem_bytes(nmax);
+    static bool attr_set = false;
+    if (!attr_set) {
+        SCATT_CUDA_TRY(cudaFuncSetAttribute(gj_panel_kernel,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)PANEL_SMEM_LIMIT));
+        attr_set = true;
+    }
+    const int steps = (nmax + NB - 1) / NB;
+    const int tiles = (nmax + UBM - 1) / UBM;
+    dim3 ugrid(tiles, tiles, count);
+    const int R = (nmax + PANEL_THREADS - 1) / PANEL_THREADS;
+    const size_t smem_reg = 2 * (size_t)nmax * sizeof(int);
+    for (int kb = 0; kb < steps; ++kb) {
+        switch (R) {
+            case 1: gj_panel_reg_kernel<1><<<count, PANEL_THREADS, smem_reg, stream>>>(entries_dev, kb); break;
+            case 2: gj_panel_reg_kernel<2><<<count, PANEL_THREADS, smem_reg, stream>>>(entries_dev, kb); break;
+            case 3: gj_panel_reg_kernel<3><<<count, PANEL_THREADS, smem_reg, stream>>>(entries_dev, kb); break;
+            default: gj_panel_kernel<<<count, PANEL_THREADS, smem, stream>>>(entries_dev, kb); break;
+        }
+        gj_update_kernel<<<ugrid, UTHREADS, 0, stream>>>(entries_dev, kb);
+    }
+    const int ft = (nmax + FT - 1) / FT;
+    gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, steps & 1,
+                                                                   symmetrize ? 1 : 0);
+    SCATT_CUDA_TRY(cudaGetLastError());
+    return SCATT_OK;
+}
+
+}  // namespace scatt

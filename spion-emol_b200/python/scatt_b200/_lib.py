@@ -1,0 +1,120 @@
+"""ctypes binding of libscatt_b200.so (the C ABI declared in include/scatt_b200.h).
+
+The library is built in-tree (spion-emol_b200/libscatt_b200.so).  Loading it
+does not need a GPU; every compute entry point returns SCATT_ERR_NO_DEVICE
+when none is visible, and this module turns non-zero statuses into
+ScattError.  There is no CPU fallback anywhere in the package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(os.path.dirname(_HERE))          # spion-emol_b200/
+LIB_PATH = os.path.join(PKG_ROOT, "libscatt_b200.so")
+
+STATUS = {
+    0: "SCATT_OK", 1: "SCATT_ERR_ARG", 2: "SCATT_ERR_CUDA", 3: "SCATT_ERR_SIZE",
+    4: "SCATT_ERR_SINGULAR", 5: "SCATT_ERR_NONFINITE", 6: "SCATT_ERR_CLOSED_CHANNEL",
+    7: "SCATT_ERR_NO_DEVICE", 8: "SCATT_ERR_STATE", 9: "SCATT_ERR_OOM", 10: "SCATT_ERR_FIT_WINDOW",
+}
+
+
+class ScattError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+dptr = C.POINTER(C.c_double)
+iptr = C.POINTER(C.c_int)
+
+
+def lib():
+    """Load (once) and return the CDLL with argtypes set."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ScattError(2, f"{LIB_PATH} is missing: build it with python spion-emol_b200/build.py")
+    L = C.CDLL(LIB_PATH)
+    L.scatt_version.restype = C.c_char_p
+    L.scatt_last_error.restype = C.c_char_p
+    L.scatt_device_count.argtypes = [iptr]
+    for f in ("scatt_wigner3j", "scatt_gaunt_real"):
+        getattr(L, f).restype = C.c_double
+        getattr(L, f).argtypes = [C.c_int] * 6
+    L.scatt_angular_dipole.restype = C.c_double
+    L.scatt_angular_dipole.argtypes = [C.c_int] * 5
+    L.scatt_velocity_coef.restype = C.c_double
+    L.scatt_velocity_coef.argtypes = [C.c_int] * 2
+    for f in ("scatt_riccati_j", "scatt_riccati_y"):
+        getattr(L, f).restype = C.c_double
+        getattr(L, f).argtypes = [C.c_int, C.c_double]
+    L.scatt_inverse_batched.argtypes = [C.c_int, C.c_int, dptr, dptr, C.c_int, iptr]
+    L.scatt_dgemm.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                              dptr, C.c_int, dptr, C.c_int, C.c_double, dptr, C.c_int]
+    L.scatt_bench_inverse.argtypes = [C.c_int, C.c_int, C.c_int, dptr]
+    _lib = L
+    return L
+
+
+def check(code: int):
+    if code != 0:
+        raise ScattError(code, lib().scatt_last_error().decode())
+
+
+def as_dptr(a: np.ndarray):
+    return a.ctypes.data_as(dptr)
+
+
+def as_iptr(a: np.ndarray):
+    return a.ctypes.data_as(iptr)
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    check(lib().scatt_device_count(C.byref(n)))
+    return n.value
+
+
+def inverse_batched(A: np.ndarray, symmetrize: bool = False):
+    """Inverse of each n x n matrix of A (shape (count, n, n) or (n, n)); returns (inv, status)."""
+    A = np.asarray(A, dtype=np.float64)
+    single = A.ndim == 2
+    if single:
+        A = A[None]
+    count, n, _ = A.shape
+    # column-major per matrix: pass the transpose's memory
+    Af = np.ascontiguousarray(np.transpose(A, (0, 2, 1)))
+    out = np.empty_like(Af)
+    st = np.zeros((count, 2), dtype=np.int32)
+    code = lib().scatt_inverse_batched(n, count, as_dptr(Af), as_dptr(out), int(symmetrize), as_iptr(st))
+    inv = np.transpose(out, (0, 2, 1))
+    if code not in (0, 4, 5):
+        check(code)
+    return (inv[0] if single else inv), st
+
+
+def dgemm(A, B, C=None, alpha=1.0, beta=0.0, opA=0, opB=0):
+    """alpha op(A) op(B) + beta C on the device."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    B = np.asfortranarray(B, dtype=np.float64)
+    M = A.shape[1] if opA else A.shape[0]
+    K = A.shape[0] if opA else A.shape[1]
+    N = B.shape[0] if opB else B.shape[1]
+    Cm = np.zeros((M, N), order="F") if C is None else np.array(C, dtype=np.float64, order="F", copy=True)
+    check(lib().scatt_dgemm(opA, opB, M, N, K, alpha, as_dptr(A), A.shape[0], as_dptr(B), B.shape[0],
+                            beta, as_dptr(Cm), M))
+    return Cm
+
+
+def bench_inverse(n: int, count: int, reps: int = 5) -> float:
+    ms = C.c_double(0.0)
+    check(lib().scatt_bench_inverse(n, count, reps, C.byref(ms)))
+    return ms.value

@@ -1,0 +1,60 @@
+"""Device building blocks against numpy fp64: batched GJ inverse and DMMA GEMM."""
+import numpy as np
+import pytest
+
+from scatt_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n,count", [(1, 1), (5, 3), (16, 2), (17, 2), (40, 4), (64, 1), (100, 3), (162, 2), (257, 1), (441, 1), (1046, 1)])
+def test_inverse_matches_numpy(n, count):
+    rng = np.random.default_rng(42 + n)
+    A = rng.standard_normal((count, n, n)) + 3.0 * np.eye(n)
+    inv, st = _lib.inverse_batched(A)
+    assert np.all(st == 0)
+    for b in range(count):
+        ref = np.linalg.inv(A[b])
+        err = np.max(np.abs(inv[b] - ref)) / np.max(np.abs(ref))
+        assert err < 1e-12, (n, b, err)
+
+
+def test_inverse_needs_pivoting():
+    # zero diagonal: no-pivot elimination would fail immediately
+    rng = np.random.default_rng(7)
+    n = 48
+    P = np.eye(n)[rng.permutation(n)]
+    A = P @ (np.diag(rng.uniform(1, 2, n)) + 0.1 * rng.standard_normal((n, n)))
+    A[np.diag_indices(n)] = 0.0
+    inv, st = _lib.inverse_batched(A)
+    assert np.all(st == 0)
+    assert np.max(np.abs(inv @ A - np.eye(n))) < 1e-11
+
+
+def test_inverse_symmetrized():
+    rng = np.random.default_rng(3)
+    n = 130
+    M = rng.standard_normal((n, n))
+    S = M + M.T + n * np.eye(n)
+    inv, st = _lib.inverse_batched(S, symmetrize=True)
+    assert np.array_equal(inv, inv.T)
+    ref = np.linalg.inv(S)
+    assert np.max(np.abs(inv - ref)) / np.max(np.abs(ref)) < 1e-13
+
+
+def test_inverse_singular_reports_status():
+    A = np.ones((3, 4, 4))
+    inv, st = _lib.inverse_batched(A)
+    assert np.all(st[:, 0] == 1)
+
+
+@pytest.mark.parametrize("opA,opB", [(0, 0), (1, 0), (0, 1), (1, 1)])
+@pytest.mark.parametrize("M,N,K", [(1, 1, 1), (7, 13, 5), (64, 64, 16), (65, 63, 17), (200, 130, 441), (441, 605, 441)])
+def test_dgemm_matches_numpy(opA, opB, M, N, K):
+    rng = np.random.default_rng(M * 1000 + N + K)
+    A = rng.standard_normal((K, M) if opA else (M, K))
+    B = rng.standard_normal((N, K) if opB else (K, N))
+    C0 = rng.standard_normal((M, N))
+    out = _lib.dgemm(A, B, C0, alpha=-0.75, beta=0.5, opA=opA, opB=opB)
+    ref = -0.75 * ((A.T if opA else A) @ (B.T if opB else B)) + 0.5 * C0
+    assert np.max(np.abs(out - ref)) <= 1e-13 * max(1.0, np.max(np.abs(ref))) * np.sqrt(K + 1)
