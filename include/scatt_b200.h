@@ -116,6 +116,7 @@ typedef struct {
     int    max_batch;             /* energies per device batch; 0 = as many as fit    */
     int    use_graphs;            /* 1: replay the radial step as a CUDA graph        */
     int    diagnostics;           /* 1: S-matrix unitarity and eigenphases            */
+    int    timing;                /* 1: CUDA-event timing of the solve (scatt_last_stats) */
 } scatt_solve_opts;
 
 /* Diagnostics per energy (index into scatt_outputs.diag). */
@@ -174,6 +175,12 @@ int scatt_solve_batch(scatt_ctx* ctx, int n_energy, const double* energies, cons
                       const scatt_solve_opts* opts, const scatt_outputs* outputs);
 /* Default policies (the reference's). */
 void scatt_default_opts(scatt_solve_opts* opts);
+/* Timing of the last scatt_solve_batch with opts.timing = 1 (device clock,
+ * CUDA events on the library stream): out[0] device seconds of the whole
+ * solve, out[1] seconds spent in the sampled R^-1 inversions, out[2] number
+ * of sampled inversions, out[3] kernel launches issued, out[4] radial-sweep
+ * seconds, out[5] post-processing seconds. */
+int scatt_last_stats(scatt_ctx* ctx, double* out6);
 
 #ifdef __cplusplus
 }

@@ -38,26 +38,46 @@ CHI_CUTOFF = 1e-15     # WavefunctionSetup.hpp:92
 
 
 # ---------------------------------------------------------------- inverses
+# The reference compiles src/scatt/LapackInverse.hpp two ways: with MKL
+# (dgetrf/dgetri; dsytrf/dsytri on the LOWER triangle, mirrored) or without
+# (Eigen partialPivLu().inverse(), plus 0.5 (M + M^T) for the "symmetric"
+# variant, LapackInverse.hpp:88-91 and :166-176).  The oracle follows the
+# Eigen build by default (BUILD = "eigen"); BUILD = "mkl" selects the MKL
+# routines.  The two builds differ from each other by O(eps * cond) per step;
+# on the synthetic configs that reaches ~2e-10 in K.
+BUILD = "eigen"
+
+
 def inverse_general(A: np.ndarray) -> np.ndarray:
-    """LapackInverse.hpp:53-92 -- dgetrf + dgetri."""
+    """LapackInverse.hpp:53-92."""
+    if BUILD == "mkl":
+        lu, piv, info = lapack.dgetrf(A)
+        if info != 0:
+            raise np.linalg.LinAlgError(f"inverse_general: dgetrf failed (singular pivot), info = {info}")
+        inv, info = lapack.dgetri(lu, piv)
+        if info != 0:
+            raise np.linalg.LinAlgError(f"inverse_general: dgetri failed, info = {info}")
+        return inv
+    # partial-pivot LU, then solve LU X = I (Eigen's partialPivLu().inverse())
     lu, piv, info = lapack.dgetrf(A)
     if info != 0:
-        raise np.linalg.LinAlgError(f"inverse_general: dgetrf failed (singular pivot), info = {info}")
-    inv, info = lapack.dgetri(lu, piv)
-    if info != 0:
-        raise np.linalg.LinAlgError(f"inverse_general: dgetri failed, info = {info}")
+        raise np.linalg.LinAlgError(f"inverse_general: singular pivot, info = {info}")
+    inv, info = lapack.dgetrs(lu, piv, np.eye(A.shape[0]))
     return inv
 
 
 def inverse_symmetric_indefinite(A: np.ndarray) -> np.ndarray:
-    """LapackInverse.hpp:120-178 -- dsytrf + dsytri on the LOWER triangle, mirrored."""
-    ldu, ipiv, info = lapack.dsytrf(A, lower=1)
-    if info != 0:
-        raise np.linalg.LinAlgError(f"inverse_symmetric_indefinite: dsytrf failed, info = {info}")
-    inv, info = lapack.dsytri(ldu, ipiv, lower=1)
-    if info != 0:
-        raise np.linalg.LinAlgError(f"inverse_symmetric_indefinite: dsytri failed, info = {info}")
-    return np.tril(inv) + np.tril(inv, -1).T
+    """LapackInverse.hpp:120-178."""
+    if BUILD == "mkl":
+        ldu, ipiv, info = lapack.dsytrf(A, lower=1)
+        if info != 0:
+            raise np.linalg.LinAlgError(f"inverse_symmetric_indefinite: dsytrf failed, info = {info}")
+        inv, info = lapack.dsytri(ldu, ipiv, lower=1)
+        if info != 0:
+            raise np.linalg.LinAlgError(f"inverse_symmetric_indefinite: dsytri failed, info = {info}")
+        return np.tril(inv) + np.tril(inv, -1).T
+    inv = inverse_general(A)
+    return 0.5 * (inv + inv.T)
 
 
 def sym(M):
@@ -468,8 +488,8 @@ def simpson(f: np.ndarray, h: float) -> np.ndarray:
 
     def one_third(m):
         s = f[..., 0] + f[..., m - 1]
-        s = s + 4.0 * np.sum(f[..., 1:m - 1:2], axis=-1)
-        s = s + 2.0 * np.sum(f[..., 2:m - 2:2], axis=-1)
+        s = s + 4.0 * np.sum(f[..., 1:max(m - 1, 0):2], axis=-1)
+        s = s + 2.0 * np.sum(f[..., 2:max(m - 2, 0):2], axis=-1)
         return s * h / 3.0
 
     if n == 2:

@@ -18,6 +18,11 @@ thread_local std::string g_last_error;
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
+unsigned long long& launch_counter() {
+    static unsigned long long c = 0;
+    return c;
+}
+
 int require_device() {
     int n = 0;
     cudaError_t e = cudaGetDeviceCount(&n);

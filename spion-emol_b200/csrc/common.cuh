@@ -42,6 +42,10 @@ inline int cuda_status(cudaError_t e, const char* what) {
         if (_s != SCATT_OK) return _s;                                          \
     } while (0)
 
+// Kernel launches issued by the library since load (benchmark bookkeeping).
+unsigned long long& launch_counter();
+#define SCATT_COUNT_LAUNCH(n) (::scatt::launch_counter() += (n))
+
 // Device-side status codes written into per-matrix status words.
 enum DeviceStatus : int {
     DEV_OK = 0,

@@ -157,6 +157,7 @@ int gemm_batched(const GemmEntry* entries_dev, int count, int maxM, int maxN,
     else if (opA == 0 && opB == 1) gemm_kernel<0, 1><<<grid, THREADS, 0, stream>>>(entries_dev);
     else                           gemm_kernel<1, 1><<<grid, THREADS, 0, stream>>>(entries_dev);
     SCATT_CUDA_TRY(cudaGetLastError());
+    SCATT_COUNT_LAUNCH(1);
     return SCATT_OK;
 }
 

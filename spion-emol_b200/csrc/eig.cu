@@ -167,6 +167,7 @@ int sym_eigvals_batched(const EigEntry* entries_dev, int count, int nmax, int nw
     dim3 g((want + 127) / 128, count);
     bisect_kernel<<<g, 128, 0, stream>>>(entries_dev, nwant);
     SCATT_CUDA_TRY(cudaGetLastError());
+    SCATT_COUNT_LAUNCH(2);
     return SCATT_OK;
 }
 

@@ -302,6 +302,171 @@ gj_panel_reg_kernel(const GjEntry* __restrict__ entries, int kb) {
     if (tid == 0) e.status[0] = s_status;
 }
 
+// Panel v3: 1024 threads, two threads per row (8 panel columns each, in
+// registers), rows tid/2 + 512 r for r < R (n <= 1536).  The pivot search is
+// a shuffle reduction (per warp, then once more over the 32 warp winners);
+// the pivot row travels through shared memory.  Two barriers per pivot.
+constexpr int P3_THREADS = 1024;
+
+__device__ __forceinline__ void better_key(double& v, int& i, double v2, int i2) {
+    if (v2 > v || (v2 == v && i2 >= 0 && (i < 0 || i2 < i))) { v = v2; i = i2; }
+}
+
+template <int QW, int R>
+__global__ void __launch_bounds__(P3_THREADS, 1)
+gj_panel3_kernel(const GjEntry* __restrict__ entries, int kb) {
+    constexpr int CW = NB / QW;                 // panel columns per thread
+    constexpr int RPP = P3_THREADS / QW;        // rows per pass
+    const GjEntry e = entries[blockIdx.x];
+    const int n = e.n;
+    const int k0 = kb * NB;
+    if (k0 >= n) return;
+    const int nb = min(NB, n - k0);
+    const double* src = buf_of(e, kb & 1);
+    double* dst = buf_of(e, (kb + 1) & 1);
+
+    extern __shared__ double smem[];
+    int* loc = reinterpret_cast<int*>(smem);
+    int* rid = loc + n;
+    __shared__ double red_v[2][32];
+    __shared__ int red_i[2][32];
+    __shared__ double prow[2][NB];
+    __shared__ double krow[2][NB];
+    __shared__ int s_status;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int q = tid / QW, h = tid % QW;       // row slot, column group
+    const int cbase = CW * h;
+    double v[R][CW];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = q + r * RPP;
+#pragma unroll
+        for (int c = 0; c < CW; ++c) {
+            const int j = cbase + c;
+            v[r][c] = (i < n && j < nb) ? src[i + (size_t)(k0 + j) * e.ld] : 0.0;
+        }
+    }
+    for (int i = tid; i < n; i += P3_THREADS) {
+        loc[i] = i;
+        rid[i] = (kb == 0) ? i : e.rowid[i];
+    }
+    if (tid == 0) s_status = (kb == 0) ? 0 : e.status[0];
+    __syncthreads();
+
+#pragma unroll 1
+    for (int j = 0; j < nb; ++j) {
+        const int k = k0 + j;
+        const int par = j & 1;
+        const int hj = j / CW, cj = j % CW;
+        // ---- pivot search over rows [k, n) of column j
+        double bv = -1.0;
+        int bi = -1;
+        if (h == hj) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = q + r * RPP;
+                double x = 0.0;
+#pragma unroll
+                for (int c = 0; c < CW; ++c) if (c == cj) x = v[r][c];
+                if (i >= k && i < n) {
+                    const double a = fabs(x);
+                    if (a > bv) { bv = a; bi = i; }
+                }
+            }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+            better_key(bv, bi, ov, oi);
+        }
+        if (lane == 0) { red_v[par][warp] = bv; red_i[par][warp] = bi; }
+        __syncthreads();
+        bv = red_v[par][lane];
+        bi = red_i[par][lane];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+            better_key(bv, bi, ov, oi);
+        }
+        const int p = bi < 0 ? k : bi;
+        if (tid == 0) {
+            int st = 0;
+            if (bi < 0 || !(bv < INFINITY)) st = DEV_NONFINITE;
+            else if (bv == 0.0) st = DEV_SINGULAR;
+            if (st && s_status == 0) { s_status = st; e.status[1] = k; }
+            if (p != k) {
+                const int a = loc[k]; loc[k] = loc[p]; loc[p] = a;
+                const int b2 = rid[k]; rid[k] = rid[p]; rid[p] = b2;
+            }
+        }
+        // ---- publish rows p and k
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = q + r * RPP;
+            if (i == p) {
+#pragma unroll
+                for (int c = 0; c < CW; ++c) prow[par][cbase + c] = v[r][c];
+            }
+            if (i == k) {
+#pragma unroll
+                for (int c = 0; c < CW; ++c) krow[par][cbase + c] = v[r][c];
+            }
+        }
+        __syncthreads();
+        double piv = prow[par][j];
+        if (piv == 0.0) piv = 1.0;              // the status word records the failure
+        const double inv = 1.0 / piv;
+        double sp[CW];
+#pragma unroll
+        for (int c = 0; c < CW; ++c) sp[c] = prow[par][cbase + c] * inv;
+        const int owner = (lane & ~(QW - 1)) | hj;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = q + r * RPP;
+            double mine = 0.0;
+#pragma unroll
+            for (int c = 0; c < CW; ++c) if (c == cj) mine = v[r][c];
+            double f = __shfl_sync(0xffffffffu, mine, owner);
+            if (i >= n) continue;
+            if (i == k) {
+#pragma unroll
+                for (int c = 0; c < CW; ++c) v[r][c] = (cbase + c == j) ? inv : sp[c];
+                continue;
+            }
+            if (i == p) {
+#pragma unroll
+                for (int c = 0; c < CW; ++c) v[r][c] = krow[par][cbase + c];
+                f = krow[par][j];
+            }
+#pragma unroll
+            for (int c = 0; c < CW; ++c) {
+                if (cbase + c == j) v[r][c] = -f * inv;
+                else v[r][c] -= f * sp[c];
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = q + r * RPP;
+        if (i < n) {
+#pragma unroll
+            for (int c = 0; c < CW; ++c) {
+                const int j = cbase + c;
+                if (j < nb) dst[i + (size_t)(k0 + j) * e.ld] = v[r][c];
+            }
+        }
+    }
+    for (int i = tid; i < n; i += P3_THREADS) {
+        e.sigma[i] = loc[i];
+        e.rowid[i] = rid[i];
+    }
+    if (tid == 0) e.status[0] = s_status;
+}
+
 constexpr int UBM = 64, UBN = 64, UPAD = 4, UTHREADS = 128;
 
 __device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1, double b0) {
@@ -312,91 +477,115 @@ __device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1
         : "d"(a0), "d"(a1), "d"(b0));
 }
 
-__global__ void __launch_bounds__(UTHREADS)
-gj_update_kernel(const GjEntry* __restrict__ entries, int kb) {
+// Update v2: 64 x 64 tile, 256 threads.  All global loads of the tile (old
+// C rows through sigma, the 16 gathered X rows, the 16 panel columns M) are
+// issued back to back into registers and parked in shared memory; the DMMA
+// works from shared memory; the result goes out through shared memory with
+// coalesced stores.
+constexpr int U2T = 256, U2S = 66;   // column stride of the C tile (bank-conflict free)
+constexpr size_t U2_SMEM = (64 * U2S + 2 * NB * 68) * sizeof(double);
+
+__global__ void __launch_bounds__(U2T)
+gj_update2_kernel(const GjEntry* __restrict__ entries, int kb) {
     const GjEntry e = entries[blockIdx.z];
     const int n = e.n;
     const int k0 = kb * NB;
     if (k0 >= n) return;
     const int nb = min(NB, n - k0);
-    const int r0 = blockIdx.x * UBM, c0 = blockIdx.y * UBN;
+    const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
     if (r0 >= n || c0 >= n) return;
-    // tiles fully inside the panel columns have nothing to do
-    if (c0 >= k0 && c0 + UBN <= k0 + nb) return;
+    if (c0 >= k0 && c0 + 64 <= k0 + nb) return;
     const double* src = buf_of(e, kb & 1);
     double* dst = buf_of(e, (kb + 1) & 1);
 
-    __shared__ double Ms[NB][UBM + UPAD];     // M[r0 + m][k0 + j]  -> Ms[j][m]
-    __shared__ double Xs[NB][UBN + UPAD];     // old[sigma(k0 + j)][c0 + c] -> Xs[j][c]
-    __shared__ int srow[UBM];
+    extern __shared__ double u2smem[];
+    double (*Cs)[U2S] = reinterpret_cast<double (*)[U2S]>(u2smem);                 // Cs[col][row]
+    double (*Ms)[68] = reinterpret_cast<double (*)[68]>(u2smem + 64 * U2S);
+    double (*Xs)[68] = reinterpret_cast<double (*)[68]>(u2smem + 64 * U2S + NB * 68);
+    __shared__ int srow[64];
     __shared__ int xrow[NB];
-
     const int tid = threadIdx.x;
-    if (tid < UBM) {
-        const int i = r0 + tid;
-        srow[tid] = (i < n) ? e.sigma[i] : 0;
+    if (tid < 64) srow[tid] = (r0 + tid < n) ? e.sigma[r0 + tid] : 0;
+    else if (tid < 64 + NB) {
+        const int j = tid - 64;
+        xrow[j] = (j < nb) ? e.sigma[k0 + j] : 0;
     }
-    if (tid < NB) xrow[tid] = (tid < nb) ? e.sigma[k0 + tid] : 0;
     __syncthreads();
-    for (int idx = tid; idx < NB * UBM; idx += UTHREADS) {
-        const int m = idx % UBM, j = idx / UBM;
-        const int i = r0 + m;
-        Ms[j][m] = (j < nb && i < n) ? dst[i + (size_t)(k0 + j) * e.ld] : 0.0;
+    double rc[16], rm[4], rx[4];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const int idx = tid + u * U2T;
+        const int row = idx & 63, col = idx >> 6;
+        const int gi = r0 + row, gc = c0 + col;
+        double v = 0.0;
+        if (gi < n && gc < n && !(gi >= k0 && gi < k0 + nb)) v = src[srow[row] + (size_t)gc * e.ld];
+        rc[u] = v;
     }
-    for (int idx = tid; idx < NB * UBN; idx += UTHREADS) {
-        const int j = idx % NB, c = idx / NB;
-        const int col = c0 + c;
-        Xs[j][c] = (j < nb && col < n) ? src[xrow[j] + (size_t)col * e.ld] : 0.0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int idx = tid + u * U2T;       // 0..1023
+        const int m = idx & 63, j = idx >> 6;
+        const int gi = r0 + m;
+        rm[u] = (j < nb && gi < n) ? dst[gi + (size_t)(k0 + j) * e.ld] : 0.0;
+        const int c = idx >> 4, jj = idx & 15;
+        const int gc = c0 + c;
+        rx[u] = (jj < nb && gc < n) ? src[xrow[jj] + (size_t)gc * e.ld] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const int idx = tid + u * U2T;
+        Cs[idx >> 6][idx & 63] = rc[u];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int idx = tid + u * U2T;
+        Ms[idx >> 6][idx & 63] = rm[u];
+        Xs[idx & 15][idx >> 4] = rx[u];
     }
     __syncthreads();
 
     const int lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
-    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
-
-    double acc[2][4][4];
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+    double acc[2][2][4];
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int jn = 0; jn < 4; ++jn)
+        for (int jn = 0; jn < 2; ++jn)
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const int rl = wm + i * 16 + g + ((v >> 1) << 3);
-                const int row = r0 + rl;
-                const int col = c0 + wn + jn * 8 + 2 * t + (v & 1);
-                double old = 0.0;
-                if (row < n && col < n && !(row >= k0 && row < k0 + nb))
-                    old = src[srow[rl] + (size_t)col * e.ld];
-                acc[i][jn][v] = old;
-            }
-
+            for (int v = 0; v < 4; ++v)
+                acc[i][jn][v] = Cs[wn + jn * 8 + 2 * t + (v & 1)][wm + i * 16 + g + ((v >> 1) << 3)];
 #pragma unroll
     for (int kk = 0; kk < NB; kk += 4) {
-        double a[2][2], b[4];
+        double a[2][2], b[2];
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
             a[i][0] = Ms[kk + t][wm + i * 16 + g];
             a[i][1] = Ms[kk + t][wm + i * 16 + g + 8];
         }
 #pragma unroll
-        for (int jn = 0; jn < 4; ++jn) b[jn] = Xs[kk + t][wn + jn * 8 + g];
+        for (int jn = 0; jn < 2; ++jn) b[jn] = Xs[kk + t][wn + jn * 8 + g];
 #pragma unroll
         for (int i = 0; i < 2; ++i)
 #pragma unroll
-            for (int jn = 0; jn < 4; ++jn) dmma_16x8x4(acc[i][jn], a[i][0], a[i][1], b[jn]);
+            for (int jn = 0; jn < 2; ++jn) dmma_16x8x4(acc[i][jn], a[i][0], a[i][1], b[jn]);
     }
-
+    __syncthreads();
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int jn = 0; jn < 4; ++jn)
+        for (int jn = 0; jn < 2; ++jn)
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const int row = r0 + wm + i * 16 + g + ((v >> 1) << 3);
-                const int col = c0 + wn + jn * 8 + 2 * t + (v & 1);
-                if (row < n && col < n && !(col >= k0 && col < k0 + nb))
-                    dst[row + (size_t)col * e.ld] = acc[i][jn][v];
-            }
+            for (int v = 0; v < 4; ++v)
+                Cs[wn + jn * 8 + 2 * t + (v & 1)][wm + i * 16 + g + ((v >> 1) << 3)] = acc[i][jn][v];
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const int idx = tid + u * U2T;
+        const int row = idx & 63, col = idx >> 6;
+        const int gi = r0 + row, gc = c0 + col;
+        if (gi < n && gc < n && !(gc >= k0 && gc < k0 + nb)) dst[gi + (size_t)gc * e.ld] = Cs[col][row];
+    }
 }
 
 constexpr int FT = 32;
@@ -467,6 +656,8 @@ int gj_inverse_batched(const GjEntry* entries_dev, int count, int nmax,
     const size_t smem = panel_smem_bytes(nmax);
     static bool attr_set = false;
     if (!attr_set) {
+        SCATT_CUDA_TRY(cudaFuncSetAttribute(gj_update2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)U2_SMEM));
         SCATT_CUDA_TRY(cudaFuncSetAttribute(gj_panel_kernel,
                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)PANEL_SMEM_LIMIT));
@@ -475,21 +666,24 @@ int gj_inverse_batched(const GjEntry* entries_dev, int count, int nmax,
     const int steps = (nmax + NB - 1) / NB;
     const int tiles = (nmax + UBM - 1) / UBM;
     dim3 ugrid(tiles, tiles, count);
-    const int R = (nmax + PANEL_THREADS - 1) / PANEL_THREADS;
     const size_t smem_reg = 2 * (size_t)nmax * sizeof(int);
     for (int kb = 0; kb < steps; ++kb) {
-        switch (R) {
-            case 1: gj_panel_reg_kernel<1><<<count, PANEL_THREADS, smem_reg, stream>>>(entries_dev, kb); break;
-            case 2: gj_panel_reg_kernel<2><<<count, PANEL_THREADS, smem_reg, stream>>>(entries_dev, kb); break;
-            case 3: gj_panel_reg_kernel<3><<<count, PANEL_THREADS, smem_reg, stream>>>(entries_dev, kb); break;
-            default: gj_panel_kernel<<<count, PANEL_THREADS, smem, stream>>>(entries_dev, kb); break;
-        }
-        gj_update_kernel<<<ugrid, UTHREADS, 0, stream>>>(entries_dev, kb);
+        if (nmax <= 512)
+            gj_panel3_kernel<2, 1><<<count, P3_THREADS, smem_reg, stream>>>(entries_dev, kb);
+        else if (nmax <= 1024)
+            gj_panel3_kernel<4, 4><<<count, P3_THREADS, smem_reg, stream>>>(entries_dev, kb);
+        else if (nmax <= 1280)
+            gj_panel3_kernel<4, 5><<<count, P3_THREADS, smem_reg, stream>>>(entries_dev, kb);
+
+        else
+            gj_panel_kernel<<<count, PANEL_THREADS, smem, stream>>>(entries_dev, kb);
+        gj_update2_kernel<<<ugrid, U2T, U2_SMEM, stream>>>(entries_dev, kb);
     }
     const int ft = (nmax + FT - 1) / FT;
     gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, steps & 1,
                                                                    symmetrize ? 1 : 0);
     SCATT_CUDA_TRY(cudaGetLastError());
+    SCATT_COUNT_LAUNCH(2 * steps + 1);
     return SCATT_OK;
 }
 

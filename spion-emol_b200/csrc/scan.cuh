@@ -54,10 +54,17 @@ struct ScanTables {
     bool ready = false;
 };
 
+struct SolveStats {
+    double device_s = 0.0, rinv_s = 0.0, sweep_s = 0.0, post_s = 0.0;
+    double rinv_calls = 0.0;
+    unsigned long long launches = 0;
+};
+
 struct Context {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::unique_ptr<ScanTables> tab;
+    SolveStats stats;
 };
 
 }  // namespace scatt

@@ -8,9 +8,9 @@
 //   k_init_S               A = (1 + h^2 E/6) I - h^2/6 V(n)          (SchurInverter.cpp:253-261)
 //   k_stab                 Johnson shift of A, n < 60               (SchurInverter.cpp:264-272)
 //   gemm                   S = A - Bs B^T, n < n_tr                  (SchurInverter.cpp:347-351)
-//   k_stab, k_mirror       shift of S (n < 60); S read through its lower triangle
-//                          (inverse_symmetric_indefinite, LapackInverse.hpp:120-178)
-//   gj_inverse             Sinv(n)
+//   k_stab                 shift of S (n < 60)                       (SchurInverter.cpp:364-371)
+//   gj_inverse             Sinv(n) = sym(S^-1)  (inverse_symmetric_indefinite, Eigen build,
+//                          LapackInverse.hpp:166-176)
 //   gemm x2                T = Sinv Bs, F = Bs^T T   (W^-1 = [[Sinv, -T], [-T^T, D^-1 + F]],
 //                          WInverseOperator.cpp:75-128 applied to I)
 //   k_assemble_R           R = 12 W^-1 - 10 I - Rinv_{n-1}           (ForwardRPropagator.cpp:332-334)
@@ -806,6 +806,7 @@ struct Launcher {
         if (ce.n < v.size()) SCATT_TRY(ce.alloc(v.size()));
         SCATT_CUDA_TRY(cudaMemcpyAsync(ce.p, v.data(), v.size() * sizeof(CopyEntry), cudaMemcpyHostToDevice, s));
         k_copy<<<dim3(64, (unsigned)v.size()), TPB, 0, s>>>(ce.p);
+        SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaGetLastError());
         return SCATT_CUDA_TRY_RET(cudaStreamSynchronize(s));
     }
@@ -941,6 +942,7 @@ int upload_static(Context& ctx, const scatt_scan_desc& D) {
         a.dr = D.dr; a.w = dw.p; a.chi_init = dci.p; a.dchi = ddc.p; a.chi = t.chi.p;
         a.C = t.Ctab.p; a.part = dpart.p;
         k_ctab<<<n_pts, TPB, 0, s>>>(a);
+        SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaGetLastError());
         std::vector<double> part((size_t)n_pts * t.n_occ * N_SLOTS);
         SCATT_CUDA_TRY(cudaMemcpyAsync(part.data(), dpart.p, part.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1038,8 +1040,10 @@ int make_shared(const ScanTables& t, const scatt_solve_opts& o, Batch& bt) {
 
 void launch_VB(const BatchDev& b, int n, cudaStream_t s) {
     k_build_V<<<cdiv(b.n_pairs, TPB), TPB, 0, s>>>(b, n);
+    SCATT_COUNT_LAUNCH(1);
     const int rows = std::max(b.Np_max * b.n_sigma, b.Nf);
     k_build_B<<<cdiv(rows, 128), 128, 0, s>>>(b, n);
+    SCATT_COUNT_LAUNCH(1);
 }
 
 // lambda_min(-h^2/6 V(n)) and lambda_min(-h^2/6 V(n) - Bs B^T) for n < stab_n (per Np)
@@ -1075,6 +1079,7 @@ int ensure_stab(Context& ctx, const scatt_solve_opts& o, int l_cont, const doubl
         for (int n = 0; n < ns; ++n) {
             launch_VB(bt.b, n, s);
             k_neg_hV<<<64, TPB, 0, s>>>(bt.b.V, t.Np_max, bt.b.h2_6, MA.p + (size_t)n * Np * Np, Np);
+            SCATT_COUNT_LAUNCH(1);
             SCATT_CUDA_TRY(cudaMemcpyAsync(MS.p + (size_t)n * Np * Np, MA.p + (size_t)n * Np * Np,
                                            (size_t)Np * Np * sizeof(double), cudaMemcpyDeviceToDevice, s));
             if (n < t.n_tr && t.Nf > 0) {
@@ -1219,29 +1224,55 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
 
     // ================================================================ radial sweep
     const dim3 eg(64, count);
+    const unsigned long long launches0 = launch_counter();
+    cudaEvent_t ev_begin = nullptr, ev_sweep = nullptr, ev_end = nullptr;
+    std::vector<cudaEvent_t> rev;           // sampled R^-1 inversions: pairs
+    const int sample_every = 16;
+    if (o.timing) {
+        cudaEventCreate(&ev_begin);
+        cudaEventCreate(&ev_sweep);
+        cudaEventCreate(&ev_end);
+        cudaEventRecord(ev_begin, s);
+    }
     for (int n = 0; n <= N; ++n) {
         k_prepare<<<cdiv(count, 128), 128, 0, s>>>(b, n);
+        SCATT_COUNT_LAUNCH(1);
         launch_VB(b, n, s);
-        if (n < b.n_start) k_vdiag<<<cdiv(b.Np_max, 128), 128, 0, s>>>(b, n + 1, b.vdiag1);
+        if (n < b.n_start) { k_vdiag<<<cdiv(b.Np_max, 128), 128, 0, s>>>(b, n + 1, b.vdiag1); SCATT_COUNT_LAUNCH(1); }
         k_init_S<<<eg, TPB, 0, s>>>(b);
-        if (n < b.stab_n) k_stab<<<count, TPB, 0, s>>>(b, n, 0);
+        SCATT_COUNT_LAUNCH(1);
+        if (n < b.stab_n) { k_stab<<<count, TPB, 0, s>>>(b, n, 0); SCATT_COUNT_LAUNCH(1); }
         const bool exch = n < b.n_tr && Nf > 0;
         if (exch) SCATT_TRY(gemm_dev(bt, b.gmS, count, bt.ed, 0, 0, 1, s));
-        if (exch && n < b.stab_n) k_stab<<<count, TPB, 0, s>>>(b, n, 1);
-        if (exch) k_mirror<<<eg, TPB, 0, s>>>(b);
+        if (exch && n < b.stab_n) { k_stab<<<count, TPB, 0, s>>>(b, n, 1); SCATT_COUNT_LAUNCH(1); }
         SCATT_TRY(gj_inverse_batched(b.gjS, count, maxNp, true, s));
         k_collect<<<cdiv(count, 128), 128, 0, s>>>(b, n, 0);
+        SCATT_COUNT_LAUNCH(1);
         if (exch) {
             SCATT_TRY(gemm_dev(bt, b.gmT, count, bt.ed, 1, 0, 0, s));
             SCATT_TRY(gemm_dev(bt, b.gmF, count, bt.ed, 2, 1, 0, s));
         }
         if (n < b.n_start) {
             k_analytic_R<<<eg, TPB, 0, s>>>(b, n);
+            SCATT_COUNT_LAUNCH(1);
             k_analytic_R_diag<<<dim3(4, count), TPB, 0, s>>>(b, n);
+            SCATT_COUNT_LAUNCH(1);
         } else {
             k_assemble_R<<<eg, TPB, 0, s>>>(b, n);
+            SCATT_COUNT_LAUNCH(1);
+            const bool sample = o.timing && (n % sample_every == 0);
+            if (sample) {
+                cudaEvent_t a0, a1;
+                cudaEventCreate(&a0);
+                cudaEventCreate(&a1);
+                rev.push_back(a0);
+                rev.push_back(a1);
+                cudaEventRecord(a0, s);
+            }
             SCATT_TRY(gj_inverse_batched(b.gjR, count, maxNt, true, s));
+            if (sample) cudaEventRecord(rev.back(), s);
             k_collect<<<cdiv(count, 128), 128, 0, s>>>(b, n, 1);
+            SCATT_COUNT_LAUNCH(1);
         }
         if (n <= N - 1) {
             if (n < b.n_pts) SCATT_TRY(gemm_dev(bt, b.gmG1, count, bt.ed, 3, 0, 0, s));
@@ -1250,6 +1281,7 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         }
     }
     SCATT_CUDA_TRY(cudaGetLastError());
+    if (o.timing) cudaEventRecord(ev_sweep, s);
     SCATT_CUDA_TRY(cudaStreamSynchronize(s));
     // read back per-energy error/shift counters
     std::vector<EnergyDev> edh(count);
@@ -1328,6 +1360,7 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         SCATT_TRY(upload_vec(dnt, nt, s));
         SCATT_TRY(dnorm.alloc(2 * (size_t)count));
         k_block_norms<<<count, TPB, 0, s>>>(dRp.p, dnp.p, dnt.p, dnorm.p);
+        SCATT_COUNT_LAUNCH(1);
         std::vector<double> norms(2 * count);
         SCATT_CUDA_TRY(cudaMemcpyAsync(norms.data(), dnorm.p, norms.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
         SCATT_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1362,7 +1395,9 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         DevBuf<KmeEntry> dke;
         SCATT_TRY(upload_vec(dke, ke, s));
         k_kme_tab<<<dim3(cdiv(maxNp, 128), count), 128, 0, s>>>(dke.p, t.d_l_of_mu.p, t.dr, t.Nr);
+        SCATT_COUNT_LAUNCH(1);
         k_kme_mats<<<dim3(64, count), TPB, 0, s>>>(dke.p);
+        SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaGetLastError());
         // K = B_mat^-1 A_mat (the reference solves with partial-pivot LU)
         std::vector<CopyEntry> c4;
@@ -1386,6 +1421,7 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         SCATT_TRY(upload_vec(dko, ko, s));
         SCATT_TRY(upload_vec(dpb, pb, s));
         k_kme_final<<<dim3(64, count), TPB, 0, s>>>(dke.p, dkr.p, dko.p, dpb.p);
+        SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaGetLastError());
         SCATT_CUDA_TRY(cudaStreamSynchronize(s));
         for (int e = 0; e < count; ++e) bt.ed[e].shiftsA = coupled[e];   // reuse slot for schur flag below
@@ -1425,6 +1461,7 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         DevBuf<ZEntry> dze;
         SCATT_TRY(upload_vec(dze, ze, s));
         k_build_Z<<<dim3(64, count), TPB, 0, s>>>(dze.p);
+        SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaGetLastError());
         // d_all = G_{N-1} Z_N (+ C_N psi_N when N is inside the dipole window)
         std::vector<GemmEntry> md, mc;
@@ -1491,8 +1528,11 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         DevBuf<AaEntry> dae;
         SCATT_TRY(upload_vec(dae, ae, s));
         k_aa_tab<<<dim3(64, count), TPB, 0, s>>>(dae.p, b.n_s, nfit, t.dr);
+        SCATT_COUNT_LAUNCH(1);
         k_aa_normal<<<dim3(cdiv(maxl + 1, 64), count), 64, 0, s>>>(dae.p, nfit);
+        SCATT_COUNT_LAUNCH(1);
         k_aa_fit<<<dim3(64, count), TPB, 0, s>>>(dae.p, t.d_l_of_mu.p, nfit);
+        SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaGetLastError());
         std::vector<const double*> rp(count);
         std::vector<int> rc(count);
@@ -1504,6 +1544,7 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         SCATT_TRY(upload_vec(drc, rc, s));
         SCATT_TRY(dout.alloc(2 * (size_t)count));
         k_max_pairs<<<count, TPB, 0, s>>>(drp.p, drc.p, dout.p);
+        SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaMemcpyAsync(aared.data(), dout.p, 2 * count * sizeof(double), cudaMemcpyDeviceToHost, s));
         SCATT_CUDA_TRY(cudaStreamSynchronize(s));
         for (int e = 0; e < count; ++e) {
@@ -1542,7 +1583,9 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         SCATT_TRY(dsk.alloc(2 * (size_t)count));
         SCATT_TRY(dsa.alloc(2 * (size_t)count));
         k_sym_err<<<count, TPB, 0, s>>>(dkp.p, dnpv.p, dsk.p);
+        SCATT_COUNT_LAUNCH(1);
         k_sym_err<<<count, TPB, 0, s>>>(dap.p, dnpv.p, dsa.p);
+        SCATT_COUNT_LAUNCH(1);
         std::vector<double> sk(2 * count), sa(2 * count);
         SCATT_CUDA_TRY(cudaMemcpyAsync(sk.data(), dsk.p, sk.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
         SCATT_CUDA_TRY(cudaMemcpyAsync(sa.data(), dsa.p, sa.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1567,6 +1610,7 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         SCATT_TRY(upload_vec(dqp, qp, s));
         SCATT_TRY(upload_vec(dnp, npv, s));
         k_embed<<<dim3(64, count), TPB, 0, s>>>(dap.p, dbp.p, dqp.p, dnp.p);
+        SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaGetLastError());
         std::vector<GjEntry> gq;
         for (int e = 0; e < count; ++e) {
@@ -1584,7 +1628,9 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         DevBuf<DmeEntry> dde;
         SCATT_TRY(upload_vec(dde, de, s));
         k_dme_o<<<dim3(64, count), TPB, 0, s>>>(dde.p);
+        SCATT_COUNT_LAUNCH(1);
         k_dme_D<<<dim3(16, count), TPB, 0, s>>>(dde.p, o.orthogonalize);
+        SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaGetLastError());
         SCATT_CUDA_TRY(cudaStreamSynchronize(s));
     }
@@ -1614,6 +1660,31 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
             SCATT_CUDA_TRY(cudaMemcpy(eiga[e].data(), P[e].eigA, Np * sizeof(double), cudaMemcpyDeviceToHost));
         }
     }
+
+    if (o.timing) {
+        cudaEventRecord(ev_end, s);
+        cudaEventSynchronize(ev_end);
+        float ms_all = 0.f, ms_sweep = 0.f;
+        cudaEventElapsedTime(&ms_all, ev_begin, ev_end);
+        cudaEventElapsedTime(&ms_sweep, ev_begin, ev_sweep);
+        double rs = 0.0;
+        for (size_t i = 0; i + 1 < rev.size(); i += 2) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, rev[i], rev[i + 1]);
+            rs += ms * 1e-3;
+            cudaEventDestroy(rev[i]);
+            cudaEventDestroy(rev[i + 1]);
+        }
+        ctx.stats.device_s += ms_all * 1e-3;
+        ctx.stats.sweep_s += ms_sweep * 1e-3;
+        ctx.stats.post_s += (ms_all - ms_sweep) * 1e-3;
+        ctx.stats.rinv_s += rs;
+        ctx.stats.rinv_calls += rev.size() / 2;
+        cudaEventDestroy(ev_begin);
+        cudaEventDestroy(ev_sweep);
+        cudaEventDestroy(ev_end);
+    }
+    ctx.stats.launches += launch_counter() - launches0;
 
     // ================================================================ outputs
     const int Npm = t.Np_max;
@@ -1739,6 +1810,19 @@ void scatt_default_opts(scatt_solve_opts* o) {
     o->max_batch = 0;
     o->use_graphs = 0;
     o->diagnostics = 1;
+    o->timing = 0;
+}
+
+int scatt_last_stats(scatt_ctx* ctx, double* out6) {
+    if (!ctx || !out6) return SCATT_ERR_ARG;
+    const SolveStats& st = ctx->c.stats;
+    out6[0] = st.device_s;
+    out6[1] = st.rinv_s;
+    out6[2] = st.rinv_calls;
+    out6[3] = (double)st.launches;
+    out6[4] = st.sweep_s;
+    out6[5] = st.post_s;
+    return SCATT_OK;
 }
 
 int scatt_ctx_create(int device, scatt_ctx** out) {
@@ -1826,6 +1910,7 @@ int scatt_solve_batch(scatt_ctx* ctx, int n_energy, const double* energies, cons
         }
     }
     bmax = std::max(1, bmax);
+    ctx->c.stats = SolveStats{};
     int first_err = SCATT_OK;
     std::string first_msg;
     for (int e0 = 0; e0 < n_energy; e0 += bmax) {

@@ -37,7 +37,8 @@ class ScanDesc(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("W_min", C.c_double), ("stab_n_max", C.c_int), ("shift_margin", C.c_double),
                 ("n_asym", C.c_int), ("allow_closed_channels", C.c_int), ("orthogonalize", C.c_int),
-                ("max_batch", C.c_int), ("use_graphs", C.c_int), ("diagnostics", C.c_int)]
+                ("max_batch", C.c_int), ("use_graphs", C.c_int), ("diagnostics", C.c_int),
+                ("timing", C.c_int)]
 
 
 class Outputs(C.Structure):
@@ -61,6 +62,7 @@ def _bind():
     L.scatt_solve_batch.argtypes = [C.c_void_p, C.c_int, dptr, iptr, C.POINTER(SolveOpts), C.POINTER(Outputs)]
     L.scatt_default_opts.argtypes = [C.POINTER(SolveOpts)]
     L.scatt_default_opts.restype = None
+    L.scatt_last_stats.argtypes = [C.c_void_p, dptr]
     _bound = True
 
 
@@ -136,6 +138,13 @@ class ScanSolver:
             self.close()
         except Exception:
             pass
+
+    def last_stats(self) -> dict:
+        """Device timing of the last solve (needs opts.timing = 1)."""
+        v = np.zeros(6)
+        check(lib().scatt_last_stats(self._ctx, as_dptr(v)))
+        return {"device_s": v[0], "rinv_s": v[1], "rinv_calls": int(v[2]), "launches": int(v[3]),
+                "sweep_s": v[4], "post_s": v[5]}
 
     def solve(self, energies, l_cont=None, opts: SolveOpts | None = None, raise_on_error=True):
         E = np.ascontiguousarray(energies, dtype=np.float64).reshape(-1)

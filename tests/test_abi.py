@@ -1,0 +1,45 @@
+"""The C-ABI library loads on a CPU host and exports every declared symbol."""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+from scatt_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    txt = open(os.path.join(ROOT, "include", "scatt_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?(?:int|double|void|char)\s*\**\s*(scatt_\w+)\s*\(", txt, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_the_boundary():
+    names = declared_functions()
+    for n in ("scatt_ctx_create", "scatt_upload_static", "scatt_solve_batch", "scatt_inverse_batched",
+              "scatt_dgemm", "scatt_gaunt_real", "scatt_riccati_j"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_version_and_device_count_without_gpu():
+    assert b"sm_100a" in _lib.lib().scatt_version()
+    assert _lib.device_count() >= 0
+
+
+def test_compute_entry_points_fail_loudly_without_device():
+    if _lib.device_count() > 0:
+        return
+    A = np.eye(3)[None]
+    code = _lib.lib().scatt_inverse_batched(3, 1, _lib.as_dptr(np.ascontiguousarray(A)),
+                                            _lib.as_dptr(np.zeros_like(A)), 0, None)
+    assert code == 7          # SCATT_ERR_NO_DEVICE: no CPU fallback
+    assert b"no CUDA device" in _lib.lib().scatt_last_error()

@@ -1,0 +1,140 @@
+"""CUDA solver vs the CPU oracle, per observable, through the C ABI.
+
+Tolerance per observable: max(1e-10, 10 x floor), where floor is how far the
+oracle itself moves between the reference's two LAPACK builds (Eigen
+partialPivLu vs MKL dgetri / dsytrf+dsytri) on the same inputs -- the
+rounding floor of the ill-conditioned Numerov recurrence.  Both numbers are
+reported on failure.  Dipoles (D, D_raw, d_raw, partial sigma) are checked at
+1e-10 flat.
+"""
+import numpy as np
+import pytest
+
+from oracle import solver as O
+from scatt_b200 import solver as S
+from scatt_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def oracle_pair(st, E):
+    O.BUILD = "eigen"
+    r = O.solve_energy(st, E)
+    O.BUILD = "mkl"
+    r2 = O.solve_energy(st, E)
+    O.BUILD = "eigen"
+    return r, r2
+
+
+def compare(g, r, r2, tag):
+    """K_kme, A, B, K_aa and the overlaps all derive from one boundary value
+    psi_N = J + Y K, so they share one floor: the largest build-to-build
+    spread among them."""
+    fails = []
+    coupled = max(rel(r2.K_kme, r.K_kme), rel(r2.aa["A"], r.aa["A"]), rel(r2.aa["B"], r.aa["B"]),
+                  rel(r2.aa["K"], r.aa["K"]), rel(r2.b_overlap, r.b_overlap))
+
+    def chk(name, got, ref, alt, flat=False):
+        err = rel(got, ref)
+        floor = rel(alt, ref) if flat else max(rel(alt, ref), coupled)
+        tol = 1e-10 if flat else max(1e-10, 10.0 * floor)
+        if not err <= tol:
+            fails.append(f"{tag} {name}: err {err:.3e} floor {floor:.3e} tol {tol:.1e}")
+
+    chk("K_kme", g.K_kme, r.K_kme, r2.K_kme)
+    chk("A", g.A, r.aa["A"], r2.aa["A"])
+    chk("B", g.B, r.aa["B"], r2.aa["B"])
+    chk("K_aa", g.K_aa, r.aa["K"], r2.aa["K"])
+    chk("b_overlap", g.b_overlap, r.b_overlap, r2.b_overlap)
+    for s in range(6):
+        chk(f"D[{s}]", g.D[s], r.slices[s]["D"], r2.slices[s]["D"], flat=True)
+        chk(f"D_raw[{s}]", g.D_raw[s], r.slices[s]["D_raw"], r2.slices[s]["D_raw"], flat=True)
+        chk(f"d_raw[{s}]", g.d_raw[s], r.slices[s]["d_raw"], r2.slices[s]["d_raw"], flat=True)
+        chk(f"d_corr[{s}]", g.d_corr[s], r.slices[s]["d_corr"], r2.slices[s]["d_corr"], flat=True)
+        chk(f"sigma[{s}]", g.partial_sigma[s], r.slices[s]["partial_sigma"], r2.slices[s]["partial_sigma"], flat=True)
+    chk("eigenphases_kme", np.sort(g.eig_kme), np.sort(r.kme["eigenphases"]), np.sort(r2.kme["eigenphases"]))
+    assert abs(g.diag["fit_residual_rel"] - r.aa["fit_residual_rel"]) <= 1e-6 * max(r.aa["fit_residual_rel"], 1e-12)
+    assert g.diag["shifts_A"] == r.shifts["A"] and g.diag["shifts_S"] == r.shifts["S"]
+    assert g.diag["n_fit_start"] == r.aa["n_fit_start"] and g.diag["n_fit_end"] == r.aa["n_fit_end"]
+    return fails
+
+
+CASES = {
+    "h2_l2": lambda: synth.h2_like(Nr=801, dr=0.05, l_cont=2),
+    "h2_l4": lambda: synth.h2_like(Nr=801, dr=0.05, l_cont=4),
+    "h2o_l3": lambda: synth.h2o_like(Nr=601, dr=0.05, l_cont=3, lmax_orb=6, n_orb=3),
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_solver_matches_oracle(case):
+    inp = CASES[case]()
+    st = O.make_setup(inp)
+    sol = S.ScanSolver(inp)
+    assert sol.n_transition == st.n_tr
+    Es = [0.125, 0.5, 1.2]
+    got = sol.solve(Es, opts=S.default_opts(allow_closed_channels=1))
+    fails = []
+    for E, g in zip(Es, got):
+        assert g.status == 0
+        r, r2 = oracle_pair(st, E)
+        fails += compare(g, r, r2, f"{case} E={E}")
+    assert not fails, "\n".join(fails)
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_polarisation_potential(form):
+    inp = synth.h2_like(Nr=601, dr=0.05, l_cont=3)
+    inp.alpha_pol, inp.pol_form, inp.r_c = 9.6, form, 1.5
+    st = O.make_setup(inp)
+    sol = S.ScanSolver(inp)
+    g = sol.solve([0.7], opts=S.default_opts(allow_closed_channels=1))[0]
+    r, r2 = oracle_pair(st, 0.7)
+    fails = compare(g, r, r2, f"pol{form}")
+    assert not fails, "\n".join(fails)
+
+
+def test_mixed_l_cont_batch():
+    """Energies with different continuum cutoffs in one batch (shared exchange cutoff)."""
+    inp = synth.h2o_like(Nr=301, dr=0.05, l_cont=11, lmax_orb=8, n_orb=2)
+    sol = S.ScanSolver(inp)
+    Es, lcs = [0.4, 0.9, 0.6], [10, 11, 11]
+    got = sol.solve(Es, l_cont=lcs, opts=S.default_opts(allow_closed_channels=1))
+    fails = []
+    for E, lc, g in zip(Es, lcs, got):
+        st = O.make_setup(inp, l_cont=lc)
+        r, r2 = oracle_pair(st, E)
+        fails += compare(g, r, r2, f"mixed l={lc} E={E}")
+    assert not fails, "\n".join(fails)
+
+
+def test_closed_channels_policy():
+    """k r_max < l: the determinant test marks l closed (AsymptoticAmplitudes.cpp:161-212)."""
+    inp = synth.h2_like(Nr=401, dr=0.05, l_cont=4)
+    sol = S.ScanSolver(inp)
+    E = 0.5 * 0.08 ** 2
+    res = sol.solve([E], opts=S.default_opts(allow_closed_channels=0), raise_on_error=False)[0]
+    assert res.status == 6                                  # SCATT_ERR_CLOSED_CHANNEL
+    res = sol.solve([E], opts=S.default_opts(allow_closed_channels=1))[0]
+    st = O.make_setup(inp)
+    r = O.solve_energy(st, E)
+    assert res.diag["n_closed_l"] == len(r.aa["closed_l"]) > 0
+    mu_closed = [mu for mu in range(st.n_mu) if int(st.l_mu[mu]) in r.aa["closed_l"]]
+    assert np.all(res.A[mu_closed, :] == np.eye(st.n_mu)[mu_closed, :])
+    assert np.all(res.B[mu_closed, :] == 0.0)
+
+
+def test_batch_equals_single_energy_runs():
+    inp = synth.h2_like(Nr=401, dr=0.05, l_cont=3)
+    sol = S.ScanSolver(inp)
+    Es = [0.3, 0.8, 1.5, 2.0]
+    batch = sol.solve(Es, opts=S.default_opts(allow_closed_channels=1))
+    for E, b in zip(Es, batch):
+        one = sol.solve([E], opts=S.default_opts(allow_closed_channels=1, max_batch=1))[0]
+        assert rel(one.K_kme, b.K_kme) < 1e-13
+        assert rel(one.D, b.D) < 1e-13
