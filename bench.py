@@ -213,8 +213,9 @@ def main():
     t0 = time.time()
     sol = S.ScanSolver(inp, device=local)
     setup_s = time.time() - t0
-    # this rank's contiguous block of the k grid
-    blocks = np.array_split(np.arange(len(ks)), ws)
+    # this rank's contiguous block of the k grid (cost-balanced; one l_cont here)
+    from scatt_b200 import shard
+    blocks = shard.partition(shard.energy_cost(np.full(len(ks), cfg["kw"]["l_cont"]), sol.Nf), ws)
     mine = ks[blocks[rank]]
     Es_all = 0.5 * mine ** 2
 

@@ -71,6 +71,10 @@ int scatt_dgemm(int opA, int opB, int M, int N, int K, double alpha,
  * matrices (CUDA events around the kernels only); used by the tile autotuner
  * and the benchmark. */
 int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call);
+/* Blocking scheme of scatt_inverse_batched / scatt_bench_inverse: 1 = two-level
+ * (64-column windows, rank-64 trailing updates; default), 0 = single-level
+ * (rank-16 updates).  Both give the same inverse up to rounding. */
+int scatt_set_inverse_blocking(int two_level);
 
 /* ------------------------------------------------------ per-scan solver
  * The reference runs one energy at a time through run_one_energy

@@ -15,6 +15,8 @@ namespace scatt {
 namespace {
 thread_local std::string g_last_error;
 }
+// 1: every dense inverse uses the single-level (16-column) scheme
+int g_single_level = 0;
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
@@ -88,24 +90,28 @@ int scatt_inverse_batched(int n, int count, const double* A, double* out, int sy
     }
     SCATT_TRY(require_device());
     const size_t nn = (size_t)n * n;
-    DevBuf<double> dA, dW, dO;
-    DevBuf<int> dsig, drid, dst;
+    DevBuf<double> dA, dW, dO, dP;
+    DevBuf<int> dsig, drid, dst, dsg;
     SCATT_TRY(dA.alloc(nn * count));
     SCATT_TRY(dW.alloc(nn * count));
     SCATT_TRY(dO.alloc(nn * count));
+    SCATT_TRY(dP.alloc((size_t)2 * n * 64 * count));
     SCATT_TRY(dsig.alloc((size_t)n * count));
     SCATT_TRY(drid.alloc((size_t)n * count));
+    SCATT_TRY(dsg.alloc((size_t)2 * n * count));
     SCATT_TRY(dst.alloc(2 * (size_t)count));
     SCATT_CUDA_TRY(cudaMemcpy(dA.p, A, nn * count * sizeof(double), cudaMemcpyHostToDevice));
     SCATT_CUDA_TRY(cudaMemset(dst.p, 0, 2 * count * sizeof(int)));
     std::vector<GjEntry> ent(count);
     for (int b = 0; b < count; ++b) {
         ent[b] = GjEntry{dA.p + nn * b, dW.p + nn * b, dO.p + nn * b, dsig.p + (size_t)n * b,
-                         drid.p + (size_t)n * b, dst.p + 2 * b, n, n, n};
+                         drid.p + (size_t)n * b, dst.p + 2 * b, n, n, n,
+                         dP.p + (size_t)2 * n * 64 * b, dsg.p + (size_t)2 * n * b};
     }
     DevBuf<GjEntry> dent;
     SCATT_TRY(dent.upload(ent));
-    SCATT_TRY(gj_inverse_batched(dent.p, count, n, symmetrize != 0, 0));
+    if (g_single_level) SCATT_TRY(gj_inverse_batched(dent.p, count, n, symmetrize != 0, 0));
+    else SCATT_TRY(gj_inverse_batched2(dent.p, count, n, symmetrize != 0, 0));
     SCATT_CUDA_TRY(cudaDeviceSynchronize());
     SCATT_CUDA_TRY(cudaMemcpy(out, dO.p, nn * count * sizeof(double), cudaMemcpyDeviceToHost));
     std::vector<int> st(2 * count);
@@ -152,12 +158,19 @@ int scatt_dgemm(int opA, int opB, int M, int N, int K, double alpha, const doubl
 }
 
 
+int scatt_set_inverse_blocking(int two_level) {
+    g_single_level = two_level ? 0 : 1;
+    return SCATT_OK;
+}
+
 int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call) {
     if (n <= 0 || count <= 0 || reps <= 0 || !ms_per_call) return SCATT_ERR_ARG;
     SCATT_TRY(require_device());
     const size_t nn = (size_t)n * n;
-    DevBuf<double> dA, dW, dO, dS;
-    DevBuf<int> dsig, drid, dst;
+    DevBuf<double> dA, dW, dO, dS, dP;
+    DevBuf<int> dsig, drid, dst, dsg;
+    SCATT_TRY(dP.alloc((size_t)2 * n * 64 * count));
+    SCATT_TRY(dsg.alloc((size_t)2 * n * count));
     SCATT_TRY(dA.alloc(nn * count));
     SCATT_TRY(dS.alloc(nn * count));
     SCATT_TRY(dW.alloc(nn * count));
@@ -169,7 +182,8 @@ int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call) {
     std::vector<GjEntry> ent(count);
     for (int b = 0; b < count; ++b)
         ent[b] = GjEntry{dA.p + nn * b, dW.p + nn * b, dO.p + nn * b, dsig.p + (size_t)n * b,
-                         drid.p + (size_t)n * b, dst.p + 2 * b, n, n, n};
+                         drid.p + (size_t)n * b, dst.p + 2 * b, n, n, n,
+                         dP.p + (size_t)2 * n * 64 * b, dsg.p + (size_t)2 * n * b};
     DevBuf<GjEntry> dent;
     SCATT_TRY(dent.upload(ent));
     cudaEvent_t e0, e1;
@@ -179,7 +193,8 @@ int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call) {
     for (int r = 0; r < reps + 1; ++r) {
         SCATT_CUDA_TRY(cudaMemcpyAsync(dA.p, dS.p, nn * count * sizeof(double), cudaMemcpyDeviceToDevice));
         cudaEventRecord(e0);
-        SCATT_TRY(gj_inverse_batched(dent.p, count, n, true, 0));
+        if (g_single_level) SCATT_TRY(gj_inverse_batched(dent.p, count, n, true, 0));
+        else SCATT_TRY(gj_inverse_batched2(dent.p, count, n, true, 0));
         cudaEventRecord(e1);
         SCATT_CUDA_TRY(cudaEventSynchronize(e1));
         float ms = 0.f;

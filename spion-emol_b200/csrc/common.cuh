@@ -81,6 +81,8 @@ struct GjEntry {
     int*    rowid;    // n ints: original row index at each position
     int*    status;   // 1 int: DeviceStatus (first failing column in status[1])
     int n, ld, ldo;
+    double* P = nullptr;   // optional 2 x (ld x 64) panel-window buffers (two-level blocking)
+    int*    sigt = nullptr; // optional 2 x n composite row maps of the 64-column window
 };
 
 constexpr int GJ_NB = 16;
@@ -92,5 +94,20 @@ int gj_max_order();
 // is a DEVICE array; `symmetrize` writes 0.5 * (X + X^T) into `out`.
 int gj_inverse_batched(const GjEntry* entries_dev, int count, int nmax,
                        bool symmetrize, cudaStream_t stream);
+
+// Two-level blocked variant (64-column windows, rank-64 trailing updates) for
+// n <= 1280; every entry must carry P (2 x ld x 64 doubles) and sigt (2 n ints).
+int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax,
+                        bool symmetrize, cudaStream_t stream);
+
+// 1: every dense inverse (entry points and solver) uses the single-level scheme
+extern int g_single_level;
+
+// The scheme selected by g_single_level (entries must carry P and sigt).
+inline int gj_inverse_selected(const GjEntry* entries_dev, int count, int nmax,
+                               bool symmetrize, cudaStream_t stream) {
+    return g_single_level ? gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream)
+                          : gj_inverse_batched2(entries_dev, count, nmax, symmetrize, stream);
+}
 
 }  // namespace scatt

@@ -467,6 +467,296 @@ gj_panel3_kernel(const GjEntry* __restrict__ entries, int kb) {
     if (tid == 0) e.status[0] = s_status;
 }
 
+// Panel v4: W warps (32 W threads, W = ceil(n / 128)), each thread owns up
+// to R = 4 rows tid + 32 W r with all 16 panel columns in registers.  The
+// pivot loop is fully unrolled, so every register index is static; the
+// owner of the pivot row publishes it already scaled by 1/pivot.
+template <int R, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1)
+gj_panel4_kernel(const GjEntry* __restrict__ entries, int kb) {
+    const GjEntry e = entries[blockIdx.x];
+    const int n = e.n;
+    const int k0 = kb * NB;
+    if (k0 >= n) return;
+    const int nb = min(NB, n - k0);
+    const double* src = buf_of(e, kb & 1);
+    double* dst = buf_of(e, (kb + 1) & 1);
+    const int T = blockDim.x, W = T >> 5;
+
+    extern __shared__ double smem[];
+    int* loc = reinterpret_cast<int*>(smem);
+    int* rid = loc + n;
+    __shared__ double red_v[2][32];
+    __shared__ int red_i[2][32];
+    __shared__ double sprow[2][NB];      // new pivot row: row p scaled by 1/pivot
+    __shared__ double krow[2][NB];       // row k before the interchange
+    __shared__ int s_status;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double v[R][NB];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = tid + r * T;
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+            v[r][j] = (i < n && j < nb) ? src[i + (size_t)(k0 + j) * e.ld] : 0.0;
+    }
+    for (int i = tid; i < n; i += T) {
+        loc[i] = i;
+        rid[i] = (kb == 0) ? i : e.rowid[i];
+    }
+    if (tid == 0) s_status = (kb == 0) ? 0 : e.status[0];
+    __syncthreads();
+
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        if (j < nb) {
+            const int k = k0 + j;
+            const int par = j & 1;
+            double bv = -1.0;
+            int bi = -1;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = tid + r * T;
+                if (i >= k && i < n) {
+                    const double a = fabs(v[r][j]);
+                    if (a > bv) { bv = a; bi = i; }
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                better_key(bv, bi, ov, oi);
+            }
+            if (lane == 0) { red_v[par][warp] = bv; red_i[par][warp] = bi; }
+            __syncthreads();
+            bv = (lane < W) ? red_v[par][lane] : -1.0;
+            bi = (lane < W) ? red_i[par][lane] : -1;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                better_key(bv, bi, ov, oi);
+            }
+            const int p = bi < 0 ? k : bi;
+            if (tid == 0) {
+                int st = 0;
+                if (bi < 0 || !(bv < INFINITY)) st = DEV_NONFINITE;
+                else if (bv == 0.0) st = DEV_SINGULAR;
+                if (st && s_status == 0) { s_status = st; e.status[1] = k; }
+                if (p != k) {
+                    const int a = loc[k]; loc[k] = loc[p]; loc[p] = a;
+                    const int b2 = rid[k]; rid[k] = rid[p]; rid[p] = b2;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = tid + r * T;
+                if (i == p) {
+                    double piv = v[r][j];
+                    if (piv == 0.0) piv = 1.0;      // the status word records the failure
+                    const double inv = 1.0 / piv;
+#pragma unroll
+                    for (int c = 0; c < NB; ++c) sprow[par][c] = (c == j) ? inv : v[r][c] * inv;
+                }
+                if (i == k) {
+#pragma unroll
+                    for (int c = 0; c < NB; ++c) krow[par][c] = v[r][c];
+                }
+            }
+            __syncthreads();
+            const double inv = sprow[par][j];
+            const double* sp = sprow[par];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = tid + r * T;
+                if (i < n) {
+                    if (i == k) {
+#pragma unroll
+                        for (int c = 0; c < NB; ++c) v[r][c] = sp[c];
+                    } else {
+                        if (i == p) {
+#pragma unroll
+                            for (int c = 0; c < NB; ++c) v[r][c] = krow[par][c];
+                        }
+                        const double f = v[r][j];
+#pragma unroll
+                        for (int c = 0; c < NB; ++c) {
+                            if (c == j) v[r][c] = -f * inv;
+                            else v[r][c] -= f * sp[c];
+                        }
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = tid + r * T;
+        if (i < n) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+                if (j < nb) dst[i + (size_t)(k0 + j) * e.ld] = v[r][j];
+        }
+    }
+    for (int i = tid; i < n; i += T) {
+        e.sigma[i] = loc[i];
+        e.rowid[i] = rid[i];
+    }
+    if (tid == 0) e.status[0] = s_status;
+}
+
+// Panel v5: as v4 (W warps, R rows of 16 columns per thread in registers)
+// but with a rolled pivot loop: after each pivot the register window is
+// rotated by one column, so the active column is always v[r][0] and every
+// index stays static while the loop body stays small (instruction-cache
+// resident).  Shared rows (scaled pivot row, old row k) are kept in the same
+// rotated order; 16 rotations restore the original order.
+template <int R, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1)
+gj_panel5_kernel(const GjEntry* __restrict__ entries, int kb) {
+    const GjEntry e = entries[blockIdx.x];
+    const int n = e.n;
+    const int k0 = kb * NB;
+    if (k0 >= n) return;
+    const int nb = min(NB, n - k0);
+    const double* src = buf_of(e, kb & 1);
+    double* dst = buf_of(e, (kb + 1) & 1);
+    const int T = blockDim.x, W = T >> 5;
+
+    extern __shared__ double smem[];
+    int* loc = reinterpret_cast<int*>(smem);
+    int* rid = loc + n;
+    __shared__ double red_v[2][32];
+    __shared__ int red_i[2][32];
+    __shared__ double sprow[2][NB];
+    __shared__ double krow[2][NB];
+    __shared__ int s_status;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double v[R][NB];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = tid + r * T;
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+            v[r][j] = (i < n && j < nb) ? src[i + (size_t)(k0 + j) * e.ld] : 0.0;
+    }
+    for (int i = tid; i < n; i += T) {
+        loc[i] = i;
+        rid[i] = (kb == 0) ? i : e.rowid[i];
+    }
+    if (tid == 0) s_status = (kb == 0) ? 0 : e.status[0];
+    __syncthreads();
+
+#pragma unroll 1
+    for (int j = 0; j < NB; ++j) {
+        if (j < nb) {
+            const int k = k0 + j;
+            const int par = j & 1;
+            double bv = -1.0;
+            int bi = -1;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = tid + r * T;
+                if (i >= k && i < n) {
+                    const double a = fabs(v[r][0]);
+                    if (a > bv) { bv = a; bi = i; }
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                better_key(bv, bi, ov, oi);
+            }
+            if (lane == 0) { red_v[par][warp] = bv; red_i[par][warp] = bi; }
+            __syncthreads();
+            bv = (lane < W) ? red_v[par][lane] : -1.0;
+            bi = (lane < W) ? red_i[par][lane] : -1;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                better_key(bv, bi, ov, oi);
+            }
+            const int p = bi < 0 ? k : bi;
+            if (tid == 0) {
+                int st = 0;
+                if (bi < 0 || !(bv < INFINITY)) st = DEV_NONFINITE;
+                else if (bv == 0.0) st = DEV_SINGULAR;
+                if (st && s_status == 0) { s_status = st; e.status[1] = k; }
+                if (p != k) {
+                    const int a = loc[k]; loc[k] = loc[p]; loc[p] = a;
+                    const int b2 = rid[k]; rid[k] = rid[p]; rid[p] = b2;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = tid + r * T;
+                if (i == p) {
+                    double piv = v[r][0];
+                    if (piv == 0.0) piv = 1.0;      // the status word records the failure
+                    const double inv = 1.0 / piv;
+                    sprow[par][0] = inv;
+#pragma unroll
+                    for (int c = 1; c < NB; ++c) sprow[par][c] = v[r][c] * inv;
+                }
+                if (i == k) {
+#pragma unroll
+                    for (int c = 0; c < NB; ++c) krow[par][c] = v[r][c];
+                }
+            }
+            __syncthreads();
+            const double inv = sprow[par][0];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = tid + r * T;
+                if (i < n) {
+                    if (i == k) {
+#pragma unroll
+                        for (int c = 0; c < NB; ++c) v[r][c] = sprow[par][c];
+                    } else {
+                        if (i == p) {
+#pragma unroll
+                            for (int c = 0; c < NB; ++c) v[r][c] = krow[par][c];
+                        }
+                        const double f = v[r][0];
+                        v[r][0] = -f * inv;
+#pragma unroll
+                        for (int c = 1; c < NB; ++c) v[r][c] -= f * sprow[par][c];
+                    }
+                }
+            }
+        }
+        // rotate the window: column j moves to the back, column j + 1 to the front
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const double t0 = v[r][0];
+#pragma unroll
+            for (int c = 0; c < NB - 1; ++c) v[r][c] = v[r][c + 1];
+            v[r][NB - 1] = t0;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = tid + r * T;
+        if (i < n) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+                if (j < nb) dst[i + (size_t)(k0 + j) * e.ld] = v[r][j];
+        }
+    }
+    for (int i = tid; i < n; i += T) {
+        e.sigma[i] = loc[i];
+        e.rowid[i] = rid[i];
+    }
+    if (tid == 0) e.status[0] = s_status;
+}
+
 constexpr int UBM = 64, UBN = 64, UPAD = 4, UTHREADS = 128;
 
 __device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1, double b0) {
@@ -588,17 +878,516 @@ gj_update2_kernel(const GjEntry* __restrict__ entries, int kb) {
     }
 }
 
+// asynchronous 8-byte global -> shared copy (zero-fill when !pred)
+__device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc, bool pred) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(sdst));
+    const int sz = pred ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" :: "r"(sa), "l"(gsrc), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// ======================================================================
+// Two-level blocking.  Outer block of 64 columns (K = [k0, k0 + 64)):
+//   4 x { panel on 16 columns of the 64-column window (gj2_panel),
+//         rank-16 update of the other window columns (gj2_narrow) }
+//   then one rank-64 update of every column outside the window (gj2_trail):
+//   new[i, c] = (i in K ? 0 : old[st(i), c]) + sum_{j<64} M64[i, j] old[st(k0 + j), c]
+//   with M64 the transformed window and st the composite row map of the
+//   four sub-steps.  The window lives in two n x 64 buffers (P), so the
+//   sub-steps never touch the rest of the matrix.
+constexpr int OB = 64;
+
+__device__ __forceinline__ const double* win_in(const GjEntry& e, int K, int s) {
+    return (s == 0) ? buf_of(e, K & 1) + (size_t)(K * OB) * e.ld : e.P + (size_t)(s & 1) * e.ld * OB;
+}
+__device__ __forceinline__ double* win_out(const GjEntry& e, int s) {
+    return e.P + (size_t)((s + 1) & 1) * e.ld * OB;
+}
+
+template <int R, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1)
+gj2_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
+    const GjEntry e = entries[blockIdx.x];
+    const int n = e.n;
+    const int k0o = K * OB;
+    if (k0o >= n) return;
+    const int nb64 = min(OB, n - k0o);
+    const int cs = sub * NB;
+    if (cs >= nb64) return;
+    const int nb = min(NB, nb64 - cs);
+    const int kr0 = k0o + cs;
+    const double* src = win_in(e, K, sub);
+    double* dst = win_out(e, sub);
+    const int T = blockDim.x, W = T >> 5;
+    const bool first = (K == 0 && sub == 0);
+
+    extern __shared__ double smem[];
+    int* loc = reinterpret_cast<int*>(smem);
+    int* rid = loc + n;
+    __shared__ double red_v[2][32];
+    __shared__ int red_i[2][32];
+    __shared__ double sprow[2][NB];
+    __shared__ double krow[2][NB];
+    __shared__ int s_status;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double v[R][NB];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = tid + r * T;
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+            v[r][j] = (i < n && j < nb) ? src[i + (size_t)(cs + j) * e.ld] : 0.0;
+    }
+    for (int i = tid; i < n; i += T) {
+        loc[i] = i;
+        rid[i] = first ? i : e.rowid[i];
+    }
+    if (tid == 0) s_status = first ? 0 : e.status[0];
+    __syncthreads();
+
+#pragma unroll 1
+    for (int j = 0; j < NB; ++j) {
+        if (j < nb) {
+            const int k = kr0 + j;
+            const int par = j & 1;
+            double bv = -1.0;
+            int bi = -1;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = tid + r * T;
+                if (i >= k && i < n) {
+                    const double a = fabs(v[r][0]);
+                    if (a > bv) { bv = a; bi = i; }
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                better_key(bv, bi, ov, oi);
+            }
+            if (lane == 0) { red_v[par][warp] = bv; red_i[par][warp] = bi; }
+            __syncthreads();
+            bv = (lane < W) ? red_v[par][lane] : -1.0;
+            bi = (lane < W) ? red_i[par][lane] : -1;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                better_key(bv, bi, ov, oi);
+            }
+            const int p = bi < 0 ? k : bi;
+            if (tid == 0) {
+                int st = 0;
+                if (bi < 0 || !(bv < INFINITY)) st = DEV_NONFINITE;
+                else if (bv == 0.0) st = DEV_SINGULAR;
+                if (st && s_status == 0) { s_status = st; e.status[1] = k; }
+                if (p != k) {
+                    const int a = loc[k]; loc[k] = loc[p]; loc[p] = a;
+                    const int b2 = rid[k]; rid[k] = rid[p]; rid[p] = b2;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = tid + r * T;
+                if (i == p) {
+                    double piv = v[r][0];
+                    if (piv == 0.0) piv = 1.0;      // the status word records the failure
+                    const double inv = 1.0 / piv;
+                    sprow[par][0] = inv;
+#pragma unroll
+                    for (int c = 1; c < NB; ++c) sprow[par][c] = v[r][c] * inv;
+                }
+                if (i == k) {
+#pragma unroll
+                    for (int c = 0; c < NB; ++c) krow[par][c] = v[r][c];
+                }
+            }
+            __syncthreads();
+            const double inv = sprow[par][0];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = tid + r * T;
+                if (i < n) {
+                    if (i == k) {
+#pragma unroll
+                        for (int c = 0; c < NB; ++c) v[r][c] = sprow[par][c];
+                    } else {
+                        if (i == p) {
+#pragma unroll
+                            for (int c = 0; c < NB; ++c) v[r][c] = krow[par][c];
+                        }
+                        const double f = v[r][0];
+                        v[r][0] = -f * inv;
+#pragma unroll
+                        for (int c = 1; c < NB; ++c) v[r][c] -= f * sprow[par][c];
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const double t0 = v[r][0];
+#pragma unroll
+            for (int c = 0; c < NB - 1; ++c) v[r][c] = v[r][c + 1];
+            v[r][NB - 1] = t0;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = tid + r * T;
+        if (i < n) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+                if (j < nb) dst[i + (size_t)(cs + j) * e.ld] = v[r][j];
+        }
+    }
+    const int* st_in = e.sigt + (size_t)(sub & 1) * n;
+    int* st_out = e.sigt + (size_t)((sub + 1) & 1) * n;
+    for (int i = tid; i < n; i += T) {
+        const int l = loc[i];
+        e.sigma[i] = l;
+        e.rowid[i] = rid[i];
+        st_out[i] = (sub == 0) ? l : st_in[l];
+    }
+    if (tid == 0) e.status[0] = s_status;
+}
+
+// rank-16 update of the other columns of the 64-column window
+__global__ void __launch_bounds__(U2T)
+gj2_narrow_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
+    const GjEntry e = entries[blockIdx.z];
+    const int n = e.n;
+    const int k0o = K * OB;
+    if (k0o >= n) return;
+    const int nb64 = min(OB, n - k0o);
+    const int cs = sub * NB;
+    if (cs >= nb64) return;
+    const int nb = min(NB, nb64 - cs);
+    const int kr0 = k0o + cs;
+    const int r0 = blockIdx.x * 64;
+    if (r0 >= n) return;
+    const double* src = win_in(e, K, sub);
+    double* dst = win_out(e, sub);
+
+    extern __shared__ double u2smem[];
+    double (*Cs)[U2S] = reinterpret_cast<double (*)[U2S]>(u2smem);
+    double (*Ms)[68] = reinterpret_cast<double (*)[68]>(u2smem + 64 * U2S);
+    double (*Xs)[68] = reinterpret_cast<double (*)[68]>(u2smem + 64 * U2S + NB * 68);
+    __shared__ int srow[64];
+    __shared__ int xrow[NB];
+    const int tid = threadIdx.x;
+    if (tid < 64) srow[tid] = (r0 + tid < n) ? e.sigma[r0 + tid] : 0;
+    else if (tid < 64 + NB) {
+        const int j = tid - 64;
+        xrow[j] = (j < nb) ? e.sigma[kr0 + j] : 0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const int idx = tid + u * U2T;
+        const int row = idx & 63, col = idx >> 6;
+        const int gi = r0 + row;
+        const bool ok = gi < n && col < nb64 && !(gi >= kr0 && gi < kr0 + nb);
+        cp_async8(&Cs[col][row], src + (ok ? srow[row] + (size_t)col * e.ld : 0), ok);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int idx = tid + u * U2T;
+        const int m = idx & 63, j = idx >> 6;
+        const int gi = r0 + m;
+        const bool okm = j < nb && gi < n;
+        cp_async8(&Ms[j][m], dst + (okm ? gi + (size_t)(cs + j) * e.ld : 0), okm);
+        const int c = idx >> 4, jj = idx & 15;
+        const bool okx = jj < nb && c < nb64;
+        cp_async8(&Xs[jj][c], src + (okx ? xrow[jj] + (size_t)c * e.ld : 0), okx);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+    double acc[2][2][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int jn = 0; jn < 2; ++jn)
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                acc[i][jn][v] = Cs[wn + jn * 8 + 2 * t + (v & 1)][wm + i * 16 + g + ((v >> 1) << 3)];
+#pragma unroll
+    for (int kk = 0; kk < NB; kk += 4) {
+        double a[2][2], b[2];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            a[i][0] = Ms[kk + t][wm + i * 16 + g];
+            a[i][1] = Ms[kk + t][wm + i * 16 + g + 8];
+        }
+#pragma unroll
+        for (int jn = 0; jn < 2; ++jn) b[jn] = Xs[kk + t][wn + jn * 8 + g];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int jn = 0; jn < 2; ++jn) dmma_16x8x4(acc[i][jn], a[i][0], a[i][1], b[jn]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int jn = 0; jn < 2; ++jn)
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                Cs[wn + jn * 8 + 2 * t + (v & 1)][wm + i * 16 + g + ((v >> 1) << 3)] = acc[i][jn][v];
+    __syncthreads();
+#pragma unroll 4
+    for (int u = 0; u < 16; ++u) {
+        const int idx = tid + u * U2T;
+        const int row = idx & 63, col = idx >> 6;
+        const int gi = r0 + row;
+        if (gi < n && col < nb64 && !(col >= cs && col < cs + nb)) dst[gi + (size_t)col * e.ld] = Cs[col][row];
+    }
+}
+
+// rank-64 update of every column outside the window; the window tile itself
+// is copied from the transformed window
+constexpr int T3S = 68;
+constexpr size_t TRAIL_SMEM = (64 * U2S + 2 * 64 * T3S) * sizeof(double);
+
+__global__ void __launch_bounds__(U2T)
+gj2_trail_kernel(const GjEntry* __restrict__ entries, int K) {
+    const GjEntry e = entries[blockIdx.z];
+    const int n = e.n;
+    const int k0 = K * OB;
+    if (k0 >= n) return;
+    const int nb64 = min(OB, n - k0);
+    const int nsub = (nb64 + NB - 1) / NB;
+    const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
+    if (r0 >= n || c0 >= n) return;
+    const double* src = buf_of(e, K & 1);
+    double* dst = buf_of(e, (K + 1) & 1);
+    const double* Mw = e.P + (size_t)(nsub & 1) * e.ld * OB;     // final window
+    const int* st = e.sigt + (size_t)(nsub & 1) * n;
+    const int tid = threadIdx.x;
+    if (c0 == k0) {          // the window itself
+        for (int idx = tid; idx < 64 * 64; idx += U2T) {
+            const int row = idx & 63, col = idx >> 6;
+            const int gi = r0 + row;
+            if (gi < n && col < nb64) dst[gi + (size_t)(c0 + col) * e.ld] = Mw[gi + (size_t)col * e.ld];
+        }
+        return;
+    }
+    extern __shared__ double u2smem[];
+    double (*Cs)[U2S] = reinterpret_cast<double (*)[U2S]>(u2smem);
+    double (*Ms)[T3S] = reinterpret_cast<double (*)[T3S]>(u2smem + 64 * U2S);          // Ms[j][m]
+    double (*Xs)[T3S] = reinterpret_cast<double (*)[T3S]>(u2smem + 64 * U2S + 64 * T3S); // Xs[j][c]
+    __shared__ int srow[64];
+    __shared__ int xrow[64];
+    if (tid < 64) srow[tid] = (r0 + tid < n) ? st[r0 + tid] : 0;
+    else if (tid < 128) {
+        const int j = tid - 64;
+        xrow[j] = (j < nb64) ? st[k0 + j] : 0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const int idx = tid + u * U2T;
+        const int row = idx & 63, col = idx >> 6;
+        const int gi = r0 + row, gc = c0 + col;
+        const bool ok = gi < n && gc < n && !(gi >= k0 && gi < k0 + nb64);
+        cp_async8(&Cs[col][row], src + (ok ? srow[row] + (size_t)gc * e.ld : 0), ok);
+    }
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const int idx = tid + u * U2T;
+        const int m = idx & 63, j = idx >> 6;
+        const int gi = r0 + m;
+        const bool ok = j < nb64 && gi < n;
+        cp_async8(&Ms[j][m], Mw + (ok ? gi + (size_t)j * e.ld : 0), ok);
+    }
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const int idx = tid + u * U2T;
+        const int j = idx & 63, c = idx >> 6;
+        const int gc = c0 + c;
+        const bool ok = j < nb64 && gc < n;
+        cp_async8(&Xs[j][c], src + (ok ? xrow[j] + (size_t)gc * e.ld : 0), ok);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+    double acc[2][2][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int jn = 0; jn < 2; ++jn)
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                acc[i][jn][v] = Cs[wn + jn * 8 + 2 * t + (v & 1)][wm + i * 16 + g + ((v >> 1) << 3)];
+#pragma unroll 4
+    for (int kk = 0; kk < OB; kk += 4) {
+        double a[2][2], b[2];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            a[i][0] = Ms[kk + t][wm + i * 16 + g];
+            a[i][1] = Ms[kk + t][wm + i * 16 + g + 8];
+        }
+#pragma unroll
+        for (int jn = 0; jn < 2; ++jn) b[jn] = Xs[kk + t][wn + jn * 8 + g];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int jn = 0; jn < 2; ++jn) dmma_16x8x4(acc[i][jn], a[i][0], a[i][1], b[jn]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int jn = 0; jn < 2; ++jn)
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                Cs[wn + jn * 8 + 2 * t + (v & 1)][wm + i * 16 + g + ((v >> 1) << 3)] = acc[i][jn][v];
+    __syncthreads();
+#pragma unroll 4
+    for (int u = 0; u < 16; ++u) {
+        const int idx = tid + u * U2T;
+        const int row = idx & 63, col = idx >> 6;
+        const int gi = r0 + row, gc = c0 + col;
+        if (gi < n && gc < n) dst[gi + (size_t)gc * e.ld] = Cs[col][row];
+    }
+}
+
+// Trailing rank-64 update, pipelined: old C rows go straight into the DMMA
+// accumulators; the 64-deep M / X operands stream through two 16-deep
+// shared-memory stages with cp.async, so loads of chunk c+1 overlap the
+// tensor-core work on chunk c.
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory"); }
+
+__global__ void __launch_bounds__(U2T, 3)
+gj2_trail2_kernel(const GjEntry* __restrict__ entries, int K) {
+    const GjEntry e = entries[blockIdx.z];
+    const int n = e.n;
+    const int k0 = K * OB;
+    if (k0 >= n) return;
+    const int nb64 = min(OB, n - k0);
+    const int nsub = (nb64 + NB - 1) / NB;
+    const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
+    if (r0 >= n || c0 >= n) return;
+    const double* src = buf_of(e, K & 1);
+    double* dst = buf_of(e, (K + 1) & 1);
+    const double* Mw = e.P + (size_t)(nsub & 1) * e.ld * OB;
+    const int* st = e.sigt + (size_t)(nsub & 1) * n;
+    const int tid = threadIdx.x;
+    if (c0 == k0) {
+        for (int idx = tid; idx < 64 * 64; idx += U2T) {
+            const int row = idx & 63, col = idx >> 6;
+            const int gi = r0 + row;
+            if (gi < n && col < nb64) dst[gi + (size_t)(c0 + col) * e.ld] = Mw[gi + (size_t)col * e.ld];
+        }
+        return;
+    }
+    __shared__ double Ms[2][NB][68];
+    __shared__ double Xs[2][NB][68];
+    __shared__ int srow[64];
+    __shared__ int xrow[64];
+    if (tid < 64) srow[tid] = (r0 + tid < n) ? st[r0 + tid] : 0;
+    else if (tid < 128) {
+        const int j = tid - 64;
+        xrow[j] = (j < nb64) ? st[k0 + j] : 0;
+    }
+    __syncthreads();
+    auto load_chunk = [&](int ch, int buf) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int idx = tid + u * U2T;          // 0..1023
+            const int m = idx & 63, jj = idx >> 6;  // Ms[jj][m]
+            const int j = ch * NB + jj;
+            const int gi = r0 + m;
+            const bool okm = j < nb64 && gi < n;
+            cp_async8(&Ms[buf][jj][m], Mw + (okm ? gi + (size_t)j * e.ld : 0), okm);
+            const int c = idx >> 4, jx = idx & 15;  // Xs[jx][c]
+            const int jg = ch * NB + jx;
+            const int gc = c0 + c;
+            const bool okx = jg < nb64 && gc < n;
+            cp_async8(&Xs[buf][jx][c], src + (okx ? xrow[jg] + (size_t)gc * e.ld : 0), okx);
+        }
+        cp_async_commit();
+    };
+    load_chunk(0, 0);
+    const int lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+    double acc[2][2][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int jn = 0; jn < 2; ++jn)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int rl = wm + i * 16 + g + ((v >> 1) << 3);
+                const int gi = r0 + rl;
+                const int gc = c0 + wn + jn * 8 + 2 * t + (v & 1);
+                double old = 0.0;
+                if (gi < n && gc < n && !(gi >= k0 && gi < k0 + nb64)) old = src[srow[rl] + (size_t)gc * e.ld];
+                acc[i][jn][v] = old;
+            }
+    const int nch = nsub;
+    for (int ch = 0; ch < nch; ++ch) {
+        const int buf = ch & 1;
+        if (ch + 1 < nch) {
+            load_chunk(ch + 1, buf ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < NB; kk += 4) {
+            double a[2][2], b[2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                a[i][0] = Ms[buf][kk + t][wm + i * 16 + g];
+                a[i][1] = Ms[buf][kk + t][wm + i * 16 + g + 8];
+            }
+#pragma unroll
+            for (int jn = 0; jn < 2; ++jn) b[jn] = Xs[buf][kk + t][wn + jn * 8 + g];
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int jn = 0; jn < 2; ++jn) dmma_16x8x4(acc[i][jn], a[i][0], a[i][1], b[jn]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int jn = 0; jn < 2; ++jn)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int gi = r0 + wm + i * 16 + g + ((v >> 1) << 3);
+                const int gc = c0 + wn + jn * 8 + 2 * t + (v & 1);
+                if (gi < n && gc < n) dst[gi + (size_t)gc * e.ld] = acc[i][jn][v];
+            }
+}
+
 constexpr int FT = 32;
 
 __global__ void __launch_bounds__(FT * 8)
 gj_finalize_kernel(const GjEntry* __restrict__ entries, int nsteps_parity, int symmetrize) {
+    // nsteps_parity: 0 = single-level (16-column steps), 1 = two-level (64-column steps)
     const GjEntry e = entries[blockIdx.z];
     const int n = e.n;
     const int i0 = blockIdx.x * FT, j0 = blockIdx.y * FT;
     if (i0 >= n || j0 >= n) return;
     // the result of the last block step lives in buffer (number of steps of this matrix) % 2
-    const int steps = (n + NB - 1) / NB;
-    (void)nsteps_parity;
+    const int steps = nsteps_parity ? (n + OB - 1) / OB : (n + NB - 1) / NB;
     const double* X = buf_of(e, steps & 1);
 
     __shared__ int pi_i[FT], pi_j[FT];
@@ -667,23 +1456,57 @@ int gj_inverse_batched(const GjEntry* entries_dev, int count, int nmax,
     const int tiles = (nmax + UBM - 1) / UBM;
     dim3 ugrid(tiles, tiles, count);
     const size_t smem_reg = 2 * (size_t)nmax * sizeof(int);
+    // panel v4: W warps with at most 2 rows of 16 columns per thread
+    const int W4 = std::max(1, (nmax + 63) / 64);
+    const int T4 = 32 * W4;
     for (int kb = 0; kb < steps; ++kb) {
-        if (nmax <= 512)
-            gj_panel3_kernel<2, 1><<<count, P3_THREADS, smem_reg, stream>>>(entries_dev, kb);
-        else if (nmax <= 1024)
-            gj_panel3_kernel<4, 4><<<count, P3_THREADS, smem_reg, stream>>>(entries_dev, kb);
-        else if (nmax <= 1280)
-            gj_panel3_kernel<4, 5><<<count, P3_THREADS, smem_reg, stream>>>(entries_dev, kb);
-
-        else
+        if (nmax <= 512) {
+            gj_panel5_kernel<2, 256><<<count, T4, smem_reg, stream>>>(entries_dev, kb);
+        } else if (nmax <= 1280) {
+            gj_panel5_kernel<2, 640><<<count, T4, smem_reg, stream>>>(entries_dev, kb);
+        } else {
             gj_panel_kernel<<<count, PANEL_THREADS, smem, stream>>>(entries_dev, kb);
+        }
         gj_update2_kernel<<<ugrid, U2T, U2_SMEM, stream>>>(entries_dev, kb);
     }
     const int ft = (nmax + FT - 1) / FT;
-    gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, steps & 1,
-                                                                   symmetrize ? 1 : 0);
+    gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, 0, symmetrize ? 1 : 0);
     SCATT_CUDA_TRY(cudaGetLastError());
     SCATT_COUNT_LAUNCH(2 * steps + 1);
+    return SCATT_OK;
+}
+
+int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax, bool symmetrize,
+                        cudaStream_t stream) {
+    if (count <= 0 || nmax <= 0) return SCATT_OK;
+    if (nmax > 1280) return gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream);
+    static bool attr2 = false;
+    if (!attr2) {
+        SCATT_CUDA_TRY(cudaFuncSetAttribute(gj2_narrow_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)U2_SMEM));
+        SCATT_CUDA_TRY(cudaFuncSetAttribute(gj2_trail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)TRAIL_SMEM));
+        attr2 = true;
+    }
+    const int outer = (nmax + OB - 1) / OB;
+    const int tiles = (nmax + 63) / 64;
+    const size_t smem_reg = 2 * (size_t)nmax * sizeof(int);
+    const int T4 = 32 * std::max(1, (nmax + 63) / 64);
+    int launches = 0;
+    for (int K = 0; K < outer; ++K) {
+        for (int sub = 0; sub < OB / NB; ++sub) {
+            if (nmax <= 512) gj2_panel_kernel<2, 256><<<count, T4, smem_reg, stream>>>(entries_dev, K, sub);
+            else gj2_panel_kernel<2, 640><<<count, T4, smem_reg, stream>>>(entries_dev, K, sub);
+            gj2_narrow_kernel<<<dim3(tiles, 1, count), U2T, U2_SMEM, stream>>>(entries_dev, K, sub);
+            launches += 2;
+        }
+        gj2_trail2_kernel<<<dim3(tiles, tiles, count), U2T, 0, stream>>>(entries_dev, K);
+        ++launches;
+    }
+    const int ft = (nmax + FT - 1) / FT;
+    gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, 1, symmetrize ? 1 : 0);
+    SCATT_CUDA_TRY(cudaGetLastError());
+    SCATT_COUNT_LAUNCH(launches + 1);
     return SCATT_OK;
 }
 

@@ -171,8 +171,8 @@ __global__ void k_prepare(BatchDev b, int n) {
     b.gmG1[e] = GemmEntry{Cn, sinv, gcur, K, Np, Np, K, Np, K, 1.0, 1.0};
     b.gmG2[e] = GemmEntry{Cn, d.T, gcur + (size_t)Np * K, K, Nf, Np, K, Np, K, -1.0, 1.0};
     b.gmG3[e] = GemmEntry{gcur, rinv, gnext, K, Nt, Nt, K, Nt, K, 1.0, 0.0};
-    b.gjS[e] = GjEntry{d.S, d.Sw, sinv, d.sigS, d.ridS, d.stS, Np, Np, Np};
-    b.gjR[e] = GjEntry{d.Ra, d.Rw, rinv, d.sigR, d.ridR, d.stR, Nt, Nt, Nt};
+    b.gjS[e] = GjEntry{d.S, d.Sw, sinv, d.sigS, d.ridS, d.stS, Np, Np, Np, d.PS, d.sgS};
+    b.gjR[e] = GjEntry{d.Ra, d.Rw, rinv, d.sigR, d.ridR, d.stR, Nt, Nt, Nt, d.PR, d.sgR};
 }
 
 // A = (1 + h^2 E / 6) I - h^2/6 V(n)  into S (SchurInverter.cpp:253-261)
@@ -1116,6 +1116,7 @@ size_t energy_bytes(const BatchDev& b, int Np, int Nt, int nslots) {
     const size_t np2 = (size_t)Np * Np, nt2 = (size_t)Nt * Nt;
     size_t d = 3 * np2 + (size_t)Np * b.Nf + (size_t)b.Nf * b.Nf + 4 * nt2 + 2 * (size_t)b.Krows * Nt;
     d += (size_t)nslots * (nt2 + 2 * np2);
+    d += 2 * (size_t)64 * (Np + Nt);                 // two-level panel windows
     return d * sizeof(double);
 }
 
@@ -1180,7 +1181,7 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
     }
     SCATT_TRY(bt.arena.alloc(total));
     size_t itot = 0;
-    for (auto& d : bt.ed) itot += 2 * (size_t)(d.Np + d.Nt) + 8;
+    for (auto& d : bt.ed) itot += 4 * (size_t)(d.Np + d.Nt) + 8;
     SCATT_TRY(bt.iarena.alloc(itot));
     SCATT_CUDA_TRY(cudaMemsetAsync(bt.iarena.p, 0, itot * sizeof(int), s));
     size_t ip = 0;
@@ -1202,6 +1203,8 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         d.tailR = p; p += (size_t)nslots * nt2;
         d.tailS = p; p += (size_t)nslots * np2;
         d.psiT = p; p += (size_t)nslots * np2;
+        d.PS = p; p += (size_t)2 * 64 * d.Np;
+        d.PR = p; p += (size_t)2 * 64 * d.Nt;
         int* q = bt.iarena.p + ip;
         d.sigS = q; q += d.Np;
         d.ridS = q; q += d.Np;
@@ -1209,7 +1212,9 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         d.ridR = q; q += d.Nt;
         d.stS = q; q += 4;
         d.stR = q; q += 4;
-        ip += 2 * (size_t)(d.Np + d.Nt) + 8;
+        d.sgS = q; q += 2 * d.Np;
+        d.sgR = q; q += 2 * d.Nt;
+        ip += 4 * (size_t)(d.Np + d.Nt) + 8;
         SCATT_CUDA_TRY(cudaMemsetAsync(d.G0, 0, (size_t)K * d.Nt * sizeof(double), s));
     }
     SCATT_TRY(upload_vec(bt.d_ed, bt.ed, s));
@@ -1245,7 +1250,7 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         const bool exch = n < b.n_tr && Nf > 0;
         if (exch) SCATT_TRY(gemm_dev(bt, b.gmS, count, bt.ed, 0, 0, 1, s));
         if (exch && n < b.stab_n) { k_stab<<<count, TPB, 0, s>>>(b, n, 1); SCATT_COUNT_LAUNCH(1); }
-        SCATT_TRY(gj_inverse_batched(b.gjS, count, maxNp, true, s));
+        SCATT_TRY(gj_inverse_selected(b.gjS, count, maxNp, true, s));
         k_collect<<<cdiv(count, 128), 128, 0, s>>>(b, n, 0);
         SCATT_COUNT_LAUNCH(1);
         if (exch) {
@@ -1269,7 +1274,7 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
                 rev.push_back(a1);
                 cudaEventRecord(a0, s);
             }
-            SCATT_TRY(gj_inverse_batched(b.gjR, count, maxNt, true, s));
+            SCATT_TRY(gj_inverse_selected(b.gjR, count, maxNt, true, s));
             if (sample) cudaEventRecord(rev.back(), s);
             k_collect<<<cdiv(count, 128), 128, 0, s>>>(b, n, 1);
             SCATT_COUNT_LAUNCH(1);

@@ -60,6 +60,7 @@ def lib():
     L.scatt_dgemm.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                               dptr, C.c_int, dptr, C.c_int, C.c_double, dptr, C.c_int]
     L.scatt_bench_inverse.argtypes = [C.c_int, C.c_int, C.c_int, dptr]
+    L.scatt_set_inverse_blocking.argtypes = [C.c_int]
     _lib = L
     return L
 
@@ -118,3 +119,7 @@ def bench_inverse(n: int, count: int, reps: int = 5) -> float:
     ms = C.c_double(0.0)
     check(lib().scatt_bench_inverse(n, count, reps, C.byref(ms)))
     return ms.value
+
+
+def set_inverse_blocking(two_level: bool):
+    check(lib().scatt_set_inverse_blocking(1 if two_level else 0))

@@ -4,8 +4,10 @@ Tolerance per observable: max(1e-10, 10 x floor), where floor is how far the
 oracle itself moves between the reference's two LAPACK builds (Eigen
 partialPivLu vs MKL dgetri / dsytrf+dsytri) on the same inputs -- the
 rounding floor of the ill-conditioned Numerov recurrence.  Both numbers are
-reported on failure.  Dipoles (D, D_raw, d_raw, partial sigma) are checked at
-1e-10 flat.
+reported on failure.  Dipoles (D, D_raw, d_raw, partial sigma) are held to
+1e-10 unless their own build-to-build spread is larger (the z dipole of the
+l_cont = 11 H2O-like case at E = 0.9 moves by 1.1e-10 between the two
+builds); their floor is not coupled to K's.
 """
 import numpy as np
 import pytest
@@ -42,7 +44,7 @@ def compare(g, r, r2, tag):
     def chk(name, got, ref, alt, flat=False):
         err = rel(got, ref)
         floor = rel(alt, ref) if flat else max(rel(alt, ref), coupled)
-        tol = 1e-10 if flat else max(1e-10, 10.0 * floor)
+        tol = max(1e-10, 10.0 * floor)
         if not err <= tol:
             fails.append(f"{tag} {name}: err {err:.3e} floor {floor:.3e} tol {tol:.1e}")
 
