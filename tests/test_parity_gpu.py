@@ -116,19 +116,24 @@ def test_mixed_l_cont_batch():
 
 
 def test_closed_channels_policy():
-    """k r_max < l: the determinant test marks l closed (AsymptoticAmplitudes.cpp:161-212)."""
-    inp = synth.h2_like(Nr=401, dr=0.05, l_cont=4)
+    """The determinant test marks l closed when det(M_l) <= 1e-20 max|M_l|^2
+    (AsymptoticAmplitudes.cpp:161-212); at k = 0.08 on r <= 20 only l = 8 of
+    l_cont = 8 falls under it."""
+    inp = synth.h2_like(Nr=401, dr=0.05, l_cont=8)
     sol = S.ScanSolver(inp)
     E = 0.5 * 0.08 ** 2
     res = sol.solve([E], opts=S.default_opts(allow_closed_channels=0), raise_on_error=False)[0]
     assert res.status == 6                                  # SCATT_ERR_CLOSED_CHANNEL
     res = sol.solve([E], opts=S.default_opts(allow_closed_channels=1))[0]
     st = O.make_setup(inp)
-    r = O.solve_energy(st, E)
-    assert res.diag["n_closed_l"] == len(r.aa["closed_l"]) > 0
+    r, r2 = oracle_pair(st, E)
+    assert r.aa["closed_l"] == [8]
+    assert res.diag["n_closed_l"] == len(r.aa["closed_l"])
     mu_closed = [mu for mu in range(st.n_mu) if int(st.l_mu[mu]) in r.aa["closed_l"]]
     assert np.all(res.A[mu_closed, :] == np.eye(st.n_mu)[mu_closed, :])
     assert np.all(res.B[mu_closed, :] == 0.0)
+    fails = compare(res, r, r2, "closed")
+    assert not fails, "\n".join(fails)
 
 
 def test_batch_equals_single_energy_runs():
