@@ -1,6 +1,6 @@
 // capi.cu -- extern "C" entry points: error handling, angular algebra,
 // device building blocks.  The per-energy-batch solver entry points live in
-// scan.cu, the per-step compatibility seam in steppers.cu.
+// solver.cu.
 #include <cstring>
 #include <string>
 #include <vector>
