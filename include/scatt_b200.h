@@ -62,6 +62,20 @@ double scatt_riccati_y(int l, double x);
 int scatt_inverse_batched(int n, int count, const double* A, double* out,
                           int symmetrize, int* status);
 
+/* scatt_inverse_batched without device allocation: every device buffer
+ * (matrix copies, ping-pong buffers, pivot maps, panel windows, status words,
+ * entry table) is carved from one static 64 MiB device array per device.
+ * Limits: n <= 1280, count <= 256, and
+ * 8 count (3 n^2 + 128 n) + 4 count (4 n + 2) + 80 count bytes (each of
+ * the nine pieces rounded up to 256) <= 64 MiB; larger requests return SCATT_ERR_SIZE before
+ * any device work.  The first call on a device resolves the array's address
+ * (cudaGetSymbolAddress) and should come before any stream capture.  Calls
+ * that overlap in time on one device (several host threads) share the
+ * array and race.  No counterpart in the reference (LapackInverse.hpp
+ * allocates its workspace per call). */
+int scatt_inverse_batched_noalloc(int n, int count, const double* A, double* out,
+                                  int symmetrize, int* status);
+
 /* C = alpha op(A) op(B) + beta C on the device, host buffers (op: 0 = N, 1 = T). */
 int scatt_dgemm(int opA, int opB, int M, int N, int K, double alpha,
                 const double* A, int lda, const double* B, int ldb,

@@ -16,6 +16,8 @@ namespace scatt {
 // Error bookkeeping: every host entry point returns an int status; the last
 // error message is kept per thread (see capi.cu).
 void set_last_error(const std::string& msg);
+// SCATT_ERR_NO_DEVICE (with the last error set) when no CUDA device is visible.
+int require_device();
 
 #define SCATT_CUDA_TRY(expr)                                                    \
     do {                                                                        \

@@ -42,8 +42,6 @@
 
 namespace scatt {
 
-int require_device();
-
 namespace {
 
 constexpr int TPB = 256;

@@ -57,6 +57,7 @@ def lib():
         getattr(L, f).restype = C.c_double
         getattr(L, f).argtypes = [C.c_int, C.c_double]
     L.scatt_inverse_batched.argtypes = [C.c_int, C.c_int, dptr, dptr, C.c_int, iptr]
+    L.scatt_inverse_batched_noalloc.argtypes = [C.c_int, C.c_int, dptr, dptr, C.c_int, iptr]
     L.scatt_dgemm.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                               dptr, C.c_int, dptr, C.c_int, C.c_double, dptr, C.c_int]
     L.scatt_bench_inverse.argtypes = [C.c_int, C.c_int, C.c_int, dptr]
@@ -84,8 +85,11 @@ def device_count() -> int:
     return n.value
 
 
-def inverse_batched(A: np.ndarray, symmetrize: bool = False):
-    """Inverse of each n x n matrix of A (shape (count, n, n) or (n, n)); returns (inv, status)."""
+def inverse_batched(A: np.ndarray, symmetrize: bool = False, noalloc: bool = False):
+    """Inverse of each n x n matrix of A (shape (count, n, n) or (n, n)); returns (inv, status).
+
+    noalloc=True goes through scatt_inverse_batched_noalloc (static device
+    scratch, no device allocation; bounded sizes)."""
     A = np.asarray(A, dtype=np.float64)
     single = A.ndim == 2
     if single:
@@ -95,7 +99,8 @@ def inverse_batched(A: np.ndarray, symmetrize: bool = False):
     Af = np.ascontiguousarray(np.transpose(A, (0, 2, 1)))
     out = np.empty_like(Af)
     st = np.zeros((count, 2), dtype=np.int32)
-    code = lib().scatt_inverse_batched(n, count, as_dptr(Af), as_dptr(out), int(symmetrize), as_iptr(st))
+    fn = lib().scatt_inverse_batched_noalloc if noalloc else lib().scatt_inverse_batched
+    code = fn(n, count, as_dptr(Af), as_dptr(out), int(symmetrize), as_iptr(st))
     inv = np.transpose(out, (0, 2, 1))
     if code not in (0, 4, 5):
         check(code)
