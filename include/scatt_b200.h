@@ -62,9 +62,14 @@ double scatt_riccati_y(int l, double x);
 int scatt_inverse_batched(int n, int count, const double* A, double* out,
                           int symmetrize, int* status);
 
-/* scatt_inverse_batched without device allocation: every device buffer
- * (matrix copies, ping-pong buffers, pivot maps, panel windows, status words,
- * entry table) is carved from one static 64 MiB device array per device.
+/* scatt_inverse_batched without device allocation, for callers that cannot
+ * call cudaMalloc: a host whose own allocator already holds the device's free
+ * memory (a framework's caching allocator, a fixed per-rank budget), or a
+ * latency-bound caller that cannot accept the device-wide synchronisation of
+ * cudaMalloc / cudaFree.  Every device buffer (matrix copies, ping-pong
+ * buffers, pivot maps, panel windows, status words, entry table) is carved
+ * from one static 64 MiB device array per device, held until exit by every
+ * GPU that loads the library.
  * Limits: n <= 1280, count <= 256, and
  * 8 count (3 n^2 + 128 n) + 4 count (4 n + 2) + 80 count bytes (each of
  * the nine pieces rounded up to 256) <= 64 MiB; larger requests return SCATT_ERR_SIZE before

@@ -1,6 +1,9 @@
 // noalloc.cu -- scatt_inverse_batched_noalloc: the batched Gauss-Jordan
 // inverse with every device buffer carved from one file-scope scratch array,
-// so a call performs no device allocation.
+// so a call performs no device allocation.  It serves callers that cannot
+// call cudaMalloc: hosts whose own allocator already owns the device's free
+// memory, and latency-bound callers that cannot take the device-wide
+// synchronisation of cudaMalloc / cudaFree.
 //
 // The scratch array is a module-level __device__ object.  This file is its
 // own CUDA module, so the array is only reserved on a device once this entry

@@ -1,6 +1,12 @@
-"""scatt_inverse_batched_noalloc (static device scratch) against the allocating
-scatt_inverse_batched on the same inputs, two calls in a row, and its size
-limits.  Collected last so it also runs after every other GPU test."""
+"""scatt_inverse_batched_noalloc against the allocating scatt_inverse_batched.
+
+The allocation-free entry point is for callers that cannot call cudaMalloc
+(their own allocator owns the device's free memory, or they cannot take the
+synchronisation of cudaMalloc / cudaFree); it uses one static device scratch
+array instead.  Checked here: the same inverses on two calls in a row (the
+array keeps the previous call's contents), singular-pivot reporting, and the
+size limits.  The file is collected last so it also runs after every other
+GPU test."""
 import numpy as np
 import pytest
 
