@@ -906,8 +906,51 @@ __device__ __forceinline__ double* win_out(const GjEntry& e, int s) {
     return e.P + (size_t)((s + 1) & 1) * e.ld * OB;
 }
 
-template <int R, int MAXT>
-__global__ void __launch_bounds__(MAXT, 1)
+// Panel of 16 columns of the 64-column window, one CTA (NW warps) per matrix.
+// Each thread keeps R rows of the panel in registers with each row's current
+// position (pos); rows never move between threads, a pivot swap only
+// relabels two positions.  Pivot choice: largest magnitude among positions
+// >= k, ties to the smallest position (partial pivoting as in dgetrf / Eigen
+// partialPivLu).  The argmax is exact: a candidate's key is the bit pattern
+// of |v| (monotone for non-negative doubles) split into two words, reduced
+// with warp max/min reductions, then the smallest position among equal keys.
+// Each warp publishes its candidate key and the candidate's whole panel row,
+// so one barrier per column hands every thread the pivot and the pivot row.
+// The loop is software pipelined: once column j's pivot is known, the next
+// column's slot is updated first and its candidate search overlaps the
+// update of the other columns.  Rows are eliminated LU-style,
+// v -= (f / piv) * pivot_row; the pivot row is rescaled by its one owner.
+// The panel columns rotate through the register slots P2_QU at a time, so
+// the active column sits in a fixed slot.
+constexpr int P2_QU = 2;         // panel columns per unrolled group (rotation step)
+
+struct PivKey {
+    unsigned hi, lo;   // hi = 0: no candidate
+    int pos;
+};
+
+// key of a non-negative magnitude (hi is offset by one so that 0 means none)
+__device__ __forceinline__ PivKey piv_key(double a, int pos) {
+    if (pos < 0) return PivKey{0u, 0u, -1};
+    const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(a));
+    return PivKey{static_cast<unsigned>(b >> 32) + 1u, static_cast<unsigned>(b), pos};
+}
+
+// warp-wide best key (every lane gets the result)
+__device__ __forceinline__ PivKey warp_best_key(PivKey x) {
+    const unsigned H = __reduce_max_sync(0xffffffffu, x.hi);
+    const unsigned L = __reduce_max_sync(0xffffffffu, x.hi == H ? x.lo : 0u);
+    const bool tie = x.hi == H && x.lo == L && x.pos >= 0;
+    const unsigned P = __reduce_min_sync(0xffffffffu, tie ? static_cast<unsigned>(x.pos) : 0xffffffffu);
+    return PivKey{H, L, H == 0u ? -1 : static_cast<int>(P)};
+}
+
+__device__ __forceinline__ double key_value(const PivKey& k) {
+    return __longlong_as_double(static_cast<long long>((static_cast<unsigned long long>(k.hi - 1u) << 32) | k.lo));
+}
+
+template <int R, int NW>
+__global__ void __launch_bounds__(NW * 32, 1)
 gj2_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
     const GjEntry e = entries[blockIdx.x];
     const int n = e.n;
@@ -923,138 +966,169 @@ gj2_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
     const int T = blockDim.x, W = T >> 5;
     const bool first = (K == 0 && sub == 0);
 
-    extern __shared__ double smem[];
-    int* loc = reinterpret_cast<int*>(smem);
-    int* rid = loc + n;
-    __shared__ double red_v[2][32];
-    __shared__ int red_i[2][32];
-    __shared__ double sprow[2][NB];
-    __shared__ double krow[2][NB];
-    __shared__ int s_status;
+    __shared__ unsigned red_hi[2][NW], red_lo[2][NW];
+    __shared__ int red_i[2][NW];
+    __shared__ double red_row[2][NW][NB];
+    // row labels travel with the rows; kept in shared memory (used at the ends only)
+    extern __shared__ int lab_s[];
+    int* stv_s = lab_s + n;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double v[R][NB];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int i = tid + r * T;
-#pragma unroll
-        for (int j = 0; j < NB; ++j)
-            v[r][j] = (i < n && j < nb) ? src[i + (size_t)(cs + j) * e.ld] : 0.0;
-    }
-    for (int i = tid; i < n; i += T) {
-        loc[i] = i;
-        rid[i] = first ? i : e.rowid[i];
-    }
-    if (tid == 0) s_status = first ? 0 : e.status[0];
-    __syncthreads();
-
-#pragma unroll 1
-    for (int j = 0; j < NB; ++j) {
-        if (j < nb) {
-            const int k = kr0 + j;
-            const int par = j & 1;
-            double bv = -1.0;
-            int bi = -1;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = tid + r * T;
-                if (i >= k && i < n) {
-                    const double a = fabs(v[r][0]);
-                    if (a > bv) { bv = a; bi = i; }
-                }
-            }
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-                better_key(bv, bi, ov, oi);
-            }
-            if (lane == 0) { red_v[par][warp] = bv; red_i[par][warp] = bi; }
-            __syncthreads();
-            bv = (lane < W) ? red_v[par][lane] : -1.0;
-            bi = (lane < W) ? red_i[par][lane] : -1;
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-                better_key(bv, bi, ov, oi);
-            }
-            const int p = bi < 0 ? k : bi;
-            if (tid == 0) {
-                int st = 0;
-                if (bi < 0 || !(bv < INFINITY)) st = DEV_NONFINITE;
-                else if (bv == 0.0) st = DEV_SINGULAR;
-                if (st && s_status == 0) { s_status = st; e.status[1] = k; }
-                if (p != k) {
-                    const int a = loc[k]; loc[k] = loc[p]; loc[p] = a;
-                    const int b2 = rid[k]; rid[k] = rid[p]; rid[p] = b2;
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = tid + r * T;
-                if (i == p) {
-                    double piv = v[r][0];
-                    if (piv == 0.0) piv = 1.0;      // the status word records the failure
-                    const double inv = 1.0 / piv;
-                    sprow[par][0] = inv;
-#pragma unroll
-                    for (int c = 1; c < NB; ++c) sprow[par][c] = v[r][c] * inv;
-                }
-                if (i == k) {
-#pragma unroll
-                    for (int c = 0; c < NB; ++c) krow[par][c] = v[r][c];
-                }
-            }
-            __syncthreads();
-            const double inv = sprow[par][0];
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = tid + r * T;
-                if (i < n) {
-                    if (i == k) {
-#pragma unroll
-                        for (int c = 0; c < NB; ++c) v[r][c] = sprow[par][c];
-                    } else {
-                        if (i == p) {
-#pragma unroll
-                            for (int c = 0; c < NB; ++c) v[r][c] = krow[par][c];
-                        }
-                        const double f = v[r][0];
-                        v[r][0] = -f * inv;
-#pragma unroll
-                        for (int c = 1; c < NB; ++c) v[r][c] -= f * sprow[par][c];
-                    }
-                }
-            }
-        }
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const double t0 = v[r][0];
-#pragma unroll
-            for (int c = 0; c < NB - 1; ++c) v[r][c] = v[r][c + 1];
-            v[r][NB - 1] = t0;
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int i = tid + r * T;
-        if (i < n) {
-#pragma unroll
-            for (int j = 0; j < NB; ++j)
-                if (j < nb) dst[i + (size_t)(cs + j) * e.ld] = v[r][j];
-        }
-    }
     const int* st_in = e.sigt + (size_t)(sub & 1) * n;
     int* st_out = e.sigt + (size_t)((sub + 1) & 1) * n;
-    for (int i = tid; i < n; i += T) {
-        const int l = loc[i];
-        e.sigma[i] = l;
-        e.rowid[i] = rid[i];
-        st_out[i] = (sub == 0) ? l : st_in[l];
+    double v[R][NB];
+    int pos[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = tid + r * T;
+        const bool ok = i < n;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) v[r][j] = (ok && j < nb) ? src[i + (size_t)(cs + j) * e.ld] : 0.0;
+        pos[r] = ok ? i : -1;
+        if (ok) {
+            lab_s[i] = first ? i : e.rowid[i];
+            stv_s[i] = (sub == 0) ? i : st_in[i];
+        }
     }
-    if (tid == 0) e.status[0] = s_status;
+    int st_code = 0, st_col = -1;
+    if (tid == 0) st_code = first ? 0 : e.status[0];
+
+    // candidate of the first column (slot 0)
+    {
+        double bv = -1.0;
+        int bi = -1;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (pos[r] >= kr0) better_key(bv, bi, fabs(v[r][0]), pos[r]);
+        const PivKey wk = warp_best_key(piv_key(bv, bi));
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const bool mine = wk.pos >= 0 && pos[r] == wk.pos;
+            if (__any_sync(0xffffffffu, mine) && mine) {
+#pragma unroll
+                for (int c = 0; c < NB; ++c) red_row[0][warp][c] = v[r][c];
+            }
+        }
+        if (lane == 0) { red_hi[0][warp] = wk.hi; red_lo[0][warp] = wk.lo; red_i[0][warp] = wk.pos; }
+    }
+
+#pragma unroll 1
+    for (int g = 0; g < NB / P2_QU; ++g) {
+#pragma unroll
+        for (int q = 0; q < P2_QU; ++q) {
+            const int jj = g * P2_QU + q;
+            if (jj < nb) {
+                const int k = kr0 + jj;
+                const int par = q & 1;
+                __syncthreads();
+                const PivKey gk = warp_best_key(lane < W ? PivKey{red_hi[par][lane], red_lo[par][lane], red_i[par][lane]}
+                                                         : PivKey{0u, 0u, -1});
+                const bool have = gk.pos >= 0;
+                // positions are unique, so exactly one warp published row gk.pos
+                const unsigned own = __ballot_sync(0xffffffffu, have && lane < W && red_i[par][lane] == gk.pos);
+                const int ws = own ? __ffs(own) - 1 : 0;
+                const int p = have ? gk.pos : k;
+                const double* prow = red_row[par][ws];
+                double piv = have ? prow[q] : 0.0;
+                if (tid == 0 && st_code == 0) {
+                    int s = 0;
+                    if (!have || !(key_value(gk) < INFINITY)) s = DEV_NONFINITE;
+                    else if (key_value(gk) == 0.0) s = DEV_SINGULAR;
+                    if (s) { st_code = s; st_col = k; }
+                }
+                if (piv == 0.0) piv = 1.0;      // the status word records the failure
+                const double inv = 1.0 / piv;
+                double m[R];
+                bool isp[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    m[r] = v[r][q] * inv;
+                    isp[r] = have && pos[r] == p;
+                    const int pr = pos[r];
+                    pos[r] = (pr == p) ? k : (pr == k ? p : pr);
+                }
+                const bool more = jj + 1 < nb;
+                // the next column's slot first, then its candidate search
+                if (have) {
+                    const double pc = prow[q + 1];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) v[r][q + 1] = fma(-m[r], pc, v[r][q + 1]);
+                }
+                PivKey nk{0u, 0u, -1};
+                if (more) {
+                    double bv = -1.0;
+                    int bi = -1;
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+                        if (pos[r] >= k + 1) better_key(bv, bi, fabs(v[r][q + 1]), pos[r]);
+                    nk = warp_best_key(piv_key(bv, bi));
+                }
+                // the other columns
+                if (have) {
+#pragma unroll
+                    for (int c = 0; c < NB; ++c) {
+                        if (c == q || c == q + 1) continue;
+                        const double pc = prow[c];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) v[r][c] = fma(-m[r], pc, v[r][c]);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    v[r][q] = -m[r];
+                    // the pivot row becomes the scaled pivot row (one thread of one warp)
+                    if (__any_sync(0xffffffffu, isp[r]) && isp[r]) {
+#pragma unroll
+                        for (int c = 0; c < NB; ++c) v[r][c] = (c == q) ? inv : prow[c] * inv;
+                    }
+                }
+                // publish the next column's candidate
+                if (more) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const bool mine = nk.pos >= 0 && pos[r] == nk.pos;
+                        if (__any_sync(0xffffffffu, mine) && mine) {
+                            // after the group's last column the slots rotate by P2_QU
+                            // before the next column reads this row
+#pragma unroll
+                            for (int c = 0; c < NB; ++c)
+                                red_row[par ^ 1][warp][c] = v[r][(q == P2_QU - 1) ? (c + P2_QU) % NB : c];
+                        }
+                    }
+                    if (lane == 0) { red_hi[par ^ 1][warp] = nk.hi; red_lo[par ^ 1][warp] = nk.lo; red_i[par ^ 1][warp] = nk.pos; }
+                }
+            }
+        }
+        // rotate the panel columns by P2_QU slots
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            double t[P2_QU];
+#pragma unroll
+            for (int c = 0; c < P2_QU; ++c) t[c] = v[r][c];
+#pragma unroll
+            for (int c = 0; c < NB - P2_QU; ++c) v[r][c] = v[r][c + P2_QU];
+#pragma unroll
+            for (int c = 0; c < P2_QU; ++c) v[r][NB - P2_QU + c] = t[c];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int ps = pos[r];
+        if (ps >= 0) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+                if (j < nb) dst[ps + (size_t)(cs + j) * e.ld] = v[r][j];
+            const int i = tid + r * T;
+            e.sigma[ps] = i;
+            e.rowid[ps] = lab_s[i];
+            st_out[ps] = stv_s[i];
+        }
+    }
+    if (tid == 0) {
+        e.status[0] = st_code;
+        if (st_col >= 0) e.status[1] = st_col;
+    }
 }
 
 // rank-16 update of the other columns of the 64-column window
@@ -1490,13 +1564,22 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax, bool sy
     }
     const int outer = (nmax + OB - 1) / OB;
     const int tiles = (nmax + 63) / 64;
-    const size_t smem_reg = 2 * (size_t)nmax * sizeof(int);
-    const int T4 = 32 * std::max(1, (nmax + 63) / 64);
+    // panel shape (rows per thread x warps): 1x8 (n <= 256), 2x8 (<= 512),
+    // 3x8 (<= 768), 3x12 (<= 1152), 5x8 (<= 1280)
+    const int pcfg = nmax <= 256 ? 0 : nmax <= 512 ? 1 : nmax <= 768 ? 2 : nmax <= 1152 ? 3 : 4;
+    const int prows = pcfg == 0 ? 1 : pcfg == 1 ? 2 : pcfg <= 3 ? 3 : 5;
+    const int pt = 32 * (((nmax + prows - 1) / prows + 31) / 32);
+    const size_t lab_smem = 2 * (size_t)nmax * sizeof(int);
     int launches = 0;
     for (int K = 0; K < outer; ++K) {
         for (int sub = 0; sub < OB / NB; ++sub) {
-            if (nmax <= 512) gj2_panel_kernel<2, 256><<<count, T4, smem_reg, stream>>>(entries_dev, K, sub);
-            else gj2_panel_kernel<2, 640><<<count, T4, smem_reg, stream>>>(entries_dev, K, sub);
+            switch (pcfg) {
+                case 0: gj2_panel_kernel<1, 8><<<count, pt, lab_smem, stream>>>(entries_dev, K, sub); break;
+                case 1: gj2_panel_kernel<2, 8><<<count, pt, lab_smem, stream>>>(entries_dev, K, sub); break;
+                case 2: gj2_panel_kernel<3, 8><<<count, pt, lab_smem, stream>>>(entries_dev, K, sub); break;
+                case 3: gj2_panel_kernel<3, 12><<<count, pt, lab_smem, stream>>>(entries_dev, K, sub); break;
+                default: gj2_panel_kernel<5, 8><<<count, pt, lab_smem, stream>>>(entries_dev, K, sub); break;
+            }
             gj2_narrow_kernel<<<dim3(tiles, 1, count), U2T, U2_SMEM, stream>>>(entries_dev, K, sub);
             launches += 2;
         }
