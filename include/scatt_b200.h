@@ -90,10 +90,14 @@ int scatt_dgemm(int opA, int opB, int M, int N, int K, double alpha,
  * matrices (CUDA events around the kernels only); used by the tile autotuner
  * and the benchmark. */
 int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call);
-/* Blocking scheme of scatt_inverse_batched / scatt_bench_inverse: 1 = two-level
- * (64-column windows, rank-64 trailing updates; default), 0 = single-level
- * (rank-16 updates).  Both give the same inverse up to rounding. */
-int scatt_set_inverse_blocking(int two_level);
+/* Blocking scheme of every dense inverse (the entry points and the solver):
+ * 0 = automatic (default): scheme 3 above order 512, scheme 2 below,
+ * 1 = single-level (rank-16 updates, row pivoting),
+ * 2 = two-level column-major (64-column windows, row pivoting),
+ * 3 = two-level on the row-contiguous view of the buffer (pivots by columns
+ *     of A, which for a symmetric A is the row-pivoting sequence).
+ * All give the same inverse up to rounding. */
+int scatt_set_inverse_blocking(int scheme);
 
 /* ------------------------------------------------------ per-scan solver
  * The reference runs one energy at a time through run_one_energy

@@ -15,8 +15,8 @@ namespace scatt {
 namespace {
 thread_local std::string g_last_error;
 }
-// 1: every dense inverse uses the single-level (16-column) scheme
-int g_single_level = 0;
+// scheme of every dense inverse (see gj_inverse_selected)
+int g_inverse_scheme = 0;
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
@@ -110,8 +110,7 @@ int scatt_inverse_batched(int n, int count, const double* A, double* out, int sy
     }
     DevBuf<GjEntry> dent;
     SCATT_TRY(dent.upload(ent));
-    if (g_single_level) SCATT_TRY(gj_inverse_batched(dent.p, count, n, symmetrize != 0, 0));
-    else SCATT_TRY(gj_inverse_batched2(dent.p, count, n, symmetrize != 0, 0));
+    SCATT_TRY(gj_inverse_selected(dent.p, count, n, symmetrize != 0, 0));
     SCATT_CUDA_TRY(cudaDeviceSynchronize());
     SCATT_CUDA_TRY(cudaMemcpy(out, dO.p, nn * count * sizeof(double), cudaMemcpyDeviceToHost));
     std::vector<int> st(2 * count);
@@ -158,8 +157,12 @@ int scatt_dgemm(int opA, int opB, int M, int N, int K, double alpha, const doubl
 }
 
 
-int scatt_set_inverse_blocking(int two_level) {
-    g_single_level = two_level ? 0 : 1;
+int scatt_set_inverse_blocking(int scheme) {
+    if (scheme < 0 || scheme > 3) {
+        set_last_error("scatt_set_inverse_blocking: scheme must be 0, 1, 2 or 3");
+        return SCATT_ERR_ARG;
+    }
+    g_inverse_scheme = scheme;
     return SCATT_OK;
 }
 
@@ -193,8 +196,7 @@ int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call) {
     for (int r = 0; r < reps + 1; ++r) {
         SCATT_CUDA_TRY(cudaMemcpyAsync(dA.p, dS.p, nn * count * sizeof(double), cudaMemcpyDeviceToDevice));
         cudaEventRecord(e0);
-        if (g_single_level) SCATT_TRY(gj_inverse_batched(dent.p, count, n, true, 0));
-        else SCATT_TRY(gj_inverse_batched2(dent.p, count, n, true, 0));
+        SCATT_TRY(gj_inverse_selected(dent.p, count, n, true, 0));
         cudaEventRecord(e1);
         SCATT_CUDA_TRY(cudaEventSynchronize(e1));
         float ms = 0.f;

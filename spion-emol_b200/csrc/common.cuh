@@ -102,14 +102,31 @@ int gj_inverse_batched(const GjEntry* entries_dev, int count, int nmax,
 int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax,
                         bool symmetrize, cudaStream_t stream);
 
-// 1: every dense inverse (entry points and solver) uses the single-level scheme
-extern int g_single_level;
+// Two-level variant on the row-contiguous view: the column-major buffer of A
+// is treated as the row-major B = A^T (inv(A) = inv(B)^T), so pivot rows and
+// window rows are contiguous runs.  Pivoting is partial pivoting on B, i.e.
+// by columns of A; for symmetric A it is the row-pivoting sequence of A.
+// Same entry requirements as gj_inverse_batched2 (P: 2 x ld x 64 doubles).
+int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax,
+                        bool symmetrize, cudaStream_t stream);
 
-// The scheme selected by g_single_level (entries must carry P and sigt).
+// Scheme of every dense inverse (entry points and solver): 0 = automatic
+// (row-contiguous two-level above order 512, where its contiguous pivot-row
+// tiles pay; column-major two-level below), 1 = single-level,
+// 2 = column-major two-level, 3 = row-contiguous two-level
+extern int g_inverse_scheme;
+
+// The scheme selected by g_inverse_scheme (entries must carry P and sigt).
 inline int gj_inverse_selected(const GjEntry* entries_dev, int count, int nmax,
                                bool symmetrize, cudaStream_t stream) {
-    return g_single_level ? gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream)
-                          : gj_inverse_batched2(entries_dev, count, nmax, symmetrize, stream);
+    switch (g_inverse_scheme) {
+        case 1: return gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream);
+        case 2: return gj_inverse_batched2(entries_dev, count, nmax, symmetrize, stream);
+        case 3: return gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream);
+        default:
+            return nmax > 512 ? gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream)
+                              : gj_inverse_batched2(entries_dev, count, nmax, symmetrize, stream);
+    }
 }
 
 }  // namespace scatt

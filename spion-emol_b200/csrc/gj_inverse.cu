@@ -906,6 +906,19 @@ __device__ __forceinline__ double* win_out(const GjEntry& e, int s) {
     return e.P + (size_t)((s + 1) & 1) * e.ld * OB;
 }
 
+// Row-contiguous layout (RM): the column-major buffer of A is read as the
+// row-major B = A^T, so row i of B (column i of A) is contiguous.  A window is
+// 64 columns of B; the window buffers P hold it row-major with row stride OB.
+// Element (row i, window column c) of the window input / output:
+__device__ __forceinline__ const double* win_in_rm(const GjEntry& e, int K, int s, int& lds) {
+    if (s == 0) { lds = e.ld; return buf_of(e, K & 1) + (size_t)K * OB; }
+    lds = OB;
+    return e.P + (size_t)(s & 1) * e.ld * OB;
+}
+__device__ __forceinline__ double* win_out_rm(const GjEntry& e, int s) {
+    return e.P + (size_t)((s + 1) & 1) * e.ld * OB;
+}
+
 // Panel of 16 columns of the 64-column window, one CTA (NW warps) per matrix.
 // Each thread keeps R rows of the panel in registers with each row's current
 // position (pos); rows never move between threads, a pivot swap only
@@ -949,7 +962,7 @@ __device__ __forceinline__ double key_value(const PivKey& k) {
     return __longlong_as_double(static_cast<long long>((static_cast<unsigned long long>(k.hi - 1u) << 32) | k.lo));
 }
 
-template <int R, int NW>
+template <int R, int NW, bool RM>
 __global__ void __launch_bounds__(NW * 32, 1)
 gj2_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
     const GjEntry e = entries[blockIdx.x];
@@ -961,10 +974,16 @@ gj2_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
     if (cs >= nb64) return;
     const int nb = min(NB, nb64 - cs);
     const int kr0 = k0o + cs;
-    const double* src = win_in(e, K, sub);
-    double* dst = win_out(e, sub);
+    int lds = e.ld;
+    const double* src = RM ? win_in_rm(e, K, sub, lds) : win_in(e, K, sub);
+    double* dst = RM ? win_out_rm(e, sub) : win_out(e, sub);
+    // (row i, window column c) -> element offset
+    const size_t rs = RM ? (size_t)lds : 1, cst = RM ? 1 : (size_t)lds;
+    const size_t drs = RM ? (size_t)OB : 1, dcs = RM ? 1 : (size_t)e.ld;
     const int T = blockDim.x, W = T >> 5;
     const bool first = (K == 0 && sub == 0);
+    // row-contiguous view: whole 16-byte pairs when the row stride and the column count are even
+    const bool vrow = RM && (rs % 2 == 0) && (nb % 2 == 0);
 
     __shared__ unsigned red_hi[2][NW], red_lo[2][NW];
     __shared__ int red_i[2][NW];
@@ -983,7 +1002,19 @@ gj2_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
         const int i = tid + r * T;
         const bool ok = i < n;
 #pragma unroll
-        for (int j = 0; j < NB; ++j) v[r][j] = (ok && j < nb) ? src[i + (size_t)(cs + j) * e.ld] : 0.0;
+        if (RM && vrow) {
+            // 16 contiguous doubles of row i in 16-byte pairs
+            const double2* rp = reinterpret_cast<const double2*>(src + i * rs + cs);
+#pragma unroll
+            for (int j = 0; j < NB / 2; ++j) {
+                const double2 x = (ok && 2 * j < nb) ? rp[j] : make_double2(0.0, 0.0);
+                v[r][2 * j] = x.x;
+                v[r][2 * j + 1] = x.y;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < NB; ++j) v[r][j] = (ok && j < nb) ? src[i * rs + (size_t)(cs + j) * cst] : 0.0;
+        }
         pos[r] = ok ? i : -1;
         if (ok) {
             lab_s[i] = first ? i : e.rowid[i];
@@ -1116,9 +1147,16 @@ gj2_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
     for (int r = 0; r < R; ++r) {
         const int ps = pos[r];
         if (ps >= 0) {
+            if (RM && vrow) {
+                double2* wp = reinterpret_cast<double2*>(dst + ps * drs + cs);
 #pragma unroll
-            for (int j = 0; j < NB; ++j)
-                if (j < nb) dst[ps + (size_t)(cs + j) * e.ld] = v[r][j];
+                for (int j = 0; j < NB / 2; ++j)
+                    if (2 * j < nb) wp[j] = make_double2(v[r][2 * j], v[r][2 * j + 1]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < NB; ++j)
+                    if (j < nb) dst[ps * drs + (size_t)(cs + j) * dcs] = v[r][j];
+            }
             const int i = tid + r * T;
             e.sigma[ps] = i;
             e.rowid[ps] = lab_s[i];
@@ -1451,10 +1489,305 @@ gj2_trail2_kernel(const GjEntry* __restrict__ entries, int K) {
             }
 }
 
+// ---------------------------------------------------------------------------
+// Row-contiguous (RM) narrow and trailing updates.  Every operand row is a
+// contiguous run: the pivot rows of the old matrix, the rows of the
+// transformed window and the C tile rows are copied with 16-byte cp.async
+// when the row stride is even (8-byte copies otherwise).
+
+__device__ __forceinline__ void cp_async16(double* sdst, const double* gsrc, bool pred) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(sdst));
+    const int sz = pred ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" :: "r"(sa), "l"(gsrc), "r"(sz));
+}
+
+constexpr int N3S = 20;      // row stride of the 64 x 16 multiplier tile (= 4 mod 16)
+constexpr int T3R = 68;      // row stride of the 64-wide tiles (= 4 mod 16)
+constexpr size_t NARROW3_SMEM = (64 * T3R + 64 * N3S + NB * T3R) * sizeof(double);
+
+// rank-16 update of the other columns of the 64-column window (RM layout):
+//   out[i, c] = (i a pivot position of this panel ? 0 : in[sigma(i), c])
+//               + sum_j Mp[i, j] in[sigma(kr0 + j), c]
+__global__ void __launch_bounds__(U2T)
+gj3_narrow_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
+    const GjEntry e = entries[blockIdx.z];
+    const int n = e.n;
+    const int k0o = K * OB;
+    if (k0o >= n) return;
+    const int nb64 = min(OB, n - k0o);
+    const int cs = sub * NB;
+    if (cs >= nb64) return;
+    const int nb = min(NB, nb64 - cs);
+    const int kr0 = k0o + cs;
+    const int r0 = blockIdx.x * 64;
+    if (r0 >= n) return;
+    int lds;
+    const double* src = win_in_rm(e, K, sub, lds);
+    double* dst = win_out_rm(e, sub);
+    // 16-byte rows need an even stride; the big buffer also needs whole pairs inside the window
+    const bool v16 = (lds % 2 == 0) && (sub > 0 || nb64 % 2 == 0);
+
+    extern __shared__ double n3smem[];
+    double (*Cs)[T3R] = reinterpret_cast<double (*)[T3R]>(n3smem);
+    double (*Ms)[N3S] = reinterpret_cast<double (*)[N3S]>(n3smem + 64 * T3R);
+    double (*Xs)[T3R] = reinterpret_cast<double (*)[T3R]>(n3smem + 64 * T3R + 64 * N3S);
+    __shared__ int srow[64];
+    __shared__ int xrow[NB];
+    const int tid = threadIdx.x;
+    if (tid < 64) srow[tid] = (r0 + tid < n) ? e.sigma[r0 + tid] : 0;
+    else if (tid < 64 + NB) {
+        const int j = tid - 64;
+        xrow[j] = (j < nb) ? e.sigma[kr0 + j] : 0;
+    }
+    __syncthreads();
+    if (v16) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {              // C: 64 rows x 32 pairs
+            const int idx = tid + u * U2T;
+            const int row = idx >> 5, c = 2 * (idx & 31);
+            const int gi = r0 + row;
+            const bool ok = gi < n && c < nb64 && !(gi >= kr0 && gi < kr0 + nb);
+            cp_async16(&Cs[row][c], src + (ok ? (size_t)srow[row] * lds + c : 0), ok);
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {              // X: 16 pivot rows x 32 pairs
+            const int idx = tid + u * U2T;
+            const int j = idx >> 5, c = 2 * (idx & 31);
+            const bool ok = j < nb && c < nb64;
+            cp_async16(&Xs[j][c], src + (ok ? (size_t)xrow[j] * lds + c : 0), ok);
+        }
+    } else {
+#pragma unroll 4
+        for (int u = 0; u < 16; ++u) {
+            const int idx = tid + u * U2T;
+            const int row = idx >> 6, c = idx & 63;
+            const int gi = r0 + row;
+            const bool ok = gi < n && c < nb64 && !(gi >= kr0 && gi < kr0 + nb);
+            cp_async8(&Cs[row][c], src + (ok ? (size_t)srow[row] * lds + c : 0), ok);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int idx = tid + u * U2T;
+            const int j = idx >> 6, c = idx & 63;
+            const bool ok = j < nb && c < nb64;
+            cp_async8(&Xs[j][c], src + (ok ? (size_t)xrow[j] * lds + c : 0), ok);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {                  // Mp: 64 rows x 16 (panel output, stride OB)
+        const int idx = tid + u * U2T;
+        const int m = idx >> 4, j = idx & 15;
+        const int gi = r0 + m;
+        const bool ok = gi < n && j < nb;
+        cp_async8(&Ms[m][j], dst + (ok ? (size_t)gi * OB + cs + j : 0), ok);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+    double acc[2][2][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int jn = 0; jn < 2; ++jn)
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                acc[i][jn][v] = Cs[wm + i * 16 + g + ((v >> 1) << 3)][wn + jn * 8 + 2 * t + (v & 1)];
+#pragma unroll
+    for (int kk = 0; kk < NB; kk += 4) {
+        double a[2][2], b[2];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            a[i][0] = Ms[wm + i * 16 + g][kk + t];
+            a[i][1] = Ms[wm + i * 16 + g + 8][kk + t];
+        }
+#pragma unroll
+        for (int jn = 0; jn < 2; ++jn) b[jn] = Xs[kk + t][wn + jn * 8 + g];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int jn = 0; jn < 2; ++jn) dmma_16x8x4(acc[i][jn], a[i][0], a[i][1], b[jn]);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int jn = 0; jn < 2; ++jn)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int gi = r0 + wm + i * 16 + g + ((v >> 1) << 3);
+                const int c = wn + jn * 8 + 2 * t + (v & 1);
+                if (gi < n && c < nb64 && !(c >= cs && c < cs + nb)) dst[(size_t)gi * OB + c] = acc[i][jn][v];
+            }
+}
+
+// rank-64 update of every column tile outside the window (RM layout), one
+// 128 x 64 tile per CTA, 8 warps of 32 x 32:
+//   new[i, c] = (i in the window rows ? 0 : old[st(i), c]) + sum_j M[i, j] old[st(k0 + j), c]
+// M = the transformed window (row-major, stride OB); the window's own column
+// tile is copied from M.  The k dimension arrives in four 16-wide cp.async
+// groups so the first DMMAs start before the whole tile has landed.
+constexpr int T3M = 128;
+constexpr size_t TRAIL3_SMEM = (T3M * T3R + OB * T3R) * sizeof(double);
+
+__global__ void __launch_bounds__(U2T, 2)
+gj3_trail_kernel(const GjEntry* __restrict__ entries, int K) {
+    const GjEntry e = entries[blockIdx.z];
+    const int n = e.n;
+    const int k0 = K * OB;
+    if (k0 >= n) return;
+    const int nb64 = min(OB, n - k0);
+    const int nsub = (nb64 + NB - 1) / NB;
+    const int r0 = blockIdx.x * T3M, c0 = blockIdx.y * 64;
+    if (r0 >= n || c0 >= n) return;
+    const size_t ld = e.ld;
+    const double* src = buf_of(e, K & 1);
+    double* dst = buf_of(e, (K + 1) & 1);
+    const double* Mw = e.P + (size_t)(nsub & 1) * e.ld * OB;
+    const int* st = e.sigt + (size_t)(nsub & 1) * n;
+    const int tid = threadIdx.x;
+    if (c0 == k0) {
+        for (int idx = tid; idx < T3M * 64; idx += U2T) {
+            const int row = idx >> 6, col = idx & 63;
+            const int gi = r0 + row;
+            if (gi < n && col < nb64) dst[gi * ld + k0 + col] = Mw[(size_t)gi * OB + col];
+        }
+        return;
+    }
+    const bool v16 = (ld % 2 == 0);          // n even: pairs never straddle a row end
+    const bool m16 = (nb64 % 2 == 0);        // whole pairs inside the window
+    extern __shared__ double t3smem[];
+    double (*Ms)[T3R] = reinterpret_cast<double (*)[T3R]>(t3smem);
+    double (*Xs)[T3R] = reinterpret_cast<double (*)[T3R]>(t3smem + T3M * T3R);
+    __shared__ int srow[T3M];
+    __shared__ int xrow[OB];
+    if (tid < T3M) srow[tid] = (r0 + tid < n) ? st[r0 + tid] : 0;
+    else if (tid < T3M + OB) {
+        const int j = tid - T3M;
+        xrow[j] = (j < nb64) ? st[k0 + j] : 0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) {
+        if (m16) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {          // M: 128 rows x 8 pairs of this chunk
+                const int idx = tid + u * U2T;
+                const int m = idx >> 3, j = ch * NB + 2 * (idx & 7);
+                const int gi = r0 + m;
+                const bool ok = gi < n && j < nb64;
+                cp_async16(&Ms[m][j], Mw + (ok ? (size_t)gi * OB + j : 0), ok);
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int idx = tid + u * U2T;
+                const int m = idx >> 4, j = ch * NB + (idx & 15);
+                const int gi = r0 + m;
+                const bool ok = gi < n && j < nb64;
+                cp_async8(&Ms[m][j], Mw + (ok ? (size_t)gi * OB + j : 0), ok);
+            }
+        }
+        if (v16) {
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {          // X: 16 pivot rows x 32 pairs
+                const int idx = tid + u * U2T;
+                const int j = ch * NB + (idx >> 5), c = 2 * (idx & 31);
+                const bool ok = j < nb64 && c0 + c < n;
+                cp_async16(&Xs[j][c], src + (ok ? (size_t)xrow[j] * ld + c0 + c : 0), ok);
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int idx = tid + u * U2T;
+                const int j = ch * NB + (idx >> 6), c = idx & 63;
+                const bool ok = j < nb64 && c0 + c < n;
+                cp_async8(&Xs[j][c], src + (ok ? (size_t)xrow[j] * ld + c0 + c : 0), ok);
+            }
+        }
+        cp_async_commit();
+    }
+    const int lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
+    double acc[2][4][4];
+    // C tile straight from the old matrix into the accumulators
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int rl = wm + i * 16 + g + 8 * h;
+            const int gi = r0 + rl;
+            const bool rok = gi < n && !(gi >= k0 && gi < k0 + nb64);
+            const double* rowp = src + (size_t)srow[rl] * ld + c0;
+#pragma unroll
+            for (int jn = 0; jn < 4; ++jn) {
+                const int c = wn + jn * 8 + 2 * t;
+                double x0 = 0.0, x1 = 0.0;
+                if (rok && c0 + c < n) {
+                    if (v16) {
+                        const double2 p2 = *reinterpret_cast<const double2*>(rowp + c);
+                        x0 = p2.x; x1 = p2.y;
+                    } else {
+                        x0 = rowp[c];
+                        if (c0 + c + 1 < n) x1 = rowp[c + 1];
+                    }
+                }
+                acc[i][jn][2 * h] = x0;
+                acc[i][jn][2 * h + 1] = x1;
+            }
+        }
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) {
+        if (ch == 0) cp_async_wait<3>();
+        else if (ch == 1) cp_async_wait<2>();
+        else if (ch == 2) cp_async_wait<1>();
+        else cp_async_wait<0>();
+        __syncthreads();
+        if (ch < nsub) {
+#pragma unroll
+            for (int kq = 0; kq < NB; kq += 4) {
+                const int kk = ch * NB + kq;
+                double a[2][2], b[4];
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    a[i][0] = Ms[wm + i * 16 + g][kk + t];
+                    a[i][1] = Ms[wm + i * 16 + g + 8][kk + t];
+                }
+#pragma unroll
+                for (int jn = 0; jn < 4; ++jn) b[jn] = Xs[kk + t][wn + jn * 8 + g];
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int jn = 0; jn < 4; ++jn) dmma_16x8x4(acc[i][jn], a[i][0], a[i][1], b[jn]);
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int gi = r0 + wm + i * 16 + g + 8 * h;
+            if (gi >= n) continue;
+            double* rowp = dst + (size_t)gi * ld + c0;
+#pragma unroll
+            for (int jn = 0; jn < 4; ++jn) {
+                const int c = wn + jn * 8 + 2 * t;
+                if (c0 + c >= n) continue;
+                if (v16) {
+                    *reinterpret_cast<double2*>(rowp + c) = make_double2(acc[i][jn][2 * h], acc[i][jn][2 * h + 1]);
+                } else {
+                    rowp[c] = acc[i][jn][2 * h];
+                    if (c0 + c + 1 < n) rowp[c + 1] = acc[i][jn][2 * h + 1];
+                }
+            }
+        }
+}
+
 constexpr int FT = 32;
 
 __global__ void __launch_bounds__(FT * 8)
-gj_finalize_kernel(const GjEntry* __restrict__ entries, int nsteps_parity, int symmetrize) {
+gj_finalize_kernel(const GjEntry* __restrict__ entries, int nsteps_parity, int symmetrize, int rm) {
     // nsteps_parity: 0 = single-level (16-column steps), 1 = two-level (64-column steps)
     const GjEntry e = entries[blockIdx.z];
     const int n = e.n;
@@ -1478,11 +1811,15 @@ gj_finalize_kernel(const GjEntry* __restrict__ entries, int nsteps_parity, int s
         if (id >= j0 && id < j0 + FT) pi_j[id - j0] = r;
     }
     __syncthreads();
-    // T1[a][b] = X[i0 + a][pi(j0 + b)],  T2[a][b] = X[j0 + a][pi(i0 + b)]
+    // column-major layout: inv[i][j] = X[i][pi(j)]
+    // row-contiguous layout (X holds inv(A^T) row-major): inv[i][j] = X[j * ld + pi(i)]
+    // T1[a][b] = inv[i0 + a][j0 + b],  T2[a][b] = inv[j0 + a][i0 + b]
     for (int b = ty; b < FT; b += 8) {
         const int a = tx;
-        if (j0 + b < n && i0 + a < n) T1[a][b] = X[(i0 + a) + (size_t)pi_j[b] * e.ld];
-        if (symmetrize && i0 + b < n && j0 + a < n) T2[a][b] = X[(j0 + a) + (size_t)pi_i[b] * e.ld];
+        if (j0 + b < n && i0 + a < n)
+            T1[a][b] = rm ? X[(size_t)(j0 + b) * e.ld + pi_i[a]] : X[(i0 + a) + (size_t)pi_j[b] * e.ld];
+        if (symmetrize && i0 + b < n && j0 + a < n)
+            T2[a][b] = rm ? X[(size_t)(i0 + b) * e.ld + pi_j[a]] : X[(j0 + a) + (size_t)pi_i[b] * e.ld];
     }
     __syncthreads();
     for (int b = ty; b < FT; b += 8) {
@@ -1494,6 +1831,26 @@ gj_finalize_kernel(const GjEntry* __restrict__ entries, int nsteps_parity, int s
             e.out[i + (size_t)j * e.ldo] = v;
         }
     }
+}
+
+template <bool RM>
+int launch_panel(int pcfg, int count, int pt, size_t smem, cudaStream_t stream, const GjEntry* ent, int K, int sub) {
+    switch (pcfg) {
+        case 0: gj2_panel_kernel<1, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub); break;
+        case 1: gj2_panel_kernel<2, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub); break;
+        case 2: gj2_panel_kernel<3, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub); break;
+        case 3: gj2_panel_kernel<3, 12, RM><<<count, pt, smem, stream>>>(ent, K, sub); break;
+        default: gj2_panel_kernel<5, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub); break;
+    }
+    return SCATT_OK;
+}
+
+// panel shape (rows per thread x warps): 1x8 (n <= 256), 2x8 (<= 512),
+// 3x8 (<= 768), 3x12 (<= 1152), 5x8 (<= 1280)
+void panel_shape(int nmax, int& pcfg, int& pt) {
+    pcfg = nmax <= 256 ? 0 : nmax <= 512 ? 1 : nmax <= 768 ? 2 : nmax <= 1152 ? 3 : 4;
+    const int prows = pcfg == 0 ? 1 : pcfg == 1 ? 2 : pcfg <= 3 ? 3 : 5;
+    pt = 32 * (((nmax + prows - 1) / prows + 31) / 32);
 }
 
 }  // namespace
@@ -1544,7 +1901,7 @@ int gj_inverse_batched(const GjEntry* entries_dev, int count, int nmax,
         gj_update2_kernel<<<ugrid, U2T, U2_SMEM, stream>>>(entries_dev, kb);
     }
     const int ft = (nmax + FT - 1) / FT;
-    gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, 0, symmetrize ? 1 : 0);
+    gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, 0, symmetrize ? 1 : 0, 0);
     SCATT_CUDA_TRY(cudaGetLastError());
     SCATT_COUNT_LAUNCH(2 * steps + 1);
     return SCATT_OK;
@@ -1564,22 +1921,13 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax, bool sy
     }
     const int outer = (nmax + OB - 1) / OB;
     const int tiles = (nmax + 63) / 64;
-    // panel shape (rows per thread x warps): 1x8 (n <= 256), 2x8 (<= 512),
-    // 3x8 (<= 768), 3x12 (<= 1152), 5x8 (<= 1280)
-    const int pcfg = nmax <= 256 ? 0 : nmax <= 512 ? 1 : nmax <= 768 ? 2 : nmax <= 1152 ? 3 : 4;
-    const int prows = pcfg == 0 ? 1 : pcfg == 1 ? 2 : pcfg <= 3 ? 3 : 5;
-    const int pt = 32 * (((nmax + prows - 1) / prows + 31) / 32);
+    int pcfg, pt;
+    panel_shape(nmax, pcfg, pt);
     const size_t lab_smem = 2 * (size_t)nmax * sizeof(int);
     int launches = 0;
     for (int K = 0; K < outer; ++K) {
         for (int sub = 0; sub < OB / NB; ++sub) {
-            switch (pcfg) {
-                case 0: gj2_panel_kernel<1, 8><<<count, pt, lab_smem, stream>>>(entries_dev, K, sub); break;
-                case 1: gj2_panel_kernel<2, 8><<<count, pt, lab_smem, stream>>>(entries_dev, K, sub); break;
-                case 2: gj2_panel_kernel<3, 8><<<count, pt, lab_smem, stream>>>(entries_dev, K, sub); break;
-                case 3: gj2_panel_kernel<3, 12><<<count, pt, lab_smem, stream>>>(entries_dev, K, sub); break;
-                default: gj2_panel_kernel<5, 8><<<count, pt, lab_smem, stream>>>(entries_dev, K, sub); break;
-            }
+            SCATT_TRY(launch_panel<false>(pcfg, count, pt, lab_smem, stream, entries_dev, K, sub));
             gj2_narrow_kernel<<<dim3(tiles, 1, count), U2T, U2_SMEM, stream>>>(entries_dev, K, sub);
             launches += 2;
         }
@@ -1587,7 +1935,42 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax, bool sy
         ++launches;
     }
     const int ft = (nmax + FT - 1) / FT;
-    gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, 1, symmetrize ? 1 : 0);
+    gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, 1, symmetrize ? 1 : 0, 0);
+    SCATT_CUDA_TRY(cudaGetLastError());
+    SCATT_COUNT_LAUNCH(launches + 1);
+    return SCATT_OK;
+}
+
+int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax, bool symmetrize,
+                        cudaStream_t stream) {
+    if (count <= 0 || nmax <= 0) return SCATT_OK;
+    if (nmax > 1280) return gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream);
+    static bool attr3 = false;
+    if (!attr3) {
+        SCATT_CUDA_TRY(cudaFuncSetAttribute(gj3_narrow_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)NARROW3_SMEM));
+        SCATT_CUDA_TRY(cudaFuncSetAttribute(gj3_trail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)TRAIL3_SMEM));
+        attr3 = true;
+    }
+    const int outer = (nmax + OB - 1) / OB;
+    const int tiles = (nmax + 63) / 64;
+    const int mtiles = (nmax + T3M - 1) / T3M;
+    int pcfg, pt;
+    panel_shape(nmax, pcfg, pt);
+    const size_t lab_smem = 2 * (size_t)nmax * sizeof(int);
+    int launches = 0;
+    for (int K = 0; K < outer; ++K) {
+        for (int sub = 0; sub < OB / NB; ++sub) {
+            SCATT_TRY(launch_panel<true>(pcfg, count, pt, lab_smem, stream, entries_dev, K, sub));
+            gj3_narrow_kernel<<<dim3(tiles, 1, count), U2T, NARROW3_SMEM, stream>>>(entries_dev, K, sub);
+            launches += 2;
+        }
+        gj3_trail_kernel<<<dim3(mtiles, tiles, count), U2T, TRAIL3_SMEM, stream>>>(entries_dev, K);
+        ++launches;
+    }
+    const int ft = (nmax + FT - 1) / FT;
+    gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, 1, symmetrize ? 1 : 0, 1);
     SCATT_CUDA_TRY(cudaGetLastError());
     SCATT_COUNT_LAUNCH(launches + 1);
     return SCATT_OK;

@@ -1115,6 +1115,7 @@ size_t energy_bytes(const BatchDev& b, int Np, int Nt, int nslots) {
     size_t d = 3 * np2 + (size_t)Np * b.Nf + (size_t)b.Nf * b.Nf + 4 * nt2 + 2 * (size_t)b.Krows * Nt;
     d += (size_t)nslots * (nt2 + 2 * np2);
     d += 2 * (size_t)64 * (Np + Nt);                 // two-level panel windows
+    d += 16 * 32;                                    // every buffer starts on a 256-byte boundary
     return d * sizeof(double);
 }
 
@@ -1174,7 +1175,7 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         d.Np = (d.l_cont + 1) * (d.l_cont + 1);
         d.Nt = d.Np + Nf;
         off[e] = total;
-        total += energy_bytes(b, d.Np, d.Nt, nslots) / sizeof(double);
+        total += (energy_bytes(b, d.Np, d.Nt, nslots) / sizeof(double) + 31) & ~size_t(31);
         SCATT_TRY(ensure_stab(ctx, o, d.l_cont, &d.lmA, &d.lmS, keep));
     }
     SCATT_TRY(bt.arena.alloc(total));
@@ -1187,22 +1188,24 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         EnergyDev& d = bt.ed[e];
         const size_t np2 = (size_t)d.Np * d.Np, nt2 = (size_t)d.Nt * d.Nt;
         double* p = bt.arena.p + off[e];
-        d.S = p; p += np2;
-        d.Sw = p; p += np2;
-        d.Sinv = p; p += np2;
-        d.T = p; p += (size_t)d.Np * Nf;
-        d.F = p; p += (size_t)Nf * Nf;
-        d.Ra = p; p += nt2;
-        d.Rw = p; p += nt2;
-        d.Rinv0 = p; p += nt2;
-        d.Rinv1 = p; p += nt2;
-        d.G0 = p; p += (size_t)K * d.Nt;
-        d.G1 = p; p += (size_t)K * d.Nt;
-        d.tailR = p; p += (size_t)nslots * nt2;
-        d.tailS = p; p += (size_t)nslots * np2;
-        d.psiT = p; p += (size_t)nslots * np2;
-        d.PS = p; p += (size_t)2 * 64 * d.Np;
-        d.PR = p; p += (size_t)2 * 64 * d.Nt;
+        // 256-byte aligned pieces (the inverse kernels copy 16-byte row pairs)
+        auto take = [&p](size_t cnt) { double* r = p; p += (cnt + 31) & ~size_t(31); return r; };
+        d.S = take(np2);
+        d.Sw = take(np2);
+        d.Sinv = take(np2);
+        d.T = take((size_t)d.Np * Nf);
+        d.F = take((size_t)Nf * Nf);
+        d.Ra = take(nt2);
+        d.Rw = take(nt2);
+        d.Rinv0 = take(nt2);
+        d.Rinv1 = take(nt2);
+        d.G0 = take((size_t)K * d.Nt);
+        d.G1 = take((size_t)K * d.Nt);
+        d.tailR = take((size_t)nslots * nt2);
+        d.tailS = take((size_t)nslots * np2);
+        d.psiT = take((size_t)nslots * np2);
+        d.PS = take((size_t)2 * 64 * d.Np);
+        d.PR = take((size_t)2 * 64 * d.Nt);
         int* q = bt.iarena.p + ip;
         d.sigS = q; q += d.Np;
         d.ridS = q; q += d.Np;

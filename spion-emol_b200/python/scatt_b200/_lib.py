@@ -126,5 +126,7 @@ def bench_inverse(n: int, count: int, reps: int = 5) -> float:
     return ms.value
 
 
-def set_inverse_blocking(two_level: bool):
-    check(lib().scatt_set_inverse_blocking(1 if two_level else 0))
+def set_inverse_blocking(scheme: int):
+    """0: automatic (default); 1: single-level; 2: two-level column-major;
+    3: two-level row-contiguous."""
+    check(lib().scatt_set_inverse_blocking(int(scheme)))

@@ -1,6 +1,6 @@
 """Device timing of the batched FP64 inverse (the per-step R^-1 / Sinv kernels).
 
-    python -m scatt_b200.inverse_bench --n 1046 --count 32 [--reps 5] [--single-level]
+    python -m scatt_b200.inverse_bench --n 1046 --count 32 [--reps 5] [--scheme 0|1|2|3]
 
 Seeded well-conditioned matrices are generated on the device; CUDA events
 bracket the inverse kernels only (scatt_bench_inverse).  Prints one JSON line
@@ -20,13 +20,15 @@ def main(argv=None):
     ap.add_argument("--n", type=int, nargs="+", default=[1046])
     ap.add_argument("--count", type=int, default=32)
     ap.add_argument("--reps", type=int, default=5)
-    ap.add_argument("--single-level", action="store_true")
+    ap.add_argument("--scheme", type=int, default=0,
+                    help="0 automatic (default), 1 single-level, 2 two-level column-major, "
+                         "3 two-level row-contiguous")
     a = ap.parse_args(argv)
-    _lib.set_inverse_blocking(not a.single_level)
+    _lib.set_inverse_blocking(a.scheme)
     for n in a.n:
         ms = _lib.bench_inverse(n, a.count, a.reps)
         print(json.dumps({"n": n, "count": a.count, "reps": a.reps,
-                          "scheme": "single-level" if a.single_level else "two-level",
+                          "scheme": a.scheme,
                           "ms_per_call": ms, "tflops": 2.0 * n ** 3 * a.count / (ms * 1e-3) / 1e12}))
 
 

@@ -58,3 +58,21 @@ def test_dgemm_matches_numpy(opA, opB, M, N, K):
     out = _lib.dgemm(A, B, C0, alpha=-0.75, beta=0.5, opA=opA, opB=opB)
     ref = -0.75 * ((A.T if opA else A) @ (B.T if opB else B)) + 0.5 * C0
     assert np.max(np.abs(out - ref)) <= 1e-13 * max(1.0, np.max(np.abs(ref))) * np.sqrt(K + 1)
+
+
+@pytest.mark.parametrize("scheme", [1, 2, 3])
+@pytest.mark.parametrize("n", [77, 441, 600, 1046])
+def test_inverse_every_scheme(scheme, n):
+    """Single-level, column-major two-level and row-contiguous two-level
+    inverses against numpy; odd orders take the 8-byte copy paths."""
+    rng = np.random.default_rng(1000 + n)
+    A = rng.standard_normal((2, n, n)) + 4.0 * np.sqrt(n) * np.eye(n)
+    try:
+        _lib.set_inverse_blocking(scheme)
+        inv, st = _lib.inverse_batched(A, symmetrize=False)
+    finally:
+        _lib.set_inverse_blocking(0)
+    assert np.all(st == 0)
+    for b in range(2):
+        ref = np.linalg.inv(A[b])
+        assert np.max(np.abs(inv[b] - ref)) / np.max(np.abs(ref)) < 1e-12
