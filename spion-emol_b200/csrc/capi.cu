@@ -95,10 +95,10 @@ int scatt_inverse_batched(int n, int count, const double* A, double* out, int sy
     SCATT_TRY(dA.alloc(nn * count));
     SCATT_TRY(dW.alloc(nn * count));
     SCATT_TRY(dO.alloc(nn * count));
-    SCATT_TRY(dP.alloc((size_t)2 * n * 64 * count));
+    SCATT_TRY(dP.alloc((size_t)4 * n * 64 * count));
     SCATT_TRY(dsig.alloc((size_t)n * count));
     SCATT_TRY(drid.alloc((size_t)n * count));
-    SCATT_TRY(dsg.alloc((size_t)2 * n * count));
+    SCATT_TRY(dsg.alloc((size_t)4 * n * count));
     SCATT_TRY(dst.alloc(2 * (size_t)count));
     SCATT_CUDA_TRY(cudaMemcpy(dA.p, A, nn * count * sizeof(double), cudaMemcpyHostToDevice));
     SCATT_CUDA_TRY(cudaMemset(dst.p, 0, 2 * count * sizeof(int)));
@@ -106,11 +106,11 @@ int scatt_inverse_batched(int n, int count, const double* A, double* out, int sy
     for (int b = 0; b < count; ++b) {
         ent[b] = GjEntry{dA.p + nn * b, dW.p + nn * b, dO.p + nn * b, dsig.p + (size_t)n * b,
                          drid.p + (size_t)n * b, dst.p + 2 * b, n, n, n,
-                         dP.p + (size_t)2 * n * 64 * b, dsg.p + (size_t)2 * n * b};
+                         dP.p + (size_t)4 * n * 64 * b, dsg.p + (size_t)4 * n * b};
     }
     DevBuf<GjEntry> dent;
     SCATT_TRY(dent.upload(ent));
-    SCATT_TRY(gj_inverse_selected(dent.p, count, n, symmetrize != 0, 0));
+    SCATT_TRY(gj_inverse_selected(dent.p, count, n, symmetrize != 0, 0, true));
     SCATT_CUDA_TRY(cudaDeviceSynchronize());
     SCATT_CUDA_TRY(cudaMemcpy(out, dO.p, nn * count * sizeof(double), cudaMemcpyDeviceToHost));
     std::vector<int> st(2 * count);
@@ -172,8 +172,8 @@ int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call) {
     const size_t nn = (size_t)n * n;
     DevBuf<double> dA, dW, dO, dS, dP;
     DevBuf<int> dsig, drid, dst, dsg;
-    SCATT_TRY(dP.alloc((size_t)2 * n * 64 * count));
-    SCATT_TRY(dsg.alloc((size_t)2 * n * count));
+    SCATT_TRY(dP.alloc((size_t)4 * n * 64 * count));
+    SCATT_TRY(dsg.alloc((size_t)4 * n * count));
     SCATT_TRY(dA.alloc(nn * count));
     SCATT_TRY(dS.alloc(nn * count));
     SCATT_TRY(dW.alloc(nn * count));
@@ -186,7 +186,7 @@ int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call) {
     for (int b = 0; b < count; ++b)
         ent[b] = GjEntry{dA.p + nn * b, dW.p + nn * b, dO.p + nn * b, dsig.p + (size_t)n * b,
                          drid.p + (size_t)n * b, dst.p + 2 * b, n, n, n,
-                         dP.p + (size_t)2 * n * 64 * b, dsg.p + (size_t)2 * n * b};
+                         dP.p + (size_t)4 * n * 64 * b, dsg.p + (size_t)4 * n * b};
     DevBuf<GjEntry> dent;
     SCATT_TRY(dent.upload(ent));
     cudaEvent_t e0, e1;
@@ -196,7 +196,7 @@ int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call) {
     for (int r = 0; r < reps + 1; ++r) {
         SCATT_CUDA_TRY(cudaMemcpyAsync(dA.p, dS.p, nn * count * sizeof(double), cudaMemcpyDeviceToDevice));
         cudaEventRecord(e0);
-        SCATT_TRY(gj_inverse_selected(dent.p, count, n, true, 0));
+        SCATT_TRY(gj_inverse_selected(dent.p, count, n, true, 0, true));
         cudaEventRecord(e1);
         SCATT_CUDA_TRY(cudaEventSynchronize(e1));
         float ms = 0.f;

@@ -83,8 +83,8 @@ struct GjEntry {
     int*    rowid;    // n ints: original row index at each position
     int*    status;   // 1 int: DeviceStatus (first failing column in status[1])
     int n, ld, ldo;
-    double* P = nullptr;   // optional 2 x (ld x 64) panel-window buffers (two-level blocking)
-    int*    sigt = nullptr; // optional 2 x n composite row maps of the 64-column window
+    double* P = nullptr;   // optional panel-window buffers, 2 x (ld x 64) (4 x with look-ahead)
+    int*    sigt = nullptr; // optional composite row maps of the 64-column window (2 n, 4 n with look-ahead)
 };
 
 constexpr int GJ_NB = 16;
@@ -106,9 +106,12 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax,
 // is treated as the row-major B = A^T (inv(A) = inv(B)^T), so pivot rows and
 // window rows are contiguous runs.  Pivoting is partial pivoting on B, i.e.
 // by columns of A; for symmetric A it is the row-pivoting sequence of A.
-// Same entry requirements as gj_inverse_batched2 (P: 2 x ld x 64 doubles).
+// With look_ahead the 16-column panels of the next 64-column window run on a
+// high-priority side stream beside the trailing update of the current one;
+// then every entry needs P of 4 x ld x 64 doubles and sigt of 4 n ints
+// (without it, 2 x ld x 64 and 2 n as for gj_inverse_batched2).
 int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax,
-                        bool symmetrize, cudaStream_t stream);
+                        bool symmetrize, cudaStream_t stream, bool look_ahead);
 
 // Scheme of every dense inverse (entry points and solver): 0 = automatic
 // (row-contiguous two-level above order 512, where its contiguous pivot-row
@@ -117,14 +120,15 @@ int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax,
 extern int g_inverse_scheme;
 
 // The scheme selected by g_inverse_scheme (entries must carry P and sigt).
+// look_ahead: as for gj_inverse_batched3 (entries sized for it).
 inline int gj_inverse_selected(const GjEntry* entries_dev, int count, int nmax,
-                               bool symmetrize, cudaStream_t stream) {
+                               bool symmetrize, cudaStream_t stream, bool look_ahead) {
     switch (g_inverse_scheme) {
         case 1: return gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream);
         case 2: return gj_inverse_batched2(entries_dev, count, nmax, symmetrize, stream);
-        case 3: return gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream);
+        case 3: return gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream, look_ahead);
         default:
-            return nmax > 512 ? gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream)
+            return nmax > 512 ? gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream, look_ahead)
                               : gj_inverse_batched2(entries_dev, count, nmax, symmetrize, stream);
     }
 }

@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 namespace scatt {
 
@@ -910,13 +911,22 @@ __device__ __forceinline__ double* win_out(const GjEntry& e, int s) {
 // row-major B = A^T, so row i of B (column i of A) is contiguous.  A window is
 // 64 columns of B; the window buffers P hold it row-major with row stride OB.
 // Element (row i, window column c) of the window input / output:
-__device__ __forceinline__ const double* win_in_rm(const GjEntry& e, int K, int s, int& lds) {
+// With look-ahead (la = 1) the window buffers and the composite row maps come
+// in two sets selected by the parity of the outer step, so the chain of the
+// next window never touches what the current trailing update reads.
+__device__ __forceinline__ double* win_set_rm(const GjEntry& e, int K, int la) {
+    return e.P + (size_t)(la ? 2 * (K & 1) : 0) * e.ld * OB;
+}
+__device__ __forceinline__ int* sigt_set(const GjEntry& e, int K, int la) {
+    return e.sigt + (size_t)(la ? 2 * (K & 1) : 0) * e.n;
+}
+__device__ __forceinline__ const double* win_in_rm(const GjEntry& e, int K, int s, int& lds, int la) {
     if (s == 0) { lds = e.ld; return buf_of(e, K & 1) + (size_t)K * OB; }
     lds = OB;
-    return e.P + (size_t)(s & 1) * e.ld * OB;
+    return win_set_rm(e, K, la) + (size_t)(s & 1) * e.ld * OB;
 }
-__device__ __forceinline__ double* win_out_rm(const GjEntry& e, int s) {
-    return e.P + (size_t)((s + 1) & 1) * e.ld * OB;
+__device__ __forceinline__ double* win_out_rm(const GjEntry& e, int K, int s, int la) {
+    return win_set_rm(e, K, la) + (size_t)((s + 1) & 1) * e.ld * OB;
 }
 
 // Panel of 16 columns of the 64-column window, one CTA (NW warps) per matrix.
@@ -964,7 +974,7 @@ __device__ __forceinline__ double key_value(const PivKey& k) {
 
 template <int R, int NW, bool RM>
 __global__ void __launch_bounds__(NW * 32, 1)
-gj2_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
+gj2_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub, int la) {
     const GjEntry e = entries[blockIdx.x];
     const int n = e.n;
     const int k0o = K * OB;
@@ -975,8 +985,8 @@ gj2_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
     const int nb = min(NB, nb64 - cs);
     const int kr0 = k0o + cs;
     int lds = e.ld;
-    const double* src = RM ? win_in_rm(e, K, sub, lds) : win_in(e, K, sub);
-    double* dst = RM ? win_out_rm(e, sub) : win_out(e, sub);
+    const double* src = RM ? win_in_rm(e, K, sub, lds, la) : win_in(e, K, sub);
+    double* dst = RM ? win_out_rm(e, K, sub, la) : win_out(e, sub);
     // (row i, window column c) -> element offset
     const size_t rs = RM ? (size_t)lds : 1, cst = RM ? 1 : (size_t)lds;
     const size_t drs = RM ? (size_t)OB : 1, dcs = RM ? 1 : (size_t)e.ld;
@@ -993,8 +1003,9 @@ gj2_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
     int* stv_s = lab_s + n;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int* st_in = e.sigt + (size_t)(sub & 1) * n;
-    int* st_out = e.sigt + (size_t)((sub + 1) & 1) * n;
+    int* sg = RM ? sigt_set(e, K, la) : e.sigt;
+    const int* st_in = sg + (size_t)(sub & 1) * n;
+    int* st_out = sg + (size_t)((sub + 1) & 1) * n;
     double v[R][NB];
     int pos[R];
 #pragma unroll
@@ -1509,7 +1520,7 @@ constexpr size_t NARROW3_SMEM = (64 * T3R + 64 * N3S + NB * T3R) * sizeof(double
 //   out[i, c] = (i a pivot position of this panel ? 0 : in[sigma(i), c])
 //               + sum_j Mp[i, j] in[sigma(kr0 + j), c]
 __global__ void __launch_bounds__(U2T)
-gj3_narrow_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
+gj3_narrow_kernel(const GjEntry* __restrict__ entries, int K, int sub, int la) {
     const GjEntry e = entries[blockIdx.z];
     const int n = e.n;
     const int k0o = K * OB;
@@ -1522,8 +1533,8 @@ gj3_narrow_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
     const int r0 = blockIdx.x * 64;
     if (r0 >= n) return;
     int lds;
-    const double* src = win_in_rm(e, K, sub, lds);
-    double* dst = win_out_rm(e, sub);
+    const double* src = win_in_rm(e, K, sub, lds, la);
+    double* dst = win_out_rm(e, K, sub, la);
     // 16-byte rows need an even stride; the big buffer also needs whole pairs inside the window
     const bool v16 = (lds % 2 == 0) && (sub > 0 || nb64 % 2 == 0);
 
@@ -1630,21 +1641,25 @@ gj3_narrow_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
 constexpr int T3M = 128;
 constexpr size_t TRAIL3_SMEM = (T3M * T3R + OB * T3R) * sizeof(double);
 
+// cols: -1 every column tile; t >= 0 only tile t; -2 - t every tile but t
 __global__ void __launch_bounds__(U2T, 2)
-gj3_trail_kernel(const GjEntry* __restrict__ entries, int K) {
+gj3_trail_kernel(const GjEntry* __restrict__ entries, int K, int la, int cols) {
     const GjEntry e = entries[blockIdx.z];
     const int n = e.n;
     const int k0 = K * OB;
     if (k0 >= n) return;
     const int nb64 = min(OB, n - k0);
     const int nsub = (nb64 + NB - 1) / NB;
-    const int r0 = blockIdx.x * T3M, c0 = blockIdx.y * 64;
+    int ct = blockIdx.y;
+    if (cols >= 0) ct = cols;
+    else if (cols <= -2 && ct >= -2 - cols) ++ct;
+    const int r0 = blockIdx.x * T3M, c0 = ct * 64;
     if (r0 >= n || c0 >= n) return;
     const size_t ld = e.ld;
     const double* src = buf_of(e, K & 1);
     double* dst = buf_of(e, (K + 1) & 1);
-    const double* Mw = e.P + (size_t)(nsub & 1) * e.ld * OB;
-    const int* st = e.sigt + (size_t)(nsub & 1) * n;
+    const double* Mw = win_set_rm(e, K, la) + (size_t)(nsub & 1) * e.ld * OB;
+    const int* st = sigt_set(e, K, la) + (size_t)(nsub & 1) * n;
     const int tid = threadIdx.x;
     if (c0 == k0) {
         for (int idx = tid; idx < T3M * 64; idx += U2T) {
@@ -1834,14 +1849,45 @@ gj_finalize_kernel(const GjEntry* __restrict__ entries, int nsteps_parity, int s
 }
 
 template <bool RM>
-int launch_panel(int pcfg, int count, int pt, size_t smem, cudaStream_t stream, const GjEntry* ent, int K, int sub) {
+int launch_panel(int pcfg, int count, int pt, size_t smem, cudaStream_t stream, const GjEntry* ent, int K, int sub,
+                 int la) {
     switch (pcfg) {
-        case 0: gj2_panel_kernel<1, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub); break;
-        case 1: gj2_panel_kernel<2, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub); break;
-        case 2: gj2_panel_kernel<3, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub); break;
-        case 3: gj2_panel_kernel<3, 12, RM><<<count, pt, smem, stream>>>(ent, K, sub); break;
-        default: gj2_panel_kernel<5, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub); break;
+        case 0: gj2_panel_kernel<1, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
+        case 1: gj2_panel_kernel<2, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
+        case 2: gj2_panel_kernel<3, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
+        case 3: gj2_panel_kernel<3, 12, RM><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
+        default: gj2_panel_kernel<5, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
     }
+    return SCATT_OK;
+}
+
+// Side stream (highest priority) and two events per device for the
+// look-ahead of the row-contiguous inverse; created once per device.  The
+// enqueueing of one inverse holds the mutex, so its event record / wait pairs
+// cannot interleave with another thread's.
+struct LookAhead {
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_main = nullptr, ev_side = nullptr;
+};
+std::mutex g_la_mutex;
+LookAhead g_la[64];
+
+int look_ahead_resources(LookAhead** out) {
+    int dev = 0;
+    SCATT_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) {
+        set_last_error("look-ahead inverse: device ordinal out of range");
+        return SCATT_ERR_ARG;
+    }
+    LookAhead& r = g_la[dev];
+    if (!r.side) {
+        int lo = 0, hi = 0;
+        SCATT_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        SCATT_CUDA_TRY(cudaStreamCreateWithPriority(&r.side, cudaStreamNonBlocking, hi));
+        SCATT_CUDA_TRY(cudaEventCreateWithFlags(&r.ev_main, cudaEventDisableTiming));
+        SCATT_CUDA_TRY(cudaEventCreateWithFlags(&r.ev_side, cudaEventDisableTiming));
+    }
+    *out = &r;
     return SCATT_OK;
 }
 
@@ -1927,7 +1973,7 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax, bool sy
     int launches = 0;
     for (int K = 0; K < outer; ++K) {
         for (int sub = 0; sub < OB / NB; ++sub) {
-            SCATT_TRY(launch_panel<false>(pcfg, count, pt, lab_smem, stream, entries_dev, K, sub));
+            SCATT_TRY(launch_panel<false>(pcfg, count, pt, lab_smem, stream, entries_dev, K, sub, 0));
             gj2_narrow_kernel<<<dim3(tiles, 1, count), U2T, U2_SMEM, stream>>>(entries_dev, K, sub);
             launches += 2;
         }
@@ -1942,7 +1988,7 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax, bool sy
 }
 
 int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax, bool symmetrize,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, bool look_ahead) {
     if (count <= 0 || nmax <= 0) return SCATT_OK;
     if (nmax > 1280) return gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream);
     static bool attr3 = false;
@@ -1960,14 +2006,42 @@ int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax, bool sy
     panel_shape(nmax, pcfg, pt);
     const size_t lab_smem = 2 * (size_t)nmax * sizeof(int);
     int launches = 0;
-    for (int K = 0; K < outer; ++K) {
+    auto chain = [&](int K, cudaStream_t st, int la) -> int {
         for (int sub = 0; sub < OB / NB; ++sub) {
-            SCATT_TRY(launch_panel<true>(pcfg, count, pt, lab_smem, stream, entries_dev, K, sub));
-            gj3_narrow_kernel<<<dim3(tiles, 1, count), U2T, NARROW3_SMEM, stream>>>(entries_dev, K, sub);
+            SCATT_TRY(launch_panel<true>(pcfg, count, pt, lab_smem, st, entries_dev, K, sub, la));
+            gj3_narrow_kernel<<<dim3(tiles, 1, count), U2T, NARROW3_SMEM, st>>>(entries_dev, K, sub, la);
             launches += 2;
         }
-        gj3_trail_kernel<<<dim3(mtiles, tiles, count), U2T, TRAIL3_SMEM, stream>>>(entries_dev, K);
-        ++launches;
+        return SCATT_OK;
+    };
+    if (!look_ahead || outer < 2) {
+        for (int K = 0; K < outer; ++K) {
+            SCATT_TRY(chain(K, stream, 0));
+            gj3_trail_kernel<<<dim3(mtiles, tiles, count), U2T, TRAIL3_SMEM, stream>>>(entries_dev, K, 0, -1);
+            ++launches;
+        }
+    } else {
+        std::lock_guard<std::mutex> lock(g_la_mutex);
+        LookAhead* la = nullptr;
+        SCATT_TRY(look_ahead_resources(&la));
+        SCATT_TRY(chain(0, stream, 1));
+        for (int K = 0; K < outer; ++K) {
+            if (K + 1 < outer) {
+                // the next window's columns first, then its chain beside the rest of the update
+                gj3_trail_kernel<<<dim3(mtiles, 1, count), U2T, TRAIL3_SMEM, stream>>>(entries_dev, K, 1, K + 1);
+                SCATT_CUDA_TRY(cudaEventRecord(la->ev_main, stream));
+                SCATT_CUDA_TRY(cudaStreamWaitEvent(la->side, la->ev_main, 0));
+                SCATT_TRY(chain(K + 1, la->side, 1));
+                SCATT_CUDA_TRY(cudaEventRecord(la->ev_side, la->side));
+                gj3_trail_kernel<<<dim3(mtiles, tiles - 1, count), U2T, TRAIL3_SMEM, stream>>>(
+                    entries_dev, K, 1, -2 - (K + 1));
+                SCATT_CUDA_TRY(cudaStreamWaitEvent(stream, la->ev_side, 0));
+                launches += 2;
+            } else {
+                gj3_trail_kernel<<<dim3(mtiles, tiles, count), U2T, TRAIL3_SMEM, stream>>>(entries_dev, K, 1, -1);
+                ++launches;
+            }
+        }
     }
     const int ft = (nmax + FT - 1) / FT;
     gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, 1, symmetrize ? 1 : 0, 1);

@@ -1114,7 +1114,7 @@ size_t energy_bytes(const BatchDev& b, int Np, int Nt, int nslots) {
     const size_t np2 = (size_t)Np * Np, nt2 = (size_t)Nt * Nt;
     size_t d = 3 * np2 + (size_t)Np * b.Nf + (size_t)b.Nf * b.Nf + 4 * nt2 + 2 * (size_t)b.Krows * Nt;
     d += (size_t)nslots * (nt2 + 2 * np2);
-    d += 2 * (size_t)64 * (Np + Nt);                 // two-level panel windows
+    d += 4 * (size_t)64 * (Np + Nt);                 // two-level panel windows (two sets)
     d += 16 * 32;                                    // every buffer starts on a 256-byte boundary
     return d * sizeof(double);
 }
@@ -1180,7 +1180,7 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
     }
     SCATT_TRY(bt.arena.alloc(total));
     size_t itot = 0;
-    for (auto& d : bt.ed) itot += 4 * (size_t)(d.Np + d.Nt) + 8;
+    for (auto& d : bt.ed) itot += 6 * (size_t)(d.Np + d.Nt) + 8;
     SCATT_TRY(bt.iarena.alloc(itot));
     SCATT_CUDA_TRY(cudaMemsetAsync(bt.iarena.p, 0, itot * sizeof(int), s));
     size_t ip = 0;
@@ -1204,8 +1204,8 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         d.tailR = take((size_t)nslots * nt2);
         d.tailS = take((size_t)nslots * np2);
         d.psiT = take((size_t)nslots * np2);
-        d.PS = take((size_t)2 * 64 * d.Np);
-        d.PR = take((size_t)2 * 64 * d.Nt);
+        d.PS = take((size_t)4 * 64 * d.Np);
+        d.PR = take((size_t)4 * 64 * d.Nt);
         int* q = bt.iarena.p + ip;
         d.sigS = q; q += d.Np;
         d.ridS = q; q += d.Np;
@@ -1213,9 +1213,9 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         d.ridR = q; q += d.Nt;
         d.stS = q; q += 4;
         d.stR = q; q += 4;
-        d.sgS = q; q += 2 * d.Np;
-        d.sgR = q; q += 2 * d.Nt;
-        ip += 4 * (size_t)(d.Np + d.Nt) + 8;
+        d.sgS = q; q += 4 * d.Np;
+        d.sgR = q; q += 4 * d.Nt;
+        ip += 6 * (size_t)(d.Np + d.Nt) + 8;
         SCATT_CUDA_TRY(cudaMemsetAsync(d.G0, 0, (size_t)K * d.Nt * sizeof(double), s));
     }
     SCATT_TRY(upload_vec(bt.d_ed, bt.ed, s));
@@ -1251,7 +1251,7 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         const bool exch = n < b.n_tr && Nf > 0;
         if (exch) SCATT_TRY(gemm_dev(bt, b.gmS, count, bt.ed, 0, 0, 1, s));
         if (exch && n < b.stab_n) { k_stab<<<count, TPB, 0, s>>>(b, n, 1); SCATT_COUNT_LAUNCH(1); }
-        SCATT_TRY(gj_inverse_selected(b.gjS, count, maxNp, true, s));
+        SCATT_TRY(gj_inverse_selected(b.gjS, count, maxNp, true, s, true));
         k_collect<<<cdiv(count, 128), 128, 0, s>>>(b, n, 0);
         SCATT_COUNT_LAUNCH(1);
         if (exch) {
@@ -1275,7 +1275,7 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
                 rev.push_back(a1);
                 cudaEventRecord(a0, s);
             }
-            SCATT_TRY(gj_inverse_selected(b.gjR, count, maxNt, true, s));
+            SCATT_TRY(gj_inverse_selected(b.gjR, count, maxNt, true, s, true));
             if (sample) cudaEventRecord(rev.back(), s);
             k_collect<<<cdiv(count, 128), 128, 0, s>>>(b, n, 1);
             SCATT_COUNT_LAUNCH(1);

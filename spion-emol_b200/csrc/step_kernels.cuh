@@ -20,8 +20,8 @@ struct EnergyDev {
     double *Ra, *Rw, *Rinv0, *Rinv1, *G0, *G1;
     double *tailR, *tailS, *psiT;
     int *sigS, *ridS, *stS, *sigR, *ridR, *stR;
-    double *PS, *PR;       // two-level panel windows (2 x Np x 64, 2 x Nt x 64)
-    int *sgS, *sgR;        // composite row maps of the windows (2 x Np, 2 x Nt)
+    double *PS, *PR;       // two-level panel windows (4 x Np x 64, 4 x Nt x 64: two sets for look-ahead)
+    int *sgS, *sgR;        // composite row maps of the windows (4 x Np, 4 x Nt)
 };
 
 // Batch-level constants and shared per-step buffers.
