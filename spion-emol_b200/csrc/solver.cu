@@ -151,6 +151,28 @@ __global__ void k_build_B(BatchDev b, int n) {
     }
 }
 
+// Sinv of step n: the window store inside the asymptotic window, else the
+// chunk slot of step n.
+__device__ __forceinline__ double* sinv_at(const BatchDev& b, const EnergyDev& d, int n) {
+    const size_t np2 = (size_t)d.Np * d.Np;
+    return n >= b.n_s ? d.tailS + (size_t)(n - b.n_s) * np2 : d.Sinv + (size_t)(n - b.cn0) * np2;
+}
+
+// Entries of one chunk's Schur GEMM and inverse, index j * count + e.
+__global__ void k_prepare_schur(BatchDev b, int C) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= b.count * C) return;
+    const int j = idx / b.count, e = idx % b.count;
+    EnergyDev& d = b.ed[e];
+    const int Np = d.Np, Nf = b.Nf;
+    const size_t np2 = (size_t)Np * Np, sl = (size_t)b.Np_max * Nf;
+    double* S = d.S + j * np2;
+    b.gmS[idx] = GemmEntry{b.Bsc + j * sl, b.Bc + j * sl, S, Np, Np, Nf, b.Np_max, b.Np_max, Np, -1.0, 1.0};
+    b.gjS[idx] = GjEntry{S, d.Sw + j * np2, sinv_at(b, d, b.cn0 + j), d.sigS + (size_t)j * Np,
+                         d.ridS + (size_t)j * Np, d.stS + 4 * j, Np, Np, Np,
+                         d.PS + (size_t)j * 4 * 64 * Np, d.sgS + (size_t)j * 4 * Np};
+}
+
 // Fills the per-step GEMM / GJ entry arrays (pointer bookkeeping only).
 __global__ void k_prepare(BatchDev b, int n) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -158,32 +180,31 @@ __global__ void k_prepare(BatchDev b, int n) {
     EnergyDev& d = b.ed[e];
     const int Np = d.Np, Nt = d.Nt, Nf = b.Nf, K = b.Krows;
     const bool tail = n >= b.n_s;
-    double* sinv = tail ? d.tailS + (size_t)(n - b.n_s) * Np * Np : d.Sinv;
+    double* sinv = sinv_at(b, d, n);
     double* rinv = tail ? d.tailR + (size_t)(n - b.n_s) * Nt * Nt : ((n & 1) ? d.Rinv1 : d.Rinv0);
     double* gcur = (n & 1) ? d.G1 : d.G0;
     double* gnext = (n & 1) ? d.G0 : d.G1;
     const double* Cn = (n < b.n_pts) ? b.Ctab + (size_t)n * K * b.Np_max : nullptr;
-    b.gmS[e] = GemmEntry{b.Bs, b.B, d.S, Np, Np, Nf, b.Np_max, b.Np_max, Np, -1.0, 1.0};
     b.gmT[e] = GemmEntry{sinv, b.Bs, d.T, Np, Nf, Np, Np, b.Np_max, Np, 1.0, 0.0};
     b.gmF[e] = GemmEntry{b.Bs, d.T, d.F, Nf, Nf, Np, b.Np_max, Np, Nf, 1.0, 0.0};
     b.gmG1[e] = GemmEntry{Cn, sinv, gcur, K, Np, Np, K, Np, K, 1.0, 1.0};
     b.gmG2[e] = GemmEntry{Cn, d.T, gcur + (size_t)Np * K, K, Nf, Np, K, Np, K, -1.0, 1.0};
     b.gmG3[e] = GemmEntry{gcur, rinv, gnext, K, Nt, Nt, K, Nt, K, 1.0, 0.0};
-    b.gjS[e] = GjEntry{d.S, d.Sw, sinv, d.sigS, d.ridS, d.stS, Np, Np, Np, d.PS, d.sgS};
     b.gjR[e] = GjEntry{d.Ra, d.Rw, rinv, d.sigR, d.ridR, d.stR, Nt, Nt, Nt, d.PR, d.sgR};
 }
 
-// A = (1 + h^2 E / 6) I - h^2/6 V(n)  into S (SchurInverter.cpp:253-261)
-__global__ void k_init_S(BatchDev b) {
+// A = (1 + h^2 E / 6) I - h^2/6 V(n)  into Schur slot j (SchurInverter.cpp:253-261)
+__global__ void k_init_S(BatchDev b, int j) {
     const int e = blockIdx.y;
     const EnergyDev& d = b.ed[e];
     const int Np = d.Np;
     const long total = (long)Np * Np;
+    double* S = d.S + (size_t)j * total;
     for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
          idx += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(idx % Np), j = (int)(idx / Np);
-        const double diag = (i == j) ? d.c : 0.0;
-        d.S[idx] = diag - b.h2_6 * b.V[i + (size_t)j * b.Np_max];
+        const int i = (int)(idx % Np), jc = (int)(idx / Np);
+        const double diag = (i == jc) ? d.c : 0.0;
+        S[idx] = diag - b.h2_6 * b.V[i + (size_t)jc * b.Np_max];
     }
 }
 
@@ -210,31 +231,33 @@ __global__ void k_stab(BatchDev b, int n, int which) {
     const int e = blockIdx.x;
     EnergyDev& d = b.ed[e];
     const int Np = d.Np;
+    const int slot = n - b.cn0;
+    double* S = d.S + (size_t)slot * Np * Np;
     __shared__ double red[33];
     double g = INFINITY;
     for (int i = threadIdx.x; i < Np; i += blockDim.x) {
         double off = 0.0;
         for (int j = 0; j < Np; ++j)
-            if (j != i) off += fabs(d.S[i + (size_t)j * Np]);
-        g = fmin(g, d.S[i + (size_t)i * Np] - off);
+            if (j != i) off += fabs(S[i + (size_t)j * Np]);
+        g = fmin(g, S[i + (size_t)i * Np] - off);
     }
     const double gersh = block_min(g, red);
     if (threadIdx.x == 0) {
         double me;
         if (gersh > b.W_min + 0.05) me = gersh;
-        else me = (which == 0) ? d.c + d.lmA[n] : (d.c + d.deltaA) + d.lmS[n];
+        else me = (which == 0) ? d.c + d.lmA[n] : (d.c + d.deltaAc[slot]) + d.lmS[n];
         double delta = 0.0;
         if (me < b.W_min) {
             delta = b.W_min - me + b.margin;
             if (which == 0) d.shiftsA += 1; else d.shiftsS += 1;
         }
-        if (which == 0) d.deltaA = delta;
+        if (which == 0) d.deltaAc[slot] = delta;
         red[0] = delta;
     }
     __syncthreads();
     const double delta = red[0];
     if (delta != 0.0)
-        for (int i = threadIdx.x; i < Np; i += blockDim.x) d.S[i + (size_t)i * Np] += delta;
+        for (int i = threadIdx.x; i < Np; i += blockDim.x) S[i + (size_t)i * Np] += delta;
 }
 
 // S <- lower triangle mirrored (dsytrf/dsytri read only the LOWER triangle)
@@ -257,7 +280,7 @@ __global__ void k_assemble_R(BatchDev b, int n) {
     const int Np = d.Np, Nt = d.Nt, Nf = b.Nf;
     const bool exch = n < b.n_tr;
     const bool tail = n >= b.n_s;
-    const double* sinv = tail ? d.tailS + (size_t)(n - b.n_s) * Np * Np : d.Sinv;
+    const double* sinv = sinv_at(b, d, n);
     const int pm = n - 1;
     const double* prev = (pm >= b.n_s) ? d.tailR + (size_t)(pm - b.n_s) * Nt * Nt
                                        : ((pm & 1) ? d.Rinv1 : d.Rinv0);
@@ -335,7 +358,7 @@ __global__ void k_collect(BatchDev b, int n, int which) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= b.count) return;
     EnergyDev& d = b.ed[e];
-    const int st = which ? d.stR[0] : d.stS[0];
+    const int st = which ? d.stR[0] : d.stS[4 * (n - b.cn0)];
     if (st != 0 && d.err_code == 0) {
         d.err_code = (st == DEV_SINGULAR) ? SCATT_ERR_SINGULAR : SCATT_ERR_NONFINITE;
         d.err_step = n;
@@ -1027,12 +1050,14 @@ int make_shared(const ScanTables& t, const scatt_solve_opts& o, Batch& bt) {
     b.Ctab = t.Ctab.p;
     b.l_of_mu = t.d_l_of_mu.p;
     b.l_sigma = t.d_l_sigma.p;
-    SCATT_TRY(bt.V.alloc((size_t)t.Np_max * t.Np_max));
+    SCATT_TRY(bt.V.alloc((size_t)SCHUR_CHUNK * t.Np_max * t.Np_max));
     SCATT_TRY(bt.vdiag1.alloc(t.Np_max));
-    SCATT_TRY(bt.B.alloc((size_t)t.Np_max * std::max(1, t.Nf)));
-    SCATT_TRY(bt.Bs.alloc((size_t)t.Np_max * std::max(1, t.Nf)));
-    SCATT_TRY(bt.Dinv.alloc(std::max(1, t.Nf)));
+    SCATT_TRY(bt.B.alloc((size_t)SCHUR_CHUNK * t.Np_max * std::max(1, t.Nf)));
+    SCATT_TRY(bt.Bs.alloc((size_t)SCHUR_CHUNK * t.Np_max * std::max(1, t.Nf)));
+    SCATT_TRY(bt.Dinv.alloc((size_t)SCHUR_CHUNK * std::max(1, t.Nf)));
+    b.Vc = bt.V.p; b.Bc = bt.B.p; b.Bsc = bt.Bs.p; b.Dinvc = bt.Dinv.p;
     b.V = bt.V.p; b.vdiag1 = bt.vdiag1.p; b.B = bt.B.p; b.Bs = bt.Bs.p; b.Dinv = bt.Dinv.p;
+    b.cn0 = 0;
     return SCATT_OK;
 }
 
@@ -1112,9 +1137,10 @@ int ensure_stab(Context& ctx, const scatt_solve_opts& o, int l_cont, const doubl
 
 size_t energy_bytes(const BatchDev& b, int Np, int Nt, int nslots) {
     const size_t np2 = (size_t)Np * Np, nt2 = (size_t)Nt * Nt;
-    size_t d = 3 * np2 + (size_t)Np * b.Nf + (size_t)b.Nf * b.Nf + 4 * nt2 + 2 * (size_t)b.Krows * Nt;
+    size_t d = 3 * SCHUR_CHUNK * np2 + (size_t)Np * b.Nf + (size_t)b.Nf * b.Nf + 4 * nt2 +
+               2 * (size_t)b.Krows * Nt;
     d += (size_t)nslots * (nt2 + 2 * np2);
-    d += 4 * (size_t)64 * (Np + Nt);                 // two-level panel windows (two sets)
+    d += 4 * (size_t)64 * (SCHUR_CHUNK * (size_t)Np + Nt);   // two-level panel windows (two sets)
     d += 16 * 32;                                    // every buffer starts on a 256-byte boundary
     return d * sizeof(double);
 }
@@ -1180,7 +1206,7 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
     }
     SCATT_TRY(bt.arena.alloc(total));
     size_t itot = 0;
-    for (auto& d : bt.ed) itot += 6 * (size_t)(d.Np + d.Nt) + 8;
+    for (auto& d : bt.ed) itot += SCHUR_CHUNK * (6 * (size_t)d.Np + 4) + 6 * (size_t)d.Nt + 4;
     SCATT_TRY(bt.iarena.alloc(itot));
     SCATT_CUDA_TRY(cudaMemsetAsync(bt.iarena.p, 0, itot * sizeof(int), s));
     size_t ip = 0;
@@ -1190,9 +1216,9 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         double* p = bt.arena.p + off[e];
         // 256-byte aligned pieces (the inverse kernels copy 16-byte row pairs)
         auto take = [&p](size_t cnt) { double* r = p; p += (cnt + 31) & ~size_t(31); return r; };
-        d.S = take(np2);
-        d.Sw = take(np2);
-        d.Sinv = take(np2);
+        d.S = take(SCHUR_CHUNK * np2);
+        d.Sw = take(SCHUR_CHUNK * np2);
+        d.Sinv = take(SCHUR_CHUNK * np2);
         d.T = take((size_t)d.Np * Nf);
         d.F = take((size_t)Nf * Nf);
         d.Ra = take(nt2);
@@ -1204,27 +1230,28 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         d.tailR = take((size_t)nslots * nt2);
         d.tailS = take((size_t)nslots * np2);
         d.psiT = take((size_t)nslots * np2);
-        d.PS = take((size_t)4 * 64 * d.Np);
+        d.PS = take((size_t)SCHUR_CHUNK * 4 * 64 * d.Np);
         d.PR = take((size_t)4 * 64 * d.Nt);
         int* q = bt.iarena.p + ip;
-        d.sigS = q; q += d.Np;
-        d.ridS = q; q += d.Np;
+        d.sigS = q; q += SCHUR_CHUNK * d.Np;
+        d.ridS = q; q += SCHUR_CHUNK * d.Np;
         d.sigR = q; q += d.Nt;
         d.ridR = q; q += d.Nt;
-        d.stS = q; q += 4;
+        d.stS = q; q += SCHUR_CHUNK * 4;
         d.stR = q; q += 4;
-        d.sgS = q; q += 4 * d.Np;
+        d.sgS = q; q += SCHUR_CHUNK * 4 * d.Np;
         d.sgR = q; q += 4 * d.Nt;
-        ip += 6 * (size_t)(d.Np + d.Nt) + 8;
+        ip += SCHUR_CHUNK * (6 * (size_t)d.Np + 4) + 6 * (size_t)d.Nt + 4;
         SCATT_CUDA_TRY(cudaMemsetAsync(d.G0, 0, (size_t)K * d.Nt * sizeof(double), s));
     }
     SCATT_TRY(upload_vec(bt.d_ed, bt.ed, s));
     b.ed = bt.d_ed.p;
-    SCATT_TRY(bt.gm.alloc(6 * (size_t)count));
-    SCATT_TRY(bt.gj.alloc(2 * (size_t)count));
-    b.gmS = bt.gm.p; b.gmT = bt.gm.p + count; b.gmF = bt.gm.p + 2 * count;
-    b.gmG1 = bt.gm.p + 3 * count; b.gmG2 = bt.gm.p + 4 * count; b.gmG3 = bt.gm.p + 5 * count;
-    b.gjS = bt.gj.p; b.gjR = bt.gj.p + count;
+    SCATT_TRY(bt.gm.alloc((5 + SCHUR_CHUNK) * (size_t)count));
+    SCATT_TRY(bt.gj.alloc((1 + SCHUR_CHUNK) * (size_t)count));
+    b.gmT = bt.gm.p; b.gmF = bt.gm.p + count;
+    b.gmG1 = bt.gm.p + 2 * count; b.gmG2 = bt.gm.p + 3 * count; b.gmG3 = bt.gm.p + 4 * count;
+    b.gmS = bt.gm.p + 5 * count;                  // SCHUR_CHUNK x count
+    b.gjR = bt.gj.p; b.gjS = bt.gj.p + count;     // gjS: SCHUR_CHUNK x count
     int maxNp = 0, maxNt = 0;
     for (auto& d : bt.ed) { maxNp = std::max(maxNp, d.Np); maxNt = std::max(maxNt, d.Nt); }
 
@@ -1240,50 +1267,81 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         cudaEventCreate(&ev_end);
         cudaEventRecord(ev_begin, s);
     }
-    for (int n = 0; n <= N; ++n) {
-        k_prepare<<<cdiv(count, 128), 128, 0, s>>>(b, n);
-        SCATT_COUNT_LAUNCH(1);
-        launch_VB(b, n, s);
-        if (n < b.n_start) { k_vdiag<<<cdiv(b.Np_max, 128), 128, 0, s>>>(b, n + 1, b.vdiag1); SCATT_COUNT_LAUNCH(1); }
-        k_init_S<<<eg, TPB, 0, s>>>(b);
-        SCATT_COUNT_LAUNCH(1);
-        if (n < b.stab_n) { k_stab<<<count, TPB, 0, s>>>(b, n, 0); SCATT_COUNT_LAUNCH(1); }
-        const bool exch = n < b.n_tr && Nf > 0;
-        if (exch) SCATT_TRY(gemm_dev(bt, b.gmS, count, bt.ed, 0, 0, 1, s));
-        if (exch && n < b.stab_n) { k_stab<<<count, TPB, 0, s>>>(b, n, 1); SCATT_COUNT_LAUNCH(1); }
-        SCATT_TRY(gj_inverse_selected(b.gjS, count, maxNp, true, s, true));
-        k_collect<<<cdiv(count, 128), 128, 0, s>>>(b, n, 0);
-        SCATT_COUNT_LAUNCH(1);
-        if (exch) {
-            SCATT_TRY(gemm_dev(bt, b.gmT, count, bt.ed, 1, 0, 0, s));
-            SCATT_TRY(gemm_dev(bt, b.gmF, count, bt.ed, 2, 1, 0, s));
+    // BatchDev with the per-step buffers pointing at chunk slot j
+    auto slot = [&](int n0, int j) {
+        BatchDev bj = b;
+        const size_t sl = (size_t)b.Np_max * std::max(1, Nf);
+        bj.V = b.Vc + (size_t)j * b.Np_max * b.Np_max;
+        bj.B = b.Bc + (size_t)j * sl;
+        bj.Bs = b.Bsc + (size_t)j * sl;
+        bj.Dinv = b.Dinvc + (size_t)j * std::max(1, Nf);
+        bj.cn0 = n0;
+        return bj;
+    };
+    for (int n0 = 0; n0 <= N; n0 += SCHUR_CHUNK) {
+        const int C = std::min(SCHUR_CHUNK, N + 1 - n0);
+        // ---- Schur complements of the chunk's steps: A(n), S(n) = A - Bs B^T, one batched inverse
+        for (int j = 0; j < C; ++j) {
+            const int n = n0 + j;
+            const BatchDev bj = slot(n0, j);
+            launch_VB(bj, n, s);
+            k_init_S<<<eg, TPB, 0, s>>>(bj, j);
+            SCATT_COUNT_LAUNCH(1);
+            if (n < b.stab_n) { k_stab<<<count, TPB, 0, s>>>(bj, n, 0); SCATT_COUNT_LAUNCH(1); }
         }
-        if (n < b.n_start) {
-            k_analytic_R<<<eg, TPB, 0, s>>>(b, n);
+        {
+            BatchDev bc = b;
+            bc.cn0 = n0;
+            k_prepare_schur<<<cdiv(count * C, 128), 128, 0, s>>>(bc, C);
             SCATT_COUNT_LAUNCH(1);
-            k_analytic_R_diag<<<dim3(4, count), TPB, 0, s>>>(b, n);
+        }
+        // the exchange steps of a chunk are its leading ones (n < n_tr)
+        const int Cx = (Nf > 0) ? std::max(0, std::min(C, b.n_tr - n0)) : 0;
+        if (Cx > 0) SCATT_TRY(gemm_dev(bt, b.gmS, count * Cx, bt.ed, 0, 0, 1, s));
+        for (int j = 0; j < Cx; ++j)
+            if (n0 + j < b.stab_n) { k_stab<<<count, TPB, 0, s>>>(slot(n0, j), n0 + j, 1); SCATT_COUNT_LAUNCH(1); }
+        SCATT_TRY(gj_inverse_selected(b.gjS, count * C, maxNp, true, s, true));
+        // ---- the R-ratio recurrence over the chunk's steps
+        for (int j = 0; j < C; ++j) {
+            const int n = n0 + j;
+            const BatchDev bj = slot(n0, j);
+            k_prepare<<<cdiv(count, 128), 128, 0, s>>>(bj, n);
             SCATT_COUNT_LAUNCH(1);
-        } else {
-            k_assemble_R<<<eg, TPB, 0, s>>>(b, n);
+            if (n < b.n_start) { k_vdiag<<<cdiv(b.Np_max, 128), 128, 0, s>>>(bj, n + 1, b.vdiag1); SCATT_COUNT_LAUNCH(1); }
+            k_collect<<<cdiv(count, 128), 128, 0, s>>>(bj, n, 0);
             SCATT_COUNT_LAUNCH(1);
-            const bool sample = o.timing && (n % sample_every == 0);
-            if (sample) {
-                cudaEvent_t a0, a1;
-                cudaEventCreate(&a0);
-                cudaEventCreate(&a1);
-                rev.push_back(a0);
-                rev.push_back(a1);
-                cudaEventRecord(a0, s);
+            const bool exch = n < b.n_tr && Nf > 0;
+            if (exch) {
+                SCATT_TRY(gemm_dev(bt, b.gmT, count, bt.ed, 1, 0, 0, s));
+                SCATT_TRY(gemm_dev(bt, b.gmF, count, bt.ed, 2, 1, 0, s));
             }
-            SCATT_TRY(gj_inverse_selected(b.gjR, count, maxNt, true, s, true));
-            if (sample) cudaEventRecord(rev.back(), s);
-            k_collect<<<cdiv(count, 128), 128, 0, s>>>(b, n, 1);
-            SCATT_COUNT_LAUNCH(1);
-        }
-        if (n <= N - 1) {
-            if (n < b.n_pts) SCATT_TRY(gemm_dev(bt, b.gmG1, count, bt.ed, 3, 0, 0, s));
-            if (n < b.n_pts && exch) SCATT_TRY(gemm_dev(bt, b.gmG2, count, bt.ed, 4, 0, 0, s));
-            SCATT_TRY(gemm_dev(bt, b.gmG3, count, bt.ed, 5, 0, 0, s));
+            if (n < b.n_start) {
+                k_analytic_R<<<eg, TPB, 0, s>>>(bj, n);
+                SCATT_COUNT_LAUNCH(1);
+                k_analytic_R_diag<<<dim3(4, count), TPB, 0, s>>>(bj, n);
+                SCATT_COUNT_LAUNCH(1);
+            } else {
+                k_assemble_R<<<eg, TPB, 0, s>>>(bj, n);
+                SCATT_COUNT_LAUNCH(1);
+                const bool sample = o.timing && (n % sample_every == 0);
+                if (sample) {
+                    cudaEvent_t a0, a1;
+                    cudaEventCreate(&a0);
+                    cudaEventCreate(&a1);
+                    rev.push_back(a0);
+                    rev.push_back(a1);
+                    cudaEventRecord(a0, s);
+                }
+                SCATT_TRY(gj_inverse_selected(b.gjR, count, maxNt, true, s, true));
+                if (sample) cudaEventRecord(rev.back(), s);
+                k_collect<<<cdiv(count, 128), 128, 0, s>>>(bj, n, 1);
+                SCATT_COUNT_LAUNCH(1);
+            }
+            if (n <= N - 1) {
+                if (n < b.n_pts) SCATT_TRY(gemm_dev(bt, b.gmG1, count, bt.ed, 3, 0, 0, s));
+                if (n < b.n_pts && exch) SCATT_TRY(gemm_dev(bt, b.gmG2, count, bt.ed, 4, 0, 0, s));
+                SCATT_TRY(gemm_dev(bt, b.gmG3, count, bt.ed, 5, 0, 0, s));
+            }
         }
     }
     SCATT_CUDA_TRY(cudaGetLastError());
