@@ -115,19 +115,47 @@ def U_real_to_complex(mR: int, mC: int) -> complex:
     return 0j
 
 
+def m3_candidates(m1: int, m2: int, l3: int):
+    """Real-harmonic m3 with a possibly nonzero real Gaunt coefficient for
+    (m1, m2): |m3| = |m1| + |m2| or ||m1| - |m2||; every other m3 gives exactly 0
+    (no complex m-triple sums to zero).  Ascending, within |m3| <= l3."""
+    a, b = abs(m1), abs(m2)
+    mags = {a + b, abs(a - b)}
+    out = set()
+    for x in mags:
+        if x <= l3:
+            out.add(x)
+            out.add(-x)
+    return sorted(out)
+
+
+def _m_candidates(mR: int):
+    """Complex m values with U_real_to_complex(mR, m) != 0, ascending."""
+    a = abs(mR)
+    return (0,) if a == 0 else (-a, a)
+
+
 @lru_cache(maxsize=1 << 22)
 def gaunt_real(l1, mR1, l2, mR2, l3, mR3) -> float:
-    """Gaunt.hpp:114-135 -- integral of three real spherical harmonics."""
+    """Gaunt.hpp:114-135 -- integral of three real spherical harmonics.
+
+    The reference sums over every (m1, m2) with m3 = -(m1 + m2); only
+    m = +-|mR| carry a nonzero U coefficient, so the loops visit exactly those
+    (in the same ascending order, hence the same accumulation order)."""
     if abs(l1 - l2) > l3 or l1 + l2 < l3:
         return 0.0
     if (l1 + l2 + l3) & 1:
         return 0.0
     acc = 0j
-    for m1 in range(-l1, l1 + 1):
+    for m1 in _m_candidates(mR1):
+        if m1 < -l1 or m1 > l1:
+            continue
         U1 = U_real_to_complex(mR1, m1)
         if U1 == 0:
             continue
-        for m2 in range(-l2, l2 + 1):
+        for m2 in _m_candidates(mR2):
+            if m2 < -l2 or m2 > l2:
+                continue
             U2 = U_real_to_complex(mR2, m2)
             if U2 == 0:
                 continue
@@ -200,7 +228,8 @@ def build_G_vector(n_mu: int, n_lambda: int, n_sigma: int):
     """WavefunctionSetup.cpp:21-81 -- non-zero G^R_{mu,lambda,sigma} (|G| > 1e-14).
 
     Enumerates only the (l, m) combinations the selection rules allow
-    (triangle, parity); the values and the 1e-14 cut are the reference's.
+    (triangle, parity, |m_sigma| = |m_mu| +- |m_lambda|); the values and the
+    1e-14 cut are the reference's.
     Returns a list of (mu, lambda, sigma, value) sorted by (mu, lambda, sigma).
     """
     lmax_mu = idx_to_lm(n_mu - 1)[0]
@@ -217,7 +246,7 @@ def build_G_vector(n_mu: int, n_lambda: int, n_sigma: int):
                     la = lm_to_idx(ll, ml)
                     if la >= n_lambda:
                         continue
-                    for ms in range(-ls, ls + 1):
+                    for ms in m3_candidates(mm, ml, ls):
                         si = lm_to_idx(ls, ms)
                         if si >= n_sigma:
                             continue

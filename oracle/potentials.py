@@ -93,7 +93,7 @@ def gaunt_pairs(l_cont: int):
             for ls in range(abs(l1 - l2), min(l1 + l2, l_exp) + 1):
                 if (l1 + ls + l2) & 1:
                     continue
-                for ms in range(-ls, ls + 1):
+                for ms in angular.m3_candidates(m1, m2, ls):
                     G = angular.gaunt_real(l2, m2, ls, ms, l1, m1)
                     if abs(G) > 1e-15:
                         rows.append((mu_p, mu))

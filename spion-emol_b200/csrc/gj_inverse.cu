@@ -170,447 +170,14 @@ gj_panel_kernel(const GjEntry* __restrict__ entries, int kb) {
     if (tid == 0) e.status[0] = s_status;
 }
 
-// Register-resident panel: thread t owns rows t, t + 512, ... (R rows) and
-// keeps their 16 panel entries in registers; only the pivot row travels
-// through shared memory.  Two barriers per pivot.
-template <int R>
-__global__ void __launch_bounds__(PANEL_THREADS)
-gj_panel_reg_kernel(const GjEntry* __restrict__ entries, int kb) {
-    const GjEntry e = entries[blockIdx.x];
-    const int n = e.n;
-    const int k0 = kb * NB;
-    if (k0 >= n) return;
-    const int nb = min(NB, n - k0);
-    const double* src = buf_of(e, kb & 1);
-    double* dst = buf_of(e, (kb + 1) & 1);
-
-    extern __shared__ double smem[];
-    int* loc = reinterpret_cast<int*>(smem);
-    int* rid = loc + n;
-    __shared__ double red_v[2][PANEL_WARPS];
-    __shared__ int red_i[2][PANEL_WARPS];
-    __shared__ double prow[2][NB];     // pivot row p before the interchange
-    __shared__ double krow[2][NB];     // row k before the interchange
-    __shared__ int s_status;
-
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double v[R][NB];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int i = tid + r * PANEL_THREADS;
-#pragma unroll
-        for (int j = 0; j < NB; ++j)
-            v[r][j] = (i < n && j < nb) ? src[i + (size_t)(k0 + j) * e.ld] : 0.0;
-    }
-    for (int i = tid; i < n; i += PANEL_THREADS) {
-        loc[i] = i;
-        rid[i] = (kb == 0) ? i : e.rowid[i];
-    }
-    if (tid == 0) s_status = (kb == 0) ? 0 : e.status[0];
-    __syncthreads();
-
-#pragma unroll
-    for (int j = 0; j < NB; ++j) {
-        if (j < nb) {
-            const int k = k0 + j;
-            const int par = j & 1;
-            double bv = -1.0;
-            int bi = -1;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = tid + r * PANEL_THREADS;
-                if (i >= k && i < n) {
-                    const double a = fabs(v[r][j]);
-                    if (a > bv) { bv = a; bi = i; }
-                }
-            }
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const double ov = __shfl_down_sync(0xffffffffu, bv, off);
-                const int oi = __shfl_down_sync(0xffffffffu, bi, off);
-                better(bv, bi, ov, oi);
-            }
-            if (lane == 0) { red_v[par][warp] = bv; red_i[par][warp] = bi; }
-            __syncthreads();
-            // every thread reduces the 16 warp winners itself (no second round trip)
-            bv = -1.0;
-            bi = -1;
-#pragma unroll
-            for (int w = 0; w < PANEL_WARPS; ++w) better(bv, bi, red_v[par][w], red_i[par][w]);
-            int p = bi;
-            if (p < 0) p = k;
-            if (tid == 0) {
-                int st = 0;
-                if (bi < 0 || !(bv < INFINITY)) st = DEV_NONFINITE;
-                else if (bv == 0.0) st = DEV_SINGULAR;
-                if (st && s_status == 0) { s_status = st; e.status[1] = k; }
-                if (p != k) {
-                    const int a = loc[k]; loc[k] = loc[p]; loc[p] = a;
-                    const int b = rid[k]; rid[k] = rid[p]; rid[p] = b;
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = tid + r * PANEL_THREADS;
-                if (i == p) {
-#pragma unroll
-                    for (int jj = 0; jj < NB; ++jj) prow[par][jj] = v[r][jj];
-                }
-                if (i == k) {
-#pragma unroll
-                    for (int jj = 0; jj < NB; ++jj) krow[par][jj] = v[r][jj];
-                }
-            }
-            __syncthreads();
-            double piv = prow[par][j];
-            if (piv == 0.0) piv = 1.0;             // the status word records the failure
-            const double inv = 1.0 / piv;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = tid + r * PANEL_THREADS;
-                if (i >= n) continue;
-                if (i == k) {
-#pragma unroll
-                    for (int jj = 0; jj < NB; ++jj) v[r][jj] = (jj == j) ? inv : prow[par][jj] * inv;
-                    continue;
-                }
-                if (i == p) {
-#pragma unroll
-                    for (int jj = 0; jj < NB; ++jj) v[r][jj] = krow[par][jj];
-                }
-                const double f = v[r][j];
-#pragma unroll
-                for (int jj = 0; jj < NB; ++jj)
-                    if (jj != j) v[r][jj] -= f * (prow[par][jj] * inv);
-                v[r][j] = -f * inv;
-            }
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int i = tid + r * PANEL_THREADS;
-        if (i < n) {
-#pragma unroll
-            for (int j = 0; j < NB; ++j)
-                if (j < nb) dst[i + (size_t)(k0 + j) * e.ld] = v[r][j];
-        }
-    }
-    for (int i = tid; i < n; i += PANEL_THREADS) {
-        e.sigma[i] = loc[i];
-        e.rowid[i] = rid[i];
-    }
-    if (tid == 0) e.status[0] = s_status;
-}
-
-// Panel v3: 1024 threads, two threads per row (8 panel columns each, in
-// registers), rows tid/2 + 512 r for r < R (n <= 1536).  The pivot search is
-// a shuffle reduction (per warp, then once more over the 32 warp winners);
-// the pivot row travels through shared memory.  Two barriers per pivot.
-constexpr int P3_THREADS = 1024;
-
+// (|value|, index) key comparison: larger magnitude wins, ties go to the
+// smaller index, NaN never wins.
 __device__ __forceinline__ void better_key(double& v, int& i, double v2, int i2) {
     if (v2 > v || (v2 == v && i2 >= 0 && (i < 0 || i2 < i))) { v = v2; i = i2; }
 }
 
-template <int QW, int R>
-__global__ void __launch_bounds__(P3_THREADS, 1)
-gj_panel3_kernel(const GjEntry* __restrict__ entries, int kb) {
-    constexpr int CW = NB / QW;                 // panel columns per thread
-    constexpr int RPP = P3_THREADS / QW;        // rows per pass
-    const GjEntry e = entries[blockIdx.x];
-    const int n = e.n;
-    const int k0 = kb * NB;
-    if (k0 >= n) return;
-    const int nb = min(NB, n - k0);
-    const double* src = buf_of(e, kb & 1);
-    double* dst = buf_of(e, (kb + 1) & 1);
-
-    extern __shared__ double smem[];
-    int* loc = reinterpret_cast<int*>(smem);
-    int* rid = loc + n;
-    __shared__ double red_v[2][32];
-    __shared__ int red_i[2][32];
-    __shared__ double prow[2][NB];
-    __shared__ double krow[2][NB];
-    __shared__ int s_status;
-
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int q = tid / QW, h = tid % QW;       // row slot, column group
-    const int cbase = CW * h;
-    double v[R][CW];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int i = q + r * RPP;
-#pragma unroll
-        for (int c = 0; c < CW; ++c) {
-            const int j = cbase + c;
-            v[r][c] = (i < n && j < nb) ? src[i + (size_t)(k0 + j) * e.ld] : 0.0;
-        }
-    }
-    for (int i = tid; i < n; i += P3_THREADS) {
-        loc[i] = i;
-        rid[i] = (kb == 0) ? i : e.rowid[i];
-    }
-    if (tid == 0) s_status = (kb == 0) ? 0 : e.status[0];
-    __syncthreads();
-
-#pragma unroll 1
-    for (int j = 0; j < nb; ++j) {
-        const int k = k0 + j;
-        const int par = j & 1;
-        const int hj = j / CW, cj = j % CW;
-        // ---- pivot search over rows [k, n) of column j
-        double bv = -1.0;
-        int bi = -1;
-        if (h == hj) {
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = q + r * RPP;
-                double x = 0.0;
-#pragma unroll
-                for (int c = 0; c < CW; ++c) if (c == cj) x = v[r][c];
-                if (i >= k && i < n) {
-                    const double a = fabs(x);
-                    if (a > bv) { bv = a; bi = i; }
-                }
-            }
-        }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-            better_key(bv, bi, ov, oi);
-        }
-        if (lane == 0) { red_v[par][warp] = bv; red_i[par][warp] = bi; }
-        __syncthreads();
-        bv = red_v[par][lane];
-        bi = red_i[par][lane];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-            better_key(bv, bi, ov, oi);
-        }
-        const int p = bi < 0 ? k : bi;
-        if (tid == 0) {
-            int st = 0;
-            if (bi < 0 || !(bv < INFINITY)) st = DEV_NONFINITE;
-            else if (bv == 0.0) st = DEV_SINGULAR;
-            if (st && s_status == 0) { s_status = st; e.status[1] = k; }
-            if (p != k) {
-                const int a = loc[k]; loc[k] = loc[p]; loc[p] = a;
-                const int b2 = rid[k]; rid[k] = rid[p]; rid[p] = b2;
-            }
-        }
-        // ---- publish rows p and k
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int i = q + r * RPP;
-            if (i == p) {
-#pragma unroll
-                for (int c = 0; c < CW; ++c) prow[par][cbase + c] = v[r][c];
-            }
-            if (i == k) {
-#pragma unroll
-                for (int c = 0; c < CW; ++c) krow[par][cbase + c] = v[r][c];
-            }
-        }
-        __syncthreads();
-        double piv = prow[par][j];
-        if (piv == 0.0) piv = 1.0;              // the status word records the failure
-        const double inv = 1.0 / piv;
-        double sp[CW];
-#pragma unroll
-        for (int c = 0; c < CW; ++c) sp[c] = prow[par][cbase + c] * inv;
-        const int owner = (lane & ~(QW - 1)) | hj;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int i = q + r * RPP;
-            double mine = 0.0;
-#pragma unroll
-            for (int c = 0; c < CW; ++c) if (c == cj) mine = v[r][c];
-            double f = __shfl_sync(0xffffffffu, mine, owner);
-            if (i >= n) continue;
-            if (i == k) {
-#pragma unroll
-                for (int c = 0; c < CW; ++c) v[r][c] = (cbase + c == j) ? inv : sp[c];
-                continue;
-            }
-            if (i == p) {
-#pragma unroll
-                for (int c = 0; c < CW; ++c) v[r][c] = krow[par][cbase + c];
-                f = krow[par][j];
-            }
-#pragma unroll
-            for (int c = 0; c < CW; ++c) {
-                if (cbase + c == j) v[r][c] = -f * inv;
-                else v[r][c] -= f * sp[c];
-            }
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int i = q + r * RPP;
-        if (i < n) {
-#pragma unroll
-            for (int c = 0; c < CW; ++c) {
-                const int j = cbase + c;
-                if (j < nb) dst[i + (size_t)(k0 + j) * e.ld] = v[r][c];
-            }
-        }
-    }
-    for (int i = tid; i < n; i += P3_THREADS) {
-        e.sigma[i] = loc[i];
-        e.rowid[i] = rid[i];
-    }
-    if (tid == 0) e.status[0] = s_status;
-}
-
-// Panel v4: W warps (32 W threads, W = ceil(n / 128)), each thread owns up
-// to R = 4 rows tid + 32 W r with all 16 panel columns in registers.  The
-// pivot loop is fully unrolled, so every register index is static; the
-// owner of the pivot row publishes it already scaled by 1/pivot.
-template <int R, int MAXT>
-__global__ void __launch_bounds__(MAXT, 1)
-gj_panel4_kernel(const GjEntry* __restrict__ entries, int kb) {
-    const GjEntry e = entries[blockIdx.x];
-    const int n = e.n;
-    const int k0 = kb * NB;
-    if (k0 >= n) return;
-    const int nb = min(NB, n - k0);
-    const double* src = buf_of(e, kb & 1);
-    double* dst = buf_of(e, (kb + 1) & 1);
-    const int T = blockDim.x, W = T >> 5;
-
-    extern __shared__ double smem[];
-    int* loc = reinterpret_cast<int*>(smem);
-    int* rid = loc + n;
-    __shared__ double red_v[2][32];
-    __shared__ int red_i[2][32];
-    __shared__ double sprow[2][NB];      // new pivot row: row p scaled by 1/pivot
-    __shared__ double krow[2][NB];       // row k before the interchange
-    __shared__ int s_status;
-
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double v[R][NB];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int i = tid + r * T;
-#pragma unroll
-        for (int j = 0; j < NB; ++j)
-            v[r][j] = (i < n && j < nb) ? src[i + (size_t)(k0 + j) * e.ld] : 0.0;
-    }
-    for (int i = tid; i < n; i += T) {
-        loc[i] = i;
-        rid[i] = (kb == 0) ? i : e.rowid[i];
-    }
-    if (tid == 0) s_status = (kb == 0) ? 0 : e.status[0];
-    __syncthreads();
-
-#pragma unroll
-    for (int j = 0; j < NB; ++j) {
-        if (j < nb) {
-            const int k = k0 + j;
-            const int par = j & 1;
-            double bv = -1.0;
-            int bi = -1;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = tid + r * T;
-                if (i >= k && i < n) {
-                    const double a = fabs(v[r][j]);
-                    if (a > bv) { bv = a; bi = i; }
-                }
-            }
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-                better_key(bv, bi, ov, oi);
-            }
-            if (lane == 0) { red_v[par][warp] = bv; red_i[par][warp] = bi; }
-            __syncthreads();
-            bv = (lane < W) ? red_v[par][lane] : -1.0;
-            bi = (lane < W) ? red_i[par][lane] : -1;
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-                better_key(bv, bi, ov, oi);
-            }
-            const int p = bi < 0 ? k : bi;
-            if (tid == 0) {
-                int st = 0;
-                if (bi < 0 || !(bv < INFINITY)) st = DEV_NONFINITE;
-                else if (bv == 0.0) st = DEV_SINGULAR;
-                if (st && s_status == 0) { s_status = st; e.status[1] = k; }
-                if (p != k) {
-                    const int a = loc[k]; loc[k] = loc[p]; loc[p] = a;
-                    const int b2 = rid[k]; rid[k] = rid[p]; rid[p] = b2;
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = tid + r * T;
-                if (i == p) {
-                    double piv = v[r][j];
-                    if (piv == 0.0) piv = 1.0;      // the status word records the failure
-                    const double inv = 1.0 / piv;
-#pragma unroll
-                    for (int c = 0; c < NB; ++c) sprow[par][c] = (c == j) ? inv : v[r][c] * inv;
-                }
-                if (i == k) {
-#pragma unroll
-                    for (int c = 0; c < NB; ++c) krow[par][c] = v[r][c];
-                }
-            }
-            __syncthreads();
-            const double inv = sprow[par][j];
-            const double* sp = sprow[par];
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = tid + r * T;
-                if (i < n) {
-                    if (i == k) {
-#pragma unroll
-                        for (int c = 0; c < NB; ++c) v[r][c] = sp[c];
-                    } else {
-                        if (i == p) {
-#pragma unroll
-                            for (int c = 0; c < NB; ++c) v[r][c] = krow[par][c];
-                        }
-                        const double f = v[r][j];
-#pragma unroll
-                        for (int c = 0; c < NB; ++c) {
-                            if (c == j) v[r][c] = -f * inv;
-                            else v[r][c] -= f * sp[c];
-                        }
-                    }
-                }
-            }
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int i = tid + r * T;
-        if (i < n) {
-#pragma unroll
-            for (int j = 0; j < NB; ++j)
-                if (j < nb) dst[i + (size_t)(k0 + j) * e.ld] = v[r][j];
-        }
-    }
-    for (int i = tid; i < n; i += T) {
-        e.sigma[i] = loc[i];
-        e.rowid[i] = rid[i];
-    }
-    if (tid == 0) e.status[0] = s_status;
-}
-
-// Panel v5: as v4 (W warps, R rows of 16 columns per thread in registers)
-// but with a rolled pivot loop: after each pivot the register window is
+// Single-level panel: W warps, R rows of 16 columns per thread in registers,
+// with a rolled pivot loop: after each pivot the register window is
 // rotated by one column, so the active column is always v[r][0] and every
 // index stays static while the loop body stays small (instruction-cache
 // resident).  Shared rows (scaled pivot row, old row k) are kept in the same
@@ -758,7 +325,7 @@ gj_panel5_kernel(const GjEntry* __restrict__ entries, int kb) {
     if (tid == 0) e.status[0] = s_status;
 }
 
-constexpr int UBM = 64, UBN = 64, UPAD = 4, UTHREADS = 128;
+constexpr int UBM = 64;
 
 __device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1, double b0) {
     asm volatile(
@@ -1012,7 +579,6 @@ gj2_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub, int la) {
     for (int r = 0; r < R; ++r) {
         const int i = tid + r * T;
         const bool ok = i < n;
-#pragma unroll
         if (RM && vrow) {
             // 16 contiguous doubles of row i in 16-byte pairs
             const double2* rp = reinterpret_cast<const double2*>(src + i * rs + cs);
@@ -1272,116 +838,6 @@ gj2_narrow_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
         const int row = idx & 63, col = idx >> 6;
         const int gi = r0 + row;
         if (gi < n && col < nb64 && !(col >= cs && col < cs + nb)) dst[gi + (size_t)col * e.ld] = Cs[col][row];
-    }
-}
-
-// rank-64 update of every column outside the window; the window tile itself
-// is copied from the transformed window
-constexpr int T3S = 68;
-constexpr size_t TRAIL_SMEM = (64 * U2S + 2 * 64 * T3S) * sizeof(double);
-
-__global__ void __launch_bounds__(U2T)
-gj2_trail_kernel(const GjEntry* __restrict__ entries, int K) {
-    const GjEntry e = entries[blockIdx.z];
-    const int n = e.n;
-    const int k0 = K * OB;
-    if (k0 >= n) return;
-    const int nb64 = min(OB, n - k0);
-    const int nsub = (nb64 + NB - 1) / NB;
-    const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
-    if (r0 >= n || c0 >= n) return;
-    const double* src = buf_of(e, K & 1);
-    double* dst = buf_of(e, (K + 1) & 1);
-    const double* Mw = e.P + (size_t)(nsub & 1) * e.ld * OB;     // final window
-    const int* st = e.sigt + (size_t)(nsub & 1) * n;
-    const int tid = threadIdx.x;
-    if (c0 == k0) {          // the window itself
-        for (int idx = tid; idx < 64 * 64; idx += U2T) {
-            const int row = idx & 63, col = idx >> 6;
-            const int gi = r0 + row;
-            if (gi < n && col < nb64) dst[gi + (size_t)(c0 + col) * e.ld] = Mw[gi + (size_t)col * e.ld];
-        }
-        return;
-    }
-    extern __shared__ double u2smem[];
-    double (*Cs)[U2S] = reinterpret_cast<double (*)[U2S]>(u2smem);
-    double (*Ms)[T3S] = reinterpret_cast<double (*)[T3S]>(u2smem + 64 * U2S);          // Ms[j][m]
-    double (*Xs)[T3S] = reinterpret_cast<double (*)[T3S]>(u2smem + 64 * U2S + 64 * T3S); // Xs[j][c]
-    __shared__ int srow[64];
-    __shared__ int xrow[64];
-    if (tid < 64) srow[tid] = (r0 + tid < n) ? st[r0 + tid] : 0;
-    else if (tid < 128) {
-        const int j = tid - 64;
-        xrow[j] = (j < nb64) ? st[k0 + j] : 0;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < 16; ++u) {
-        const int idx = tid + u * U2T;
-        const int row = idx & 63, col = idx >> 6;
-        const int gi = r0 + row, gc = c0 + col;
-        const bool ok = gi < n && gc < n && !(gi >= k0 && gi < k0 + nb64);
-        cp_async8(&Cs[col][row], src + (ok ? srow[row] + (size_t)gc * e.ld : 0), ok);
-    }
-#pragma unroll
-    for (int u = 0; u < 16; ++u) {
-        const int idx = tid + u * U2T;
-        const int m = idx & 63, j = idx >> 6;
-        const int gi = r0 + m;
-        const bool ok = j < nb64 && gi < n;
-        cp_async8(&Ms[j][m], Mw + (ok ? gi + (size_t)j * e.ld : 0), ok);
-    }
-#pragma unroll
-    for (int u = 0; u < 16; ++u) {
-        const int idx = tid + u * U2T;
-        const int j = idx & 63, c = idx >> 6;
-        const int gc = c0 + c;
-        const bool ok = j < nb64 && gc < n;
-        cp_async8(&Xs[j][c], src + (ok ? xrow[j] + (size_t)gc * e.ld : 0), ok);
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    const int lane = tid & 31, warp = tid >> 5;
-    const int g = lane >> 2, t = lane & 3;
-    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
-    double acc[2][2][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int jn = 0; jn < 2; ++jn)
-#pragma unroll
-            for (int v = 0; v < 4; ++v)
-                acc[i][jn][v] = Cs[wn + jn * 8 + 2 * t + (v & 1)][wm + i * 16 + g + ((v >> 1) << 3)];
-#pragma unroll 4
-    for (int kk = 0; kk < OB; kk += 4) {
-        double a[2][2], b[2];
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            a[i][0] = Ms[kk + t][wm + i * 16 + g];
-            a[i][1] = Ms[kk + t][wm + i * 16 + g + 8];
-        }
-#pragma unroll
-        for (int jn = 0; jn < 2; ++jn) b[jn] = Xs[kk + t][wn + jn * 8 + g];
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-            for (int jn = 0; jn < 2; ++jn) dmma_16x8x4(acc[i][jn], a[i][0], a[i][1], b[jn]);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int jn = 0; jn < 2; ++jn)
-#pragma unroll
-            for (int v = 0; v < 4; ++v)
-                Cs[wn + jn * 8 + 2 * t + (v & 1)][wm + i * 16 + g + ((v >> 1) << 3)] = acc[i][jn][v];
-    __syncthreads();
-#pragma unroll 4
-    for (int u = 0; u < 16; ++u) {
-        const int idx = tid + u * U2T;
-        const int row = idx & 63, col = idx >> 6;
-        const int gi = r0 + row, gc = c0 + col;
-        if (gi < n && gc < n) dst[gi + (size_t)gc * e.ld] = Cs[col][row];
     }
 }
 
@@ -1961,8 +1417,6 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax, bool sy
     if (!attr2) {
         SCATT_CUDA_TRY(cudaFuncSetAttribute(gj2_narrow_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)U2_SMEM));
-        SCATT_CUDA_TRY(cudaFuncSetAttribute(gj2_trail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)TRAIL_SMEM));
         attr2 = true;
     }
     const int outer = (nmax + OB - 1) / OB;
