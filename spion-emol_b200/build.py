@@ -1,9 +1,10 @@
-"""Build libscatt_b200.so (sm_100a) in-tree with nvcc.
+"""Build libscatt_b200.so (sm_100a) in-tree with nvcc, and the C++ host driver.
 
     python spion-emol_b200/build.py [--force] [-j N]
 
 Objects go to spion-emol_b200/_build/; the shared library lands next to this
-file so it travels with the source tree.
+file so it travels with the source tree.  host/scan_driver (the command-line
+use of host/scatt_b200.hpp) links against it with an $ORIGIN-relative rpath.
 """
 from __future__ import annotations
 
@@ -20,6 +21,8 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libscatt_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
+HOST = os.path.join(HERE, "host")
+DRIVER = os.path.join(HOST, "scan_driver")
 
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -81,7 +84,22 @@ def build(force: bool = False, jobs: int = 8, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    build_host(force)
     return LIB
+
+
+def build_host(force: bool = False) -> str:
+    """g++ build of host/scan_driver against the in-tree library."""
+    src = os.path.join(HOST, "scan_driver.cpp")
+    deps = [src, os.path.join(HOST, "scatt_b200.hpp"), os.path.join(INCLUDE, "scatt_b200.h"), LIB]
+    if not force and os.path.exists(DRIVER) and os.path.getmtime(DRIVER) >= max(os.path.getmtime(d) for d in deps):
+        return DRIVER
+    cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-I", INCLUDE, "-I", HOST, src, "-o", DRIVER,
+           "-L", HERE, "-lscatt_b200", "-Wl,-rpath,$ORIGIN/.."]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"host driver build failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return DRIVER
 
 
 if __name__ == "__main__":
