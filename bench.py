@@ -46,6 +46,12 @@ CONFIGS = {
 }
 
 
+# DRAM bytes (read + write) of one batched R^-1 inversion, summed over its
+# kernels from an ncu launch-list capture of the same call
+# (profiles/gj_inverse_n1046_b32.md); algorithmic minimum ~10.1 GB.
+INVERSE_TRAFFIC = {(1046, 32): 11.21e9}
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -276,7 +282,8 @@ def main():
                     "d2h_bytes_per_step": out_bytes},
             "gpu_launches": int(launches),
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": (achieved / peak) if (achieved and peak) else None, "traffic": None,
+                         "frac": (achieved / peak) if (achieved and peak) else None,
+                         "traffic": INVERSE_TRAFFIC.get((Nt, B)),
                          "kernel": f"batched R^-1 (Gauss-Jordan, N_t={Nt}, batch {B}); "
                                    "peak = cuBLAS DGEMM 8192^3 measured in this run (FP64 of measured)"},
             "clocks": ck,
