@@ -260,19 +260,6 @@ __global__ void k_stab(BatchDev b, int n, int which) {
         for (int i = threadIdx.x; i < Np; i += blockDim.x) S[i + (size_t)i * Np] += delta;
 }
 
-// S <- lower triangle mirrored (dsytrf/dsytri read only the LOWER triangle)
-__global__ void k_mirror(BatchDev b) {
-    const int e = blockIdx.y;
-    const EnergyDev& d = b.ed[e];
-    const int Np = d.Np;
-    const long total = (long)Np * Np;
-    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
-         idx += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(idx % Np), j = (int)(idx / Np);
-        if (i < j) d.S[idx] = d.S[j + (size_t)i * Np];
-    }
-}
-
 // R = 12 W^-1 - 10 I - Rinv_prev, W^-1 = [[Sinv, -T], [-T^T, D^-1 + F]]
 __global__ void k_assemble_R(BatchDev b, int n) {
     const int e = blockIdx.y;
