@@ -66,6 +66,10 @@ struct GemmEntry {
     int M, N, K;
     int lda, ldb, ldc;
     double alpha, beta;
+    // 1: op(A) op(B) is symmetric (M == N) and C starts symmetric: only the
+    // lower-triangle tiles are computed and each result is mirrored, so C
+    // comes out exactly symmetric
+    int sym = 0;
 };
 
 // opA / opB: 0 = no transpose, 1 = transpose.  `entries` is a DEVICE array.

@@ -7,6 +7,9 @@
 // tile's tensor-core work.  Transposes are resolved at load time (opA, opB
 // template flags), so A^T B, A B^T, ... need no extra pass.
 //
+// Entries flagged sym (a symmetric product added to a symmetric C) compute
+// only the lower-triangle tiles and mirror each result.
+//
 // This is the contraction engine behind the Schur complement
 // S = A - (B D^-1) B^T, the W^-1 blocks (Sinv B, B^T Sinv B), the dipole /
 // overlap row sweeps and the outer-region products.
@@ -34,6 +37,8 @@ gemm_kernel(const GemmEntry* __restrict__ entries) {
     const int m0 = blockIdx.x * BM;
     const int n0 = blockIdx.y * BN;
     if (m0 >= e.M || n0 >= e.N) return;
+    const bool sym = e.sym != 0;
+    if (sym && n0 > m0) return;                 // strictly upper tiles come from the mirror
 
     __shared__ double As[2][BK][BM + PAD];
     __shared__ double Bs[2][BK][BN + PAD];
@@ -133,11 +138,12 @@ gemm_kernel(const GemmEntry* __restrict__ entries) {
             for (int v = 0; v < 4; ++v) {
                 const int row = m0 + wm + i * 16 + g + ((v >> 1) << 3);
                 const int col = n0 + wn + j * 8 + 2 * t + (v & 1);
-                if (row < e.M && col < e.N) {
+                if (row < e.M && col < e.N && !(sym && col > row)) {
                     double* c = e.C + row + (size_t)col * e.ldc;
                     double r = e.alpha * acc[i][j][v];
                     if (e.beta != 0.0) r += e.beta * *c;
                     *c = r;
+                    if (sym && col != row) e.C[col + (size_t)row * e.ldc] = r;
                 }
             }
 }

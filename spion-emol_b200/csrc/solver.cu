@@ -167,7 +167,8 @@ __global__ void k_prepare_schur(BatchDev b, int C) {
     const int Np = d.Np, Nf = b.Nf;
     const size_t np2 = (size_t)Np * Np, sl = (size_t)b.Np_max * Nf;
     double* S = d.S + j * np2;
-    b.gmS[idx] = GemmEntry{b.Bsc + j * sl, b.Bc + j * sl, S, Np, Np, Nf, b.Np_max, b.Np_max, Np, -1.0, 1.0};
+    // Bs B^T = B D^-1 B^T and A are symmetric: lower tiles only, mirrored
+    b.gmS[idx] = GemmEntry{b.Bsc + j * sl, b.Bc + j * sl, S, Np, Np, Nf, b.Np_max, b.Np_max, Np, -1.0, 1.0, 1};
     b.gjS[idx] = GjEntry{S, d.Sw + j * np2, sinv_at(b, d, b.cn0 + j), d.sigS + (size_t)j * Np,
                          d.ridS + (size_t)j * Np, d.stS + 4 * j, Np, Np, Np,
                          d.PS + (size_t)j * 4 * 64 * Np, d.sgS + (size_t)j * 4 * Np};
@@ -186,7 +187,8 @@ __global__ void k_prepare(BatchDev b, int n) {
     double* gnext = (n & 1) ? d.G0 : d.G1;
     const double* Cn = (n < b.n_pts) ? b.Ctab + (size_t)n * K * b.Np_max : nullptr;
     b.gmT[e] = GemmEntry{sinv, b.Bs, d.T, Np, Nf, Np, Np, b.Np_max, Np, 1.0, 0.0};
-    b.gmF[e] = GemmEntry{b.Bs, d.T, d.F, Nf, Nf, Np, b.Np_max, Np, Nf, 1.0, 0.0};
+    // F = Bs^T Sinv Bs is symmetric: lower tiles only, mirrored
+    b.gmF[e] = GemmEntry{b.Bs, d.T, d.F, Nf, Nf, Np, b.Np_max, Np, Nf, 1.0, 0.0, 1};
     b.gmG1[e] = GemmEntry{Cn, sinv, gcur, K, Np, Np, K, Np, K, 1.0, 1.0};
     b.gmG2[e] = GemmEntry{Cn, d.T, gcur + (size_t)Np * K, K, Nf, Np, K, Np, K, -1.0, 1.0};
     b.gmG3[e] = GemmEntry{gcur, rinv, gnext, K, Nt, Nt, K, Nt, K, 1.0, 0.0};
