@@ -1355,6 +1355,27 @@ void panel_shape(int nmax, int& pcfg, int& pt) {
     pt = 32 * (((nmax + prows - 1) / prows + 31) / 32);
 }
 
+// Kernel attributes are per device: one flag bit per device and scheme.
+std::mutex g_attr_mutex;
+unsigned long long g_attr_done[3] = {0, 0, 0};
+
+// Runs set() once per (scheme, current device); returns its status.
+template <class F>
+int once_per_device(int scheme, F set) {
+    int dev = 0;
+    SCATT_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) {
+        set_last_error("inverse: device ordinal out of range");
+        return SCATT_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_attr_mutex);
+    const unsigned long long bit = 1ull << dev;
+    if (g_attr_done[scheme] & bit) return SCATT_OK;
+    const int st = set();
+    if (st == SCATT_OK) g_attr_done[scheme] |= bit;
+    return st;
+}
+
 }  // namespace
 
 int gj_max_order() {
@@ -1376,15 +1397,14 @@ int gj_inverse_batched(const GjEntry* entries_dev, int count, int nmax,
         return SCATT_ERR_SIZE;
     }
     const size_t smem = panel_smem_bytes(nmax);
-    static bool attr_set = false;
-    if (!attr_set) {
+    SCATT_TRY(once_per_device(0, [&]() -> int {
         SCATT_CUDA_TRY(cudaFuncSetAttribute(gj_update2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)U2_SMEM));
         SCATT_CUDA_TRY(cudaFuncSetAttribute(gj_panel_kernel,
                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)PANEL_SMEM_LIMIT));
-        attr_set = true;
-    }
+        return SCATT_OK;
+    }));
     const int steps = (nmax + NB - 1) / NB;
     const int tiles = (nmax + UBM - 1) / UBM;
     dim3 ugrid(tiles, tiles, count);
@@ -1413,12 +1433,11 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax, bool sy
                         cudaStream_t stream) {
     if (count <= 0 || nmax <= 0) return SCATT_OK;
     if (nmax > 1280) return gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream);
-    static bool attr2 = false;
-    if (!attr2) {
+    SCATT_TRY(once_per_device(1, [&]() -> int {
         SCATT_CUDA_TRY(cudaFuncSetAttribute(gj2_narrow_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)U2_SMEM));
-        attr2 = true;
-    }
+        return SCATT_OK;
+    }));
     const int outer = (nmax + OB - 1) / OB;
     const int tiles = (nmax + 63) / 64;
     int pcfg, pt;
@@ -1445,14 +1464,13 @@ int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax, bool sy
                         cudaStream_t stream, bool look_ahead) {
     if (count <= 0 || nmax <= 0) return SCATT_OK;
     if (nmax > 1280) return gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream);
-    static bool attr3 = false;
-    if (!attr3) {
+    SCATT_TRY(once_per_device(2, [&]() -> int {
         SCATT_CUDA_TRY(cudaFuncSetAttribute(gj3_narrow_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)NARROW3_SMEM));
         SCATT_CUDA_TRY(cudaFuncSetAttribute(gj3_trail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)TRAIL3_SMEM));
-        attr3 = true;
-    }
+        return SCATT_OK;
+    }));
     const int outer = (nmax + OB - 1) / OB;
     const int tiles = (nmax + 63) / 64;
     const int mtiles = (nmax + T3M - 1) / T3M;
