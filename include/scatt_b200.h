@@ -99,6 +99,39 @@ int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call);
  * All give the same inverse up to rounding. */
 int scatt_set_inverse_blocking(int scheme);
 
+/* ------------------------------------------- per-step compatibility seam
+ * The reference's per-radial-step device interface (GpuForwardStepper,
+ * GpuSinvStepper, GpuBackStepper in src/scatt/GpuPropagate.hpp:83-279),
+ * kept for callers and checks written against it.  Each stepper keeps its
+ * carried state on the device and takes one step's operands as host
+ * buffers (column-major FP64); the batched solver does not use them.
+ * max_asym_out (may be NULL) receives max |X - X^T| of the result. */
+typedef struct scatt_fwd_stepper scatt_fwd_stepper;
+typedef struct scatt_sinv_stepper scatt_sinv_stepper;
+typedef struct scatt_back_stepper scatt_back_stepper;
+
+/* Rinv_n = sym((12 W_inv - 10 I - Rinv_{n-1})^-1); Rinv_{n-1} starts at 0
+ * or at the matrix given to scatt_fwd_stepper_init. */
+int scatt_fwd_stepper_create(int device, int n_total, scatt_fwd_stepper** out);
+int scatt_fwd_stepper_destroy(scatt_fwd_stepper* h);
+int scatt_fwd_stepper_init(scatt_fwd_stepper* h, const double* rprev_inv);
+int scatt_fwd_stepper_step(scatt_fwd_stepper* h, const double* w_inv, double* rinv_out,
+                           double* max_asym_out);
+/* Sinv = sym((A - B diag(Dinv) B^T)^-1); B = Dinv = NULL gives sym(A^-1)
+ * (GpuSinvStepper::step_inverse_only). */
+int scatt_sinv_stepper_create(int device, int n_psi, int n_f, scatt_sinv_stepper** out);
+int scatt_sinv_stepper_destroy(scatt_sinv_stepper* h);
+int scatt_sinv_stepper_step(scatt_sinv_stepper* h, const double* A, const double* B,
+                            const double* dinv, double* sinv_out, double* max_asym_out);
+/* Z <- Rinv Z; Y = W_inv Z; psi = first n_psi rows of Y (n_psi x n_psi),
+ * f = the rest (n_f x n_psi, may be NULL). */
+int scatt_back_stepper_create(int device, int n_total, int n_psi, scatt_back_stepper** out);
+int scatt_back_stepper_destroy(scatt_back_stepper* h);
+int scatt_back_stepper_init(scatt_back_stepper* h, const double* Z);
+int scatt_back_stepper_step(scatt_back_stepper* h, const double* rinv, const double* w_inv,
+                            double* psi_out, double* f_out);
+int scatt_back_stepper_get_z(scatt_back_stepper* h, double* Z_out);
+
 /* ------------------------------------------------------ per-scan solver
  * The reference runs one energy at a time through run_one_energy
  * (src/main.cpp:1081-1623); here a batch of energies is solved together,
