@@ -2,6 +2,7 @@
 //
 //   scan_driver solve   <inputs.bin> <results.bin>
 //   scan_driver inverse <matrix.bin> <inverse.bin>
+//   scan_driver stepper <n>      one GpuForwardStepper step with a known answer
 //
 // inputs.bin (little endian): 13 int32
 //   Nr l_cont n_occ n_orb Nlm_store Nr_store init_state n_H n_atoms pol_form
@@ -13,7 +14,9 @@
 // then the six partial sigmas.
 // matrix.bin: int32 n, float64 A (n x n column-major); inverse.bin: the inverse.
 // Failures print the library's message to stderr and exit with status 2.
+#include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <iostream>
@@ -108,9 +111,31 @@ int run_inverse(const char* in_path, const char* out_path) {
 
 }  // namespace
 
+// One forward step of order n from W_inv = I / 2 and R_prev_inv = 0:
+// Rinv = (6 I - 10 I)^-1 = -I / 4 (a check of the stepper wrappers).
+int run_stepper(int n) {
+    scatt_b200::GpuForwardStepper f(n);
+    scatt_b200::Matrix W(n, n), R;
+    for (int i = 0; i < n; ++i) W(i, i) = 0.5;
+    f.step(W, R);
+    double err = 0.0;
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) err = std::max(err, std::abs(R(i, j) - (i == j ? -0.25 : 0.0)));
+    std::cout << err << "\n";
+    return err < 1e-15 ? 0 : 3;
+}
+
 int main(int argc, char** argv) {
+    if (argc == 3 && std::strcmp(argv[1], "stepper") == 0) {
+        try {
+            return run_stepper(std::atoi(argv[2]));
+        } catch (const std::exception& ex) {
+            std::cerr << ex.what() << "\n";
+            return 2;
+        }
+    }
     if (argc != 4 || (std::strcmp(argv[1], "solve") != 0 && std::strcmp(argv[1], "inverse") != 0)) {
-        std::cerr << "usage: scan_driver solve|inverse <input> <output>\n";
+        std::cerr << "usage: scan_driver solve|inverse <input> <output> | stepper <n>\n";
         return 1;
     }
     try {

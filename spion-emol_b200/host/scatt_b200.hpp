@@ -6,8 +6,9 @@
 // AsymptoticAmplitudes.hpp:50-68) and DipoleResult (src/scatt/
 // DipoleMatrixElement.hpp:80-91), failures throw std::runtime_error with the
 // library's message as the reference's classes do (src/scatt/
-// LapackInverse.hpp:73-86, AsymptoticAmplitudes.cpp:177-186), and the dense
-// inverse helpers keep the names of src/scatt/LapackInverse.hpp:53-178.
+// LapackInverse.hpp:73-86, AsymptoticAmplitudes.cpp:177-186), the dense
+// inverse helpers keep the names of src/scatt/LapackInverse.hpp:53-178, and
+// the per-step steppers those of src/scatt/GpuPropagate.hpp:83-279.
 // Matrices are column-major (Eigen's default layout) in a plain vector, so
 // the header needs nothing beyond the standard library and scatt_b200.h.
 #pragma once
@@ -210,6 +211,87 @@ private:
     ScanInputs in_;
     scatt_ctx* ctx_ = nullptr;
     int n_transition_ = 0, Np_ = 0;
+};
+
+// The reference's per-radial-step seam (src/scatt/GpuPropagate.hpp:83-279):
+// carried state stays on the device, one step's operands are host matrices.
+class GpuForwardStepper {
+public:
+    GpuForwardStepper(int n_total, int device = 0) : n_(n_total) {
+        check(scatt_fwd_stepper_create(device, n_total, &h_));
+    }
+    ~GpuForwardStepper() { scatt_fwd_stepper_destroy(h_); }
+    GpuForwardStepper(const GpuForwardStepper&) = delete;
+    GpuForwardStepper& operator=(const GpuForwardStepper&) = delete;
+    void init_R_prev_inv(const Matrix& R) { check(scatt_fwd_stepper_init(h_, R.data.data())); }
+    // Rinv_out = sym((12 W_inv - 10 I - R_prev_inv)^-1); returns max |Rinv - Rinv^T|
+    double step(const Matrix& W_inv, Matrix& Rinv_out) {
+        Rinv_out = Matrix(n_, n_);
+        double asym = 0.0;
+        check(scatt_fwd_stepper_step(h_, W_inv.data.data(), Rinv_out.data.data(), &asym));
+        return asym;
+    }
+
+private:
+    int n_;
+    scatt_fwd_stepper* h_ = nullptr;
+};
+
+class GpuSinvStepper {
+public:
+    GpuSinvStepper(int n_psi, int n_f, int device = 0) : np_(n_psi) {
+        check(scatt_sinv_stepper_create(device, n_psi, n_f, &h_));
+    }
+    ~GpuSinvStepper() { scatt_sinv_stepper_destroy(h_); }
+    GpuSinvStepper(const GpuSinvStepper&) = delete;
+    GpuSinvStepper& operator=(const GpuSinvStepper&) = delete;
+    // Sinv = sym((A - B diag(Dinv) B^T)^-1)
+    double step(const Matrix& A, const Matrix& B, const std::vector<double>& Dinv, Matrix& Sinv_out) {
+        Sinv_out = Matrix(np_, np_);
+        double asym = 0.0;
+        check(scatt_sinv_stepper_step(h_, A.data.data(), B.data.data(), Dinv.data(), Sinv_out.data.data(), &asym));
+        return asym;
+    }
+    // Sinv = sym(A^-1) (no exchange coupling)
+    double step_inverse_only(const Matrix& A, Matrix& Sinv_out) {
+        Sinv_out = Matrix(np_, np_);
+        double asym = 0.0;
+        check(scatt_sinv_stepper_step(h_, A.data.data(), nullptr, nullptr, Sinv_out.data.data(), &asym));
+        return asym;
+    }
+
+private:
+    int np_;
+    scatt_sinv_stepper* h_ = nullptr;
+};
+
+class GpuBackStepper {
+public:
+    GpuBackStepper(int n_total, int n_psi, int device = 0) : nt_(n_total), np_(n_psi) {
+        check(scatt_back_stepper_create(device, n_total, n_psi, &h_));
+    }
+    ~GpuBackStepper() { scatt_back_stepper_destroy(h_); }
+    GpuBackStepper(const GpuBackStepper&) = delete;
+    GpuBackStepper& operator=(const GpuBackStepper&) = delete;
+    void init_Z(const Matrix& Z) { check(scatt_back_stepper_init(h_, Z.data.data())); }
+    // Z <- Rinv Z; Y = W_inv Z; psi_out = Y[0:n_psi, :]; f_out = Y[n_psi:, :] when compute_f
+    void step(const Matrix& Rinv, const Matrix& W_inv, Matrix& psi_out, Matrix* f_out, bool compute_f) {
+        psi_out = Matrix(np_, np_);
+        double* f = nullptr;
+        if (compute_f && f_out) {
+            *f_out = Matrix(nt_ - np_, np_);
+            f = f_out->data.data();
+        }
+        check(scatt_back_stepper_step(h_, Rinv.data.data(), W_inv.data.data(), psi_out.data.data(), f));
+    }
+    void get_Z(Matrix& Z_out) const {
+        Z_out = Matrix(nt_, np_);
+        check(scatt_back_stepper_get_z(h_, Z_out.data.data()));
+    }
+
+private:
+    int nt_, np_;
+    scatt_back_stepper* h_ = nullptr;
 };
 
 // Dense inverses on the device, named as in LapackInverse.hpp:53-178; a

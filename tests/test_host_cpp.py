@@ -74,6 +74,8 @@ def test_driver_reports_missing_device(tmp_path):
     r = subprocess.run([_driver(), "solve", str(fin), str(fout)], capture_output=True, text=True)
     assert r.returncode == 2
     assert "no CUDA device" in r.stderr
+    r = subprocess.run([_driver(), "stepper", "8"], capture_output=True, text=True)
+    assert r.returncode == 2 and "no CUDA device" in r.stderr
     m = tmp_path / "m.bin"
     m.write_bytes(struct.pack("<i", 2) + np.eye(2).tobytes())
     r = subprocess.run([_driver(), "inverse", str(m), str(tmp_path / "x.bin")], capture_output=True, text=True)
@@ -115,3 +117,11 @@ def test_driver_inverse_and_singular_throw(tmp_path):
     m.write_bytes(struct.pack("<i", 3) + np.ones((3, 3)).tobytes())
     r = subprocess.run([_driver(), "inverse", str(m), str(x)], capture_output=True, text=True)
     assert r.returncode == 2 and "singular" in r.stderr
+
+
+@pytest.mark.gpu
+def test_driver_forward_stepper_wrapper():
+    # W_inv = I/2, R_prev_inv = 0: Rinv = (6 I - 10 I)^-1 = -I/4 exactly
+    r = subprocess.run([_driver(), "stepper", "8"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert float(r.stdout.strip()) == 0.0
