@@ -99,3 +99,69 @@ def test_exchange_coupling_equals_triple_loop(setup):
         ref *= 2.0 * math.sqrt(2.0 * math.pi) / r
         scale = max(np.max(np.abs(ref)), 1e-300)
         assert np.max(np.abs(Q - ref)) / scale < 1e-12
+
+
+def _riccati_j(l, x):
+    from scipy.special import spherical_jn
+    return x * spherical_jn(l, x)
+
+
+def test_forward_analytic_start():
+    """test_forward_r_propagator.cpp (1): Rinv(n) for 1 <= n < n_start is the
+    diagonal (M_n y_n) / (M_{n+1} y_{n+1}), off-diagonal zero (1e-14);
+    r_n = r_min + n h with r_min = h, V at index n, y = x j_l(x) for the
+    continuum channels and r^(l+1) for the exchange channels (:121-166)."""
+    inp = synth.h2_like(Nr=201, dr=0.05, l_cont=10)
+    st = O.make_setup(inp)
+    E = 0.5
+    h = st.dr
+    h2_6, h2_12 = h * h / 6.0, h * h / 12.0
+    k = math.sqrt(2.0 * E)
+    ns = O.n_start(st)
+    assert ns > 3
+    for n in range(1, ns):
+        R = O.analytic_init(st, E, n)
+        rn, rn1 = h + n * h, h + (n + 1) * h
+        Vn, Vn1 = O.V_at(st, n), O.V_at(st, n + 1)
+        ref = np.zeros(st.Nt)
+        for mu in range(st.n_mu):
+            l = int(st.l_mu[mu])
+            Mn, Mn1 = 1.0 + h2_6 * (E - Vn[mu, mu]), 1.0 + h2_6 * (E - Vn1[mu, mu])
+            den = Mn1 * _riccati_j(l, k * rn1)
+            if abs(den) > 1e-300:
+                ref[mu] = Mn * _riccati_j(l, k * rn) / den
+        for f in range(st.Nf):
+            l = int(st.l_sigma_f[f])
+            Mn = max(1.0 - h2_12 * l * (l + 1) / (rn * rn), O.W_MIN)
+            Mn1 = max(1.0 - h2_12 * l * (l + 1) / (rn1 * rn1), O.W_MIN)
+            den = Mn1 * rn1 ** (l + 1)
+            if abs(den) > 1e-300:
+                ref[st.n_mu + f] = Mn * rn ** (l + 1) / den
+        off = R - np.diag(np.diag(R))
+        assert np.max(np.abs(off)) == 0.0
+        assert np.max(np.abs(np.diag(R) - ref)) < 1e-14
+
+
+def test_forward_recursion_gold_standard(setup):
+    """test_forward_r_propagator.cpp (2)-(3): the recursion against an
+    independent path (LU inverse of the assembled W, then of 12 W^-1 - 10 I -
+    Rinv_prev, symmetrised; :170-205) to 1e-8, and symmetric to 1e-12."""
+    st = setup
+    E = 0.9
+    ns = O.n_start(st)
+    I = np.eye(st.Nt)
+    prev_o = O.analytic_init(st, E, ns - 1)
+    prev_r = prev_o.copy()
+    probes = {ns, ns + 1, ns + 5, 50, 200, st.Nr - 2, st.Nr - 1}
+    worst = 0.0
+    for n in range(ns, st.Nr):
+        prev_o = O.frp_step(st, n, O.sinv_at(st, E, n), prev_o)
+        Wi = np.linalg.inv(assembled_W(st, E, n)) if n >= O.STAB_N_MAX else \
+            O.winv_apply(st, n, O.sinv_at(st, E, n), I)
+        Rn = np.linalg.inv(12.0 * Wi - 10.0 * I - prev_r)
+        prev_r = 0.5 * (Rn + Rn.T)
+        if n in probes:
+            worst = max(worst, np.max(np.abs(prev_o - prev_r)) / np.max(np.abs(prev_r)))
+            assert np.all(np.isfinite(prev_o))
+            assert np.max(np.abs(prev_o - prev_o.T)) / np.max(np.abs(prev_o)) < 1e-12
+    assert worst < 1e-8
