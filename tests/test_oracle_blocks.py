@@ -165,3 +165,46 @@ def test_forward_recursion_gold_standard(setup):
             assert np.all(np.isfinite(prev_o))
             assert np.max(np.abs(prev_o - prev_o.T)) / np.max(np.abs(prev_o)) < 1e-12
     assert worst < 1e-8
+
+
+def test_back_propagation_checks():
+    """test_back_propagator.cpp (1) the three-point Numerov identity
+    W_{n+1} Y_{n+1} - (12 I - 10 W_n) Y_n + W_{n-1} Y_{n-1} = 0 (1e-8 rel),
+    (2) psi_N == psi_boundary (1e-14), (3) psi_0 = 0 (1e-12), (4) psi_n close
+    to J_n + Y_n K near the outer edge (1e-1 rel)."""
+    inp = synth.h2_like(Nr=801, dr=0.05, l_cont=2)
+    st = O.make_setup(inp)
+    E = 0.8
+    r = O.solve_energy(st, E, keep_rinv=True, keep_psi=True)
+    N, Np = st.Nr - 1, st.n_mu
+    bc = O.psi_boundary(st, E, r.K_kme)
+    assert np.max(np.abs(r.psi_keep[N] - bc)) < 1e-14
+    assert np.max(np.abs(r.psi_keep[0])) < 1e-12
+    k = math.sqrt(2.0 * E)
+    from scipy.special import spherical_jn, spherical_yn
+    worst = 0.0
+    for n in (N - 1, N - 2, N - 5, N - 10, N - 50, N - 100):
+        rn = st.dr + n * st.dr
+        lv = st.l_mu.astype(int)
+        J = np.diag(k * rn * spherical_jn(lv, k * rn))
+        Y = np.diag(k * rn * spherical_yn(lv, k * rn))
+        ans = J + Y @ r.K_kme
+        worst = max(worst, np.max(np.abs(r.psi_keep[n] - ans)) / np.max(np.abs(ans)))
+    assert worst < 1e-1
+    # backward sweep with the full Y = W^-1 Z (psi and f) for the identity
+    h2_6 = st.dr * st.dr / 6.0
+    B_N = O.B_at(st, N)
+    f_N = -(O.dinv_at(st, N)[:, None] * (B_N.T @ bc))
+    Z = np.zeros((st.Nt, Np))
+    Z[:Np] = bc + h2_6 * E * bc - h2_6 * O.V_at(st, N) @ bc + B_N @ f_N
+    Ys = {}
+    probe = 300
+    for n in range(N - 1, probe - 2, -1):
+        Z = r.rinv[n] @ Z
+        if n <= probe + 1:
+            Ys[n] = O.winv_apply(st, n, O.sinv_at(st, E, n), Z)
+    I = np.eye(st.Nt)
+    Wp, Wn, Wq = (assembled_W(st, E, m) for m in (probe - 1, probe, probe + 1))
+    res = Wq @ Ys[probe + 1] - (12.0 * I - 10.0 * Wn) @ Ys[probe] + Wp @ Ys[probe - 1]
+    scale = max(np.max(np.abs(Ys[m])) for m in (probe - 1, probe, probe + 1))
+    assert np.max(np.abs(res)) / scale < 1e-8
