@@ -74,3 +74,31 @@ def test_asymptotic_amplitude_checks(h2):
         delta = np.arctan(np.linalg.eigvals(K).real)
         ev = np.sort(np.angle(np.linalg.eigvals(S)))
         assert np.max(np.abs(ev - np.sort(_wrap(2 * delta)))) < max(1e-9, 10 * ksym)
+
+
+@pytest.mark.parametrize("name", ["h2", "h2o"])
+def test_setup_rules(name):
+    """src/tests/test_wavefunction_setup.cpp: l_x = min(l_cont, 10), channel
+    counts, chi(j, lambda)(r) = r psi_lm(j, lambda)(r) with r = ir dr, and the
+    n_transition rule of WavefunctionSetup.cpp:270-320 (last ir with any
+    |psi_lm| > chi_cutoff over the occupied orbitals, plus a max(100, 5/dr)
+    buffer, clamped to Nr and to the stored radial length)."""
+    inp = synth.h2_like(Nr=801, dr=0.05, l_cont=12) if name == "h2" else \
+        synth.h2o_like(Nr=601, dr=0.05, l_cont=3, lmax_orb=6, n_orb=3)
+    st = O.make_setup(inp)
+    lc = inp.l_cont
+    lx = min(lc, 10)
+    assert st.l_x == lx
+    assert st.n_mu == (lc + 1) ** 2 and st.n_sigma == (lx + 1) ** 2
+    assert st.n_lambda == (lc + lx + 1) ** 2
+    assert st.Nf == inp.n_occ * st.n_sigma and st.Nt == st.n_mu + st.Nf
+    psi = inp.psi_lm
+    nl = min(st.n_lambda, psi.shape[1])
+    mx = np.max(np.abs(psi[:inp.n_occ, :nl, :]), axis=(0, 1))
+    over = np.nonzero(mx > 1e-15)[0]
+    last = int(over[-1]) if over.size else 0
+    n_tr = min(inp.Nr, psi.shape[2], last + 1 + max(100, int(5.0 / inp.dr)))
+    assert st.n_tr == max(1, n_tr)
+    ir = 5
+    ref = ir * inp.dr * psi[:inp.n_occ, :nl, ir]
+    assert np.max(np.abs(st.chi_r[:, :nl, ir] - ref)) < 1e-14
