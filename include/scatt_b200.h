@@ -174,7 +174,8 @@ typedef struct {
     int    allow_closed_channels; /* (0)     AsymptoticAmplitudes.hpp:72-102          */
     int    orthogonalize;         /* (1)     DipoleMatrixElement.hpp:104-148          */
     int    max_batch;             /* energies per device batch; 0 = as many as fit    */
-    int    use_graphs;            /* 1: replay the radial step as a CUDA graph        */
+    int    use_graphs;            /* reserved, ignored: the radial step is launched
+                                     directly; graph replay is not implemented    */
     int    diagnostics;           /* 1: S-matrix unitarity and eigenphases            */
     int    timing;                /* 1: CUDA-event timing of the solve (scatt_last_stats) */
 } scatt_solve_opts;
