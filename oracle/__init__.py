@@ -22,10 +22,11 @@ cannot be pinned to the reference binary (it needs Eigen, HDF5 and GSL,
 none of which exist in this image), so the end-to-end restatement is
 "parity unpinned" against the reference binary.  It is checked instead
 against the acceptance criteria of the reference's component tests, with
-their thresholds (tests/test_oracle_properties.py, tests/test_oracle_blocks.py):
-the W^-1 operator against an LU inverse of the assembled W, Sinv S = I,
-the exchange coupling against the triple loop, the analytic start and an
-independent LU recursion, the three-point Numerov identity on the
-back-propagated solution, K symmetry, S unitarity, eigenphases, matching-
-radius invariance and the asymptotic-fit checks.
+their thresholds (tests/test_oracle_properties.py, tests/test_oracle_blocks.py,
+tests/test_oracle_gauge.py): the W^-1 operator against an LU inverse of the
+assembled W, Sinv S = I, the exchange coupling against the triple loop, the
+analytic start and an independent LU recursion, the three-point Numerov
+identity on the back-propagated solution, K symmetry, S unitarity,
+eigenphases, matching-radius invariance, the asymptotic-fit checks, the
+setup rules, and the per-channel length/velocity gauge identity.
 """
