@@ -7,7 +7,12 @@ reference's component tests (thresholds as there):
       block-diagonal [Sinv, diag(1/D_clamp)];
   src/tests/test_schur_inverter.cpp  Sinv S == I, Sinv symmetric;
   src/tests/test_exchange_coupling.cpp  the CSR exchange coupling == the
-      triple loop sum_lambda G(mu, lambda, sigma) chi_{i,lambda}(r).
+      triple loop sum_lambda G(mu, lambda, sigma) chi_{i,lambda}(r);
+  src/tests/test_lapack_inverse.cpp  A A^-1 = I and agreement with a
+      partial-pivot LU inverse (1e-11), in both LAPACK builds;
+  src/tests/test_sinv_symmetric_inverse.cpp  the dsytrf/dsytri Sinv exactly
+      symmetric, Sinv S = I and within 1e-10 of the symmetrised LU inverse;
+  src/tests/test_forward_r_propagator.cpp, test_back_propagator.cpp  (below).
 """
 import dataclasses
 import math
@@ -208,3 +213,53 @@ def test_back_propagation_checks():
     res = Wq @ Ys[probe + 1] - (12.0 * I - 10.0 * Wn) @ Ys[probe] + Wp @ Ys[probe - 1]
     scale = max(np.max(np.abs(Ys[m])) for m in (probe - 1, probe, probe + 1))
     assert np.max(np.abs(res)) / scale < 1e-8
+
+
+@pytest.mark.parametrize("build", ["eigen", "mkl"])
+def test_lapack_inverse(monkeypatch, build):
+    """test_lapack_inverse.cpp: for n in {1, 4, 17, 49, 121, 256}, on
+    X^T X + n I and X + n I with X uniform in [-1, 1],
+    ||A A^-1 - I||_inf / max(||A||_inf, 1) < 1e-11, and the inverse within
+    1e-11 (relative) of a partial-pivot LU inverse."""
+    monkeypatch.setattr(O, "BUILD", build)
+    rng = np.random.default_rng(0xBEEF)
+    for n in (1, 4, 17, 49, 121, 256):
+        X = rng.uniform(-1.0, 1.0, (n, n))
+        spd = X.T @ X + n * np.eye(n)
+        gen = rng.uniform(-1.0, 1.0, (n, n)) + n * np.eye(n)
+        for A in (spd, gen):
+            res = A @ O.inverse_general(A) - np.eye(n)
+            assert np.max(np.abs(res)) / max(np.max(np.abs(A)), 1.0) < 1e-11
+        ref = np.linalg.solve(gen, np.eye(n))
+        assert np.max(np.abs(ref - O.inverse_general(gen))) / np.max(np.abs(ref)) < 1e-11
+
+
+def schur_S(st, E, n):
+    """The matrix sinv_at inverts: A - B D^-1 B^T with the stability shifts."""
+    h2_6 = st.dr * st.dr / 6.0
+    A = (1.0 + h2_6 * E) * np.eye(st.n_mu) - h2_6 * O.V_at(st, n)
+    if n < O.STAB_N_MAX:
+        A, _ = O.stability_shift(O.sym(A))
+    if n >= st.n_tr:
+        return A
+    B = O.B_at(st, n)
+    S = A - (B * O.dinv_at(st, n)[None, :]) @ B.T
+    if n < O.STAB_N_MAX:
+        S, _ = O.stability_shift(S)
+    return S
+
+
+def test_sinv_symmetric_inverse(monkeypatch, setup):
+    """test_sinv_symmetric_inverse.cpp, at every radial point: the
+    dsytrf + dsytri Sinv is exactly symmetric, Sinv S = I to 1e-10, and it
+    is within 1e-10 (relative) of the LU inverse symmetrised as 0.5 (M + M^T)."""
+    st = setup
+    E = 0.9
+    for n in range(st.Nr):
+        monkeypatch.setattr(O, "BUILD", "mkl")
+        new = O.sinv_at(st, E, n)
+        monkeypatch.setattr(O, "BUILD", "eigen")
+        legacy = O.sinv_at(st, E, n)
+        assert np.array_equal(new, new.T)
+        assert np.max(np.abs(new @ schur_S(st, E, n) - np.eye(st.n_mu))) < 1e-10
+        assert np.max(np.abs(new - legacy)) / np.max(np.abs(legacy)) < 1e-10
