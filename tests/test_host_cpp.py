@@ -121,7 +121,8 @@ def test_driver_inverse_and_singular_throw(tmp_path):
 
 @pytest.mark.gpu
 def test_driver_forward_stepper_wrapper():
-    # W_inv = I/2, R_prev_inv = 0: Rinv = (6 I - 10 I)^-1 = -I/4 exactly
+    # W_inv = I/2, R_prev_inv = 0: Rinv = (6 I - 10 I)^-1 = -I/4 (every
+    # operation exact in binary floating point; the driver exits 3 above 1e-15)
     r = subprocess.run([_driver(), "stepper", "8"], capture_output=True, text=True)
-    assert r.returncode == 0, r.stderr
-    assert float(r.stdout.strip()) == 0.0
+    assert r.returncode == 0, (r.stdout, r.stderr)
+    assert float(r.stdout.strip()) < 1e-15
