@@ -9,7 +9,9 @@ element of each dominant channel (|d_raw^L| >= 5 % of the largest) equals
 
 (a) in sign on every dominant channel and (b) within 50 % relative, the
 allowance it makes for the static-exchange continuum and the bound state not
-being eigenstates of one Hamiltonian.
+being eigenstates of one Hamiltonian.  test_dipole_matrix_element.cpp adds
+(5) sigma_V / (omega^2 sigma_L) within [0.1, 10] and (7) the raw reduced
+dipole unchanged by the orthogonalisation flag.
 
 Its H2O fixture is not available here.  A hydrogen atom stands in: one Z = 1
 nucleus, no Hartree potential, and a hydrogenic orbital (1s or 2p_z) as the
@@ -32,7 +34,7 @@ from scatt_b200.synth import ScanInputs, lm_to_idx
 E_KIN = 0.5
 
 
-def _hydrogen(state: str, eps: float, Nr: int, dr: float):
+def _hydrogen(state: str, eps: float, Nr: int, dr: float, keep_psi: bool = False):
     """F_lambda(r) of a hydrogenic orbital on r = ir * dr, psi = F(r) Y_lambda."""
     r = np.arange(Nr) * dr
     F = np.zeros((1, 4, Nr))
@@ -46,7 +48,7 @@ def _hydrogen(state: str, eps: float, Nr: int, dr: float):
                      atoms=np.array([[1.0, 0.0, 0.0, 0.0]]), psi_lm=F,
                      orb_energies=np.array([e]), n_occ=1, V_H=np.zeros((1, Nr)))
     st = O.make_setup(inp, 4)
-    return st, O.solve_energy(st, E_KIN), E_KIN - e
+    return st, O.solve_energy(st, E_KIN, keep_psi=keep_psi), E_KIN - e
 
 
 def _per_channel(res, omega):
@@ -63,7 +65,7 @@ def _per_channel(res, omega):
 
 
 def test_gauge_per_channel_reference_criteria():
-    st, res, omega = _hydrogen("1s", 1.0, 4001, 0.01)
+    st, res, omega = _hydrogen("1s", 1.0, 4001, 0.01, keep_psi=True)
     checks = _per_channel(res, omega)
     for n_dom, bad_sign, dev in checks:
         assert n_dom >= 1
@@ -71,6 +73,18 @@ def test_gauge_per_channel_reference_criteria():
         assert dev < 0.5
     # a spherical initial state: x, y and z see the same raw elements
     assert checks[0][2] == pytest.approx(checks[2][2], rel=1e-9)
+    # test_dipole_matrix_element.cpp (5): sigma_V / (omega^2 sigma_L) in [0.1, 10]
+    for p in range(3):
+        ratio = res.slices[3 + p]["partial_sigma"] / (omega ** 2 * res.slices[p]["partial_sigma"])
+        assert 0.1 < ratio < 10.0
+    # test_dipole_matrix_element.cpp (7): the raw reduced dipole does not depend
+    # on the orthogonalisation flag (1e-12); here it is the same to the bit.
+    # (The correction itself vanishes here: it is <1s| r |1s> = 0.)
+    n_hi = min(st.Nr, min(st.Nr - 1, max(1, st.n_tr - 1)) + 1)
+    off, _ = O.dme_compute_six(st, res.aa["A"], res.aa["B"], lambda ir: res.psi_keep[ir], 0, n_hi,
+                               orthogonalize=False)
+    for s in range(6):
+        assert np.array_equal(off[s]["D_raw"], res.slices[s]["D_raw"])
 
 
 def test_gauge_identity_without_exchange_is_first_order_in_dr():

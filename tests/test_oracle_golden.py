@@ -2,7 +2,8 @@
 to the golden vectors of the reference's own unit tests and to mpmath.
 
 Reference tests restated: src/tests/test_gaunt.cpp, test_real_gaunt_dipole.cpp,
-test_freeparticle_dipole.cpp, test_dipole_matrix_element.cpp:80-113.
+test_freeparticle_dipole.cpp, test_dipole_matrix_element.cpp:80-113 and its
+isotropy sum rule (:156-196).
 """
 import json
 import math
@@ -64,6 +65,26 @@ def test_angular_dipole_and_velocity_coef(impl):
     assert abs(ad(1, 0, 1, 0, 0)) < 1e-12
     for (lm, ln, want) in [(1, 0, -1.0), (2, 1, -2.0), (0, 1, 1.0), (1, 2, 2.0), (0, 0, 0.0)]:
         assert vc(lm, ln) == want
+
+
+@pytest.mark.parametrize("impl", ["oracle", "library"])
+def test_angular_dipole_isotropy_sum_rule(impl):
+    """test_dipole_matrix_element.cpp (3): at fixed l_nu the sum over m_nu, l_mu
+    = l_nu +- 1 and m_mu of |A(l_mu m_mu; q; l_nu m_nu)|^2 is the same for
+    q = -1, 0, 1 (to 1e-12); there for l_nu <= 3, here up to 12."""
+    _, ad, _ = implementations()[impl]
+    for l_nu in range(13):
+        sums = []
+        for q in (-1, 0, 1):
+            s = 0.0
+            for m_nu in range(-l_nu, l_nu + 1):
+                for l_mu in (l_nu - 1, l_nu + 1):
+                    if l_mu < 0:
+                        continue
+                    for m_mu in range(-l_mu, l_mu + 1):
+                        s += ad(l_mu, m_mu, q, l_nu, m_nu) ** 2
+            sums.append(s)
+        assert max(sums) - min(sums) < 1e-12
 
 
 def test_wigner3j_library_matches_exact():
