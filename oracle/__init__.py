@@ -23,10 +23,17 @@ none of which exist in this image), so the end-to-end restatement is
 "parity unpinned" against the reference binary.  It is checked instead
 against the acceptance criteria of the reference's component tests, with
 their thresholds (tests/test_oracle_properties.py, tests/test_oracle_blocks.py,
-tests/test_oracle_gauge.py): the W^-1 operator against an LU inverse of the
+tests/test_oracle_gauge.py, tests/test_oracle_potential.py,
+tests/test_oracle_gaunt_l50.py): the W^-1 operator against an LU inverse of the
 assembled W, Sinv S = I, the exchange coupling against the triple loop, the
 analytic start and an independent LU recursion, the three-point Numerov
 identity on the back-propagated solution, K symmetry, S unitarity,
 eigenphases, matching-radius invariance, the asymptotic-fit checks, the
-setup rules, and the per-channel length/velocity gauge identity.
+setup rules, the per-channel length/velocity gauge identity, the channel
+potential and the real Gaunt coefficients to l = 50.
+
+oracle/adjoint.py is the gradient checker for the adjoint (the reference
+has none): the forward path restated in float64 torch and differentiated by
+reverse mode, held to central finite differences of this oracle
+(tests/test_adjoint_oracle.py).
 """
