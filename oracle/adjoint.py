@@ -234,10 +234,10 @@ def _dme(P: Problem, A, B, psi: dict, n_lo: int, n_hi: int):
     return out
 
 
-def dipoles(P: Problem, E: float, alpha, r_c, dV=None):
-    """The six orthogonalised reduced dipoles D of one energy (solver.solve_energy)."""
+def _forward(P: Problem, E: float, alpha, r_c, dV, n_last: int):
+    """V(n), Sinv(n) for every n and Rinv(n) up to n_last (solver.solve_energy)."""
     st = P.st
-    Nr, Np, Nt = st.Nr, st.n_mu, st.Nt
+    Nr, Nt = st.Nr, st.Nt
     Vs = [P.V(n, alpha, r_c, dV) for n in range(Nr)]
     Sinv = [_sinv(P, E, n, Vs[n]) for n in range(Nr)]
     ns = O.n_start(st)
@@ -246,10 +246,25 @@ def dipoles(P: Problem, E: float, alpha, r_c, dV=None):
     for n in range(ns):
         Rinv[n] = _analytic_init(P, E, n, Vs[n], Vs[n + 1])
     prev = Rinv[ns - 1]
-    for n in range(ns, Nr):
+    for n in range(ns, n_last + 1):
         U = 12.0 * _winv_apply(P, n, Sinv[n], I) - 10.0 * I
         prev = _sym(torch.linalg.inv(U - prev))
         Rinv[n] = prev
+    return Vs, Sinv, Rinv
+
+
+def k_matrix(P: Problem, E: float, alpha, r_c, dV=None):
+    """K of one energy (KMatrixExtractor at n_match = Nr - 2)."""
+    n_match = P.st.Nr - 2
+    _, _, Rinv = _forward(P, E, alpha, r_c, dV, n_match)
+    return _kme(P, E, Rinv[n_match], n_match)
+
+
+def dipoles(P: Problem, E: float, alpha, r_c, dV=None):
+    """The six orthogonalised reduced dipoles D of one energy (solver.solve_energy)."""
+    st = P.st
+    Nr, Np, Nt = st.Nr, st.n_mu, st.Nt
+    Vs, Sinv, Rinv = _forward(P, E, alpha, r_c, dV, Nr - 1)
     n_match = Nr - 2
     K = _kme(P, E, Rinv[n_match], n_match)
     k = math.sqrt(2.0 * E)
