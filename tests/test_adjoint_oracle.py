@@ -117,6 +117,9 @@ def test_gradients_through_a_stability_shift():
     Pd = rng.standard_normal((base.Nr, P.st.n_mu, P.st.n_mu))
     Pd = 0.5 * (Pd + Pd.transpose(0, 2, 1))
     Pd[O.STAB_N_MAX:] = 0.0
+    # the shift at n = 1 has a degenerate lambda_min (the m = +-l pair), where
+    # the shift is not differentiable; along c I (how alpha and r_c act) it is
+    Pd[1] = 0.7 * np.eye(P.st.n_mu)
     h = 1e-4
     checks = [
         (ga.item(), dataclasses.replace(base, alpha_pol=ALPHA + h), dataclasses.replace(base, alpha_pol=ALPHA - h), None),
