@@ -87,8 +87,8 @@ int scatt_dgemm(int opA, int opB, int M, int N, int K, double alpha,
                 double beta, double* C, int ldc);
 
 /* Device-resident timing of scatt_inverse_batched's kernels on seeded
- * matrices (CUDA events around the kernels only); used by the tile autotuner
- * and the benchmark. */
+ * matrices (CUDA events around the kernels only); used by the inverse
+ * benchmark (python -m scatt_b200.inverse_bench). */
 int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call);
 /* Blocking scheme of every dense inverse (the entry points and the solver):
  * 0 = automatic (default): scheme 3 above order 512, scheme 2 below,
@@ -96,7 +96,8 @@ int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call);
  * 2 = two-level column-major (64-column windows, row pivoting),
  * 3 = two-level on the row-contiguous view of the buffer (pivots by columns
  *     of A, which for a symmetric A is the row-pivoting sequence).
- * All give the same inverse up to rounding. */
+ * All give the same inverse up to rounding.  The setting is process-wide and
+ * applies from the next inverse on, also in solves running on other threads. */
 int scatt_set_inverse_blocking(int scheme);
 
 /* ------------------------------------------- per-step compatibility seam

@@ -16,12 +16,12 @@ namespace {
 thread_local std::string g_last_error;
 }
 // scheme of every dense inverse (see gj_inverse_selected)
-int g_inverse_scheme = 0;
+std::atomic<int> g_inverse_scheme{0};
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
-unsigned long long& launch_counter() {
-    static unsigned long long c = 0;
+std::atomic<unsigned long long>& launch_counter() {
+    static std::atomic<unsigned long long> c{0};
     return c;
 }
 
@@ -162,7 +162,7 @@ int scatt_set_inverse_blocking(int scheme) {
         set_last_error("scatt_set_inverse_blocking: scheme must be 0, 1, 2 or 3");
         return SCATT_ERR_ARG;
     }
-    g_inverse_scheme = scheme;
+    g_inverse_scheme.store(scheme, std::memory_order_relaxed);
     return SCATT_OK;
 }
 

@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -44,9 +45,10 @@ inline int cuda_status(cudaError_t e, const char* what) {
         if (_s != SCATT_OK) return _s;                                          \
     } while (0)
 
-// Kernel launches issued by the library since load (benchmark bookkeeping).
-unsigned long long& launch_counter();
-#define SCATT_COUNT_LAUNCH(n) (::scatt::launch_counter() += (n))
+// Kernel launches issued by the library since load, by every thread
+// (benchmark bookkeeping; atomic because solves may run on several threads).
+std::atomic<unsigned long long>& launch_counter();
+#define SCATT_COUNT_LAUNCH(n) (::scatt::launch_counter().fetch_add((n), std::memory_order_relaxed))
 
 // Device-side status codes written into per-matrix status words.
 enum DeviceStatus : int {
@@ -120,14 +122,16 @@ int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax,
 // Scheme of every dense inverse (entry points and solver): 0 = automatic
 // (row-contiguous two-level above order 512, where its contiguous pivot-row
 // tiles pay; column-major two-level below), 1 = single-level,
-// 2 = column-major two-level, 3 = row-contiguous two-level
-extern int g_inverse_scheme;
+// 2 = column-major two-level, 3 = row-contiguous two-level.  Process-wide;
+// atomic because it may be set while another thread solves (a call reads it
+// once per inverse, so a change applies from the next inverse on).
+extern std::atomic<int> g_inverse_scheme;
 
 // The scheme selected by g_inverse_scheme (entries must carry P and sigt).
 // look_ahead: as for gj_inverse_batched3 (entries sized for it).
 inline int gj_inverse_selected(const GjEntry* entries_dev, int count, int nmax,
                                bool symmetrize, cudaStream_t stream, bool look_ahead) {
-    switch (g_inverse_scheme) {
+    switch (g_inverse_scheme.load(std::memory_order_relaxed)) {
         case 1: return gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream);
         case 2: return gj_inverse_batched2(entries_dev, count, nmax, symmetrize, stream);
         case 3: return gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream, look_ahead);
