@@ -289,7 +289,7 @@ def main():
             "clocks": ck,
             "setup_s": setup_s,
         }
-        if not a.no_cpu_baseline:
+        if not a.no_cpu_baseline and ws == 1:         # the CPU baseline is an N = 1 figure
             try:
                 line["cpu_baseline"] = {k: v for k, v in oracle_baseline(oracle_setup(inp), ks, a.cpu_budget).items()
                                         if k in ("value", "unit", "cores", "kind", "sample")}
