@@ -2,7 +2,7 @@
 //
 //   scan_driver solve   <inputs.bin> <results.bin>
 //   scan_driver inverse <matrix.bin> <inverse.bin>
-//   scan_driver stepper <n>      one GpuForwardStepper step with a known answer
+//   scan_driver stepper <n>      a GpuForwardStepper step and a GpuDipoleEngine product with known answers
 //
 // inputs.bin (little endian): 13 int32
 //   Nr l_cont n_occ n_orb Nlm_store Nr_store init_state n_H n_atoms pol_form
@@ -111,18 +111,32 @@ int run_inverse(const char* in_path, const char* out_path) {
 
 }  // namespace
 
-// One forward step of order n from W_inv = I / 2 and R_prev_inv = 0:
-// Rinv = (6 I - 10 I)^-1 = -I / 4 (a check of the stepper wrappers).
+// The per-step seam on exact cases, built as the reference's stage classes
+// build it: a forward step of order n from W_inv = I / 2 and R_prev_inv = 0
+// gives Rinv = (6 I - 10 I)^-1 = -I / 4, and the dipole engine's product
+// V . (2 I) = 2 V of small integers.  Prints the largest error of each.
 int run_stepper(int n) {
-    scatt_b200::GpuForwardStepper f(n);
+    scatt_b200::GpuContext ctx(true);
+    scatt_b200::GpuForwardStepper f(ctx, n);
     scatt_b200::Matrix W(n, n), R;
     for (int i = 0; i < n; ++i) W(i, i) = 0.5;
     f.step(W, R);
     double err = 0.0;
     for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i) err = std::max(err, std::abs(R(i, j) - (i == j ? -0.25 : 0.0)));
-    std::cout << err << "\n";
-    return err < 1e-15 ? 0 : 3;
+    const int slots = 3;
+    scatt_b200::GpuDipoleEngine eng(ctx, n, slots);
+    scatt_b200::Matrix V(slots, n), psi(n, n), out;
+    for (int j = 0; j < n; ++j) {
+        psi(j, j) = 2.0;
+        for (int s = 0; s < slots; ++s) V(s, j) = s + j;
+    }
+    eng.step(V, psi, out);
+    double err_d = 0.0;
+    for (int j = 0; j < n; ++j)
+        for (int s = 0; s < slots; ++s) err_d = std::max(err_d, std::abs(out(s, j) - 2.0 * (s + j)));
+    std::cout << err << " " << err_d << "\n";
+    return (err < 1e-15 && err_d == 0.0 && f.stats().n_steps == 1 && eng.stats().n_steps == 1) ? 0 : 3;
 }
 
 int main(int argc, char** argv) {

@@ -14,7 +14,10 @@
 #pragma once
 
 #include <array>
+#include <chrono>
 #include <complex>
+#include <cstddef>
+#include <cstdint>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -213,85 +216,269 @@ private:
     int n_transition_ = 0, Np_ = 0;
 };
 
-// The reference's per-radial-step seam (src/scatt/GpuPropagate.hpp:83-279):
-// carried state stays on the device, one step's operands are host matrices.
+// ------------------------------------------------------------ per-step seam
+// The reference's device seam -- GpuContext and the Sinv, forward and back
+// steppers of src/scatt/GpuPropagate.hpp:52-279, and GpuDipoleEngine of
+// src/scatt/GpuDipoleEngine.hpp:85-149 -- with their constructors, methods
+// and Stats fields, over the per-step entry points of the C ABI.  The
+// reference's stage classes (SchurInverter, ForwardRPropagator,
+// BackPropagator, DipoleMatrixElement with use_gpu) build these objects
+// exactly as written there; host/seam/scatt/ holds the two headers that put
+// them into namespace scatt in place of the reference's own.
+// Matrix arguments are Eigen::MatrixXd / Eigen::VectorXd or any column-major
+// contiguous type with rows(), cols(), data() and resize(r, c) (size() and
+// data() for vectors), or scatt_b200::Matrix / std::vector<double>.
+// The carried state (R_prev^-1, Z) stays on the device between steps.
+// One step is one library call on the device's stream (upload, device work,
+// download); its host time is reported in the step's main timing field
+// (t_inverse_ns, t_gemm_z_ns, t_gemm_ns) and the other fields stay 0.
+namespace detail {
+template <class M> inline int rows_of(const M& m) { return static_cast<int>(m.rows()); }
+template <class M> inline int cols_of(const M& m) { return static_cast<int>(m.cols()); }
+template <class M> inline const double* data_of(const M& m) { return m.data(); }
+template <class M> inline double* resized(M& m, int r, int c) { m.resize(r, c); return m.data(); }
+inline int rows_of(const Matrix& m) { return m.rows; }
+inline int cols_of(const Matrix& m) { return m.cols; }
+inline const double* data_of(const Matrix& m) { return m.data.data(); }
+inline double* resized(Matrix& m, int r, int c) { m = Matrix(r, c); return m.data.data(); }
+template <class V> inline int size_of(const V& v) { return static_cast<int>(v.size()); }
+template <class M> inline void need_shape(const M& m, int r, int c, const char* what) {
+    if (rows_of(m) != r || cols_of(m) != c)
+        throw std::runtime_error(std::string(what) + ": expected a " + std::to_string(r) + " x " +
+                                 std::to_string(c) + " matrix");
+}
+using Clock = std::chrono::steady_clock;
+inline std::uint64_t ns_since(Clock::time_point t0) {
+    return static_cast<std::uint64_t>(
+        std::chrono::duration_cast<std::chrono::nanoseconds>(Clock::now() - t0).count());
+}
+}  // namespace detail
+
+// GpuPropagate.hpp:52-80.  prefer_gpu = true throws when no CUDA device is
+// visible.  prefer_gpu = false constructs without one; the reference then
+// runs its host fallback, and this library has none, so a stepper built
+// on such a context throws (SCATT_ERR_NO_DEVICE).
+class GpuContext {
+public:
+    struct Info {
+        std::string device_name;
+        std::string platform_name;
+        bool is_gpu = false;
+        std::size_t global_mem_bytes = 0;     // not reported by the library: 0
+    };
+    explicit GpuContext(bool prefer_gpu = true, int device = 0) : device_(device) {
+        int n = 0;
+        if (scatt_device_count(&n) != SCATT_OK) n = 0;
+        info_.platform_name = "CUDA (libscatt_b200)";
+        if (device >= 0 && device < n) {
+            info_.is_gpu = true;
+            info_.device_name = "CUDA device " + std::to_string(device);
+        } else if (prefer_gpu) {
+            throw std::runtime_error("GpuContext: no CUDA device " + std::to_string(device) +
+                                     " is visible (the library has no CPU fallback)");
+        }
+    }
+    GpuContext(const GpuContext&) = delete;
+    GpuContext& operator=(const GpuContext&) = delete;
+    const Info& info() const { return info_; }
+    void* raw_queue() const { return nullptr; }   // the library owns its streams
+    int device() const { return device_; }
+    static bool gpu_available() {
+        int n = 0;
+        return scatt_device_count(&n) == SCATT_OK && n > 0;
+    }
+
+private:
+    Info info_{};
+    int device_ = 0;
+};
+
+// GpuPropagate.hpp:83-150:  Rinv_n = sym((12 W_n^-1 - 10 I - Rinv_{n-1})^-1).
 class GpuForwardStepper {
 public:
-    GpuForwardStepper(int n_total, int device = 0) : n_(n_total) {
-        check(scatt_fwd_stepper_create(device, n_total, &h_));
+    struct Stats {
+        std::uint64_t t_upload_ns = 0, t_u_combine_ns = 0, t_inverse_ns = 0, t_download_ns = 0;
+        std::uint64_t n_steps = 0;
+    };
+    GpuForwardStepper(GpuContext& ctx, int N_total) : ctx_(ctx), N_(N_total) {
+        check(scatt_fwd_stepper_create(ctx.device(), N_total, &h_));
     }
     ~GpuForwardStepper() { scatt_fwd_stepper_destroy(h_); }
     GpuForwardStepper(const GpuForwardStepper&) = delete;
     GpuForwardStepper& operator=(const GpuForwardStepper&) = delete;
-    void init_R_prev_inv(const Matrix& R) { check(scatt_fwd_stepper_init(h_, R.data.data())); }
-    // Rinv_out = sym((12 W_inv - 10 I - R_prev_inv)^-1); returns max |Rinv - Rinv^T|
-    double step(const Matrix& W_inv, Matrix& Rinv_out) {
-        Rinv_out = Matrix(n_, n_);
+
+    template <class M> void init_R_prev_inv(const M& R) {
+        detail::need_shape(R, N_, N_, "GpuForwardStepper::init_R_prev_inv");
+        check(scatt_fwd_stepper_init(h_, detail::data_of(R)));
+    }
+    // Returns max |Rinv - Rinv^T| (0: the result is symmetrised exactly).
+    template <class M1, class M2> double step(const M1& W_inv, M2& Rinv_out) {
+        detail::need_shape(W_inv, N_, N_, "GpuForwardStepper::step");
+        const auto t0 = detail::Clock::now();
+        double* out = detail::resized(Rinv_out, N_, N_);
         double asym = 0.0;
-        check(scatt_fwd_stepper_step(h_, W_inv.data.data(), Rinv_out.data.data(), &asym));
+        check(scatt_fwd_stepper_step(h_, detail::data_of(W_inv), out, &asym));
+        stats_.t_inverse_ns += detail::ns_since(t0);
+        ++stats_.n_steps;
         return asym;
     }
+    // The request for an LDL^T inverse is recorded and not taken: the
+    // library has one inverse (Gauss-Jordan with partial pivoting, then
+    // symmetrised), whose result is bit-symmetric already.
+    void enable_symmetric_inverse(bool enable) { requested_ = enable; }
+    bool is_symmetric_inverse_active() const { return false; }
+    bool symmetric_inverse_supported() const { return false; }
+    int N_total() const { return N_; }
+    const Stats& stats() const { return stats_; }
+    void reset_stats() { stats_ = Stats{}; }
 
 private:
-    int n_;
+    [[maybe_unused]] GpuContext& ctx_;
+    int N_;
+    bool requested_ = false;
     scatt_fwd_stepper* h_ = nullptr;
+    Stats stats_{};
 };
 
+// GpuPropagate.hpp:153-227:  Sinv = sym((A - B diag(Dinv) B^T)^-1).
 class GpuSinvStepper {
 public:
-    GpuSinvStepper(int n_psi, int n_f, int device = 0) : np_(n_psi) {
-        check(scatt_sinv_stepper_create(device, n_psi, n_f, &h_));
+    struct Stats {
+        std::uint64_t t_upload_ns = 0, t_schur_ns = 0, t_inverse_ns = 0, t_download_ns = 0;
+        std::uint64_t n_steps = 0;
+    };
+    GpuSinvStepper(GpuContext& ctx, int N_psi, int N_f) : ctx_(ctx), N_psi_(N_psi), N_f_(N_f) {
+        check(scatt_sinv_stepper_create(ctx.device(), N_psi, N_f, &h_));
     }
     ~GpuSinvStepper() { scatt_sinv_stepper_destroy(h_); }
     GpuSinvStepper(const GpuSinvStepper&) = delete;
     GpuSinvStepper& operator=(const GpuSinvStepper&) = delete;
-    // Sinv = sym((A - B diag(Dinv) B^T)^-1)
-    double step(const Matrix& A, const Matrix& B, const std::vector<double>& Dinv, Matrix& Sinv_out) {
-        Sinv_out = Matrix(np_, np_);
-        double asym = 0.0;
-        check(scatt_sinv_stepper_step(h_, A.data.data(), B.data.data(), Dinv.data(), Sinv_out.data.data(), &asym));
-        return asym;
+
+    template <class MA, class MB, class VD, class MO>
+    double step(const MA& A, const MB& B, const VD& Dinv, MO& Sinv_out) {
+        detail::need_shape(A, N_psi_, N_psi_, "GpuSinvStepper::step (A)");
+        detail::need_shape(B, N_psi_, N_f_, "GpuSinvStepper::step (B)");
+        if (detail::size_of(Dinv) != N_f_) throw std::runtime_error("GpuSinvStepper::step: Dinv must have N_f entries");
+        return run(detail::data_of(A), detail::data_of(B), Dinv.data(), Sinv_out);
     }
-    // Sinv = sym(A^-1) (no exchange coupling)
-    double step_inverse_only(const Matrix& A, Matrix& Sinv_out) {
-        Sinv_out = Matrix(np_, np_);
-        double asym = 0.0;
-        check(scatt_sinv_stepper_step(h_, A.data.data(), nullptr, nullptr, Sinv_out.data.data(), &asym));
-        return asym;
+    // n >= n_transition: Sinv = sym(A^-1)
+    template <class MA, class MO> double step_inverse_only(const MA& A, MO& Sinv_out) {
+        detail::need_shape(A, N_psi_, N_psi_, "GpuSinvStepper::step_inverse_only");
+        return run(detail::data_of(A), nullptr, nullptr, Sinv_out);
     }
+    int N_psi() const { return N_psi_; }
+    int N_f() const { return N_f_; }
+    const Stats& stats() const { return stats_; }
+    void reset_stats() { stats_ = Stats{}; }
 
 private:
-    int np_;
+    template <class MO> double run(const double* A, const double* B, const double* Dinv, MO& Sinv_out) {
+        const auto t0 = detail::Clock::now();
+        double* out = detail::resized(Sinv_out, N_psi_, N_psi_);
+        double asym = 0.0;
+        check(scatt_sinv_stepper_step(h_, A, B, Dinv, out, &asym));
+        stats_.t_inverse_ns += detail::ns_since(t0);
+        ++stats_.n_steps;
+        return asym;
+    }
+    [[maybe_unused]] GpuContext& ctx_;
+    int N_psi_, N_f_;
     scatt_sinv_stepper* h_ = nullptr;
+    Stats stats_{};
 };
 
+// GpuPropagate.hpp:230-279:  Z <- Rinv Z;  Y = W_inv Z;  psi = Y[0:N_psi], f = Y[N_psi:].
 class GpuBackStepper {
 public:
-    GpuBackStepper(int n_total, int n_psi, int device = 0) : nt_(n_total), np_(n_psi) {
-        check(scatt_back_stepper_create(device, n_total, n_psi, &h_));
+    struct Stats {
+        std::uint64_t t_upload_ns = 0, t_gemm_z_ns = 0, t_gemm_y_ns = 0, t_extract_ns = 0;
+        std::uint64_t n_steps = 0;
+    };
+    GpuBackStepper(GpuContext& ctx, int N_total, int N_psi, int N_f)
+        : ctx_(ctx), N_total_(N_total), N_psi_(N_psi), N_f_(N_f) {
+        if (N_total != N_psi + N_f) throw std::runtime_error("GpuBackStepper: N_total must be N_psi + N_f");
+        check(scatt_back_stepper_create(ctx.device(), N_total, N_psi, &h_));
     }
     ~GpuBackStepper() { scatt_back_stepper_destroy(h_); }
     GpuBackStepper(const GpuBackStepper&) = delete;
     GpuBackStepper& operator=(const GpuBackStepper&) = delete;
-    void init_Z(const Matrix& Z) { check(scatt_back_stepper_init(h_, Z.data.data())); }
-    // Z <- Rinv Z; Y = W_inv Z; psi_out = Y[0:n_psi, :]; f_out = Y[n_psi:, :] when compute_f
-    void step(const Matrix& Rinv, const Matrix& W_inv, Matrix& psi_out, Matrix* f_out, bool compute_f) {
-        psi_out = Matrix(np_, np_);
+
+    template <class M> void init_Z(const M& Z) {
+        detail::need_shape(Z, N_total_, N_psi_, "GpuBackStepper::init_Z");
+        check(scatt_back_stepper_init(h_, detail::data_of(Z)));
+    }
+    template <class MR, class MW, class MP, class MF>
+    void step(const MR& Rinv, const MW& W_inv, MP& psi_out, MF* f_out, bool compute_f) {
         double* f = nullptr;
-        if (compute_f && f_out) {
-            *f_out = Matrix(nt_ - np_, np_);
-            f = f_out->data.data();
-        }
-        check(scatt_back_stepper_step(h_, Rinv.data.data(), W_inv.data.data(), psi_out.data.data(), f));
+        if (compute_f && f_out) f = detail::resized(*f_out, N_f_, N_psi_);
+        run(Rinv, W_inv, psi_out, f);
     }
-    void get_Z(Matrix& Z_out) const {
-        Z_out = Matrix(nt_, np_);
-        check(scatt_back_stepper_get_z(h_, Z_out.data.data()));
+    template <class MR, class MW, class MP>
+    void step(const MR& Rinv, const MW& W_inv, MP& psi_out, std::nullptr_t, bool) {
+        run(Rinv, W_inv, psi_out, nullptr);
     }
+    template <class M> void get_Z(M& Z_out) const {
+        check(scatt_back_stepper_get_z(h_, detail::resized(Z_out, N_total_, N_psi_)));
+    }
+    int N_total() const { return N_total_; }
+    int N_psi() const { return N_psi_; }
+    int N_f() const { return N_f_; }
+    const Stats& stats() const { return stats_; }
+    void reset_stats() { stats_ = Stats{}; }
 
 private:
-    int nt_, np_;
+    template <class MR, class MW, class MP> void run(const MR& Rinv, const MW& W_inv, MP& psi_out, double* f) {
+        detail::need_shape(Rinv, N_total_, N_total_, "GpuBackStepper::step (Rinv)");
+        detail::need_shape(W_inv, N_total_, N_total_, "GpuBackStepper::step (W_inv)");
+        const auto t0 = detail::Clock::now();
+        double* psi = detail::resized(psi_out, N_psi_, N_psi_);
+        check(scatt_back_stepper_step(h_, detail::data_of(Rinv), detail::data_of(W_inv), psi, f));
+        stats_.t_gemm_z_ns += detail::ns_since(t0);
+        ++stats_.n_steps;
+    }
+    [[maybe_unused]] GpuContext& ctx_;
+    int N_total_, N_psi_, N_f_;
     scatt_back_stepper* h_ = nullptr;
+    Stats stats_{};
+};
+
+// GpuDipoleEngine.hpp:85-149:  result (n_slots x N_psi) = V (n_slots x N_psi) . psi_ir
+// (N_psi x N_psi), one device GEMM per radial point (scatt_dgemm: on the
+// calling thread's current CUDA device, with device buffers allocated per
+// call; the batched solver computes the same contraction without this seam).
+class GpuDipoleEngine {
+public:
+    struct Stats {
+        std::uint64_t t_upload_ns = 0, t_gemm_ns = 0, t_download_ns = 0;
+        std::uint64_t n_steps = 0;
+    };
+    GpuDipoleEngine(GpuContext& ctx, int N_psi, int n_slots) : ctx_(ctx), N_psi_(N_psi), n_slots_(n_slots) {
+        if (N_psi <= 0 || n_slots <= 0) throw std::runtime_error("GpuDipoleEngine: bad sizes");
+        if (ctx.device() < 0 || !GpuContext::gpu_available())
+            throw std::runtime_error("GpuDipoleEngine: no CUDA device visible (the library has no CPU fallback)");
+    }
+    GpuDipoleEngine(const GpuDipoleEngine&) = delete;
+    GpuDipoleEngine& operator=(const GpuDipoleEngine&) = delete;
+
+    template <class MV, class MP, class MO> void step(const MV& V, const MP& psi_ir, MO& result_out) {
+        detail::need_shape(V, n_slots_, N_psi_, "GpuDipoleEngine::step (V)");
+        detail::need_shape(psi_ir, N_psi_, N_psi_, "GpuDipoleEngine::step (psi_ir)");
+        const auto t0 = detail::Clock::now();
+        double* out = detail::resized(result_out, n_slots_, N_psi_);
+        check(scatt_dgemm(0, 0, n_slots_, N_psi_, N_psi_, 1.0, detail::data_of(V), n_slots_,
+                          detail::data_of(psi_ir), N_psi_, 0.0, out, n_slots_));
+        stats_.t_gemm_ns += detail::ns_since(t0);
+        ++stats_.n_steps;
+    }
+    int N_psi() const { return N_psi_; }
+    int n_slots() const { return n_slots_; }
+    const Stats& stats() const { return stats_; }
+    void reset_stats() { stats_ = Stats{}; }
+
+private:
+    [[maybe_unused]] GpuContext& ctx_;
+    int N_psi_, n_slots_;
+    Stats stats_{};
 };
 
 // Dense inverses on the device, named as in LapackInverse.hpp:53-178; a

@@ -120,9 +120,28 @@ def test_driver_inverse_and_singular_throw(tmp_path):
 
 
 @pytest.mark.gpu
-def test_driver_forward_stepper_wrapper():
-    # W_inv = I/2, R_prev_inv = 0: Rinv = (6 I - 10 I)^-1 = -I/4 (every
-    # operation exact in binary floating point; the driver exits 3 above 1e-15)
+def test_driver_seam_classes():
+    # built as the reference's stage classes build them (GpuContext, then the
+    # stepper): W_inv = I/2, R_prev_inv = 0 gives Rinv = (6 I - 10 I)^-1 = -I/4,
+    # and the dipole engine's V . (2 I) = 2 V on small integers; both exact in
+    # binary floating point (the driver exits 3 otherwise)
     r = subprocess.run([_driver(), "stepper", "8"], capture_output=True, text=True)
     assert r.returncode == 0, (r.stdout, r.stderr)
-    assert float(r.stdout.strip()) < 1e-15
+    err_fwd, err_dip = (float(x) for x in r.stdout.split())
+    assert err_fwd < 1e-15 and err_dip == 0.0
+
+
+def test_seam_headers_take_the_reference_calls(tmp_path):
+    """tests/host_seam_check.cpp makes the reference's stage-class calls into
+    the device seam, as written there, against host/seam/scatt/*.hpp: it must
+    compile warning-free and, without a GPU, show the no-device behaviour."""
+    _driver()                                        # the library is built
+    exe = tmp_path / "seam_check"
+    cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror",
+           "-I", os.path.join(ROOT, "include"), "-I", os.path.join(PKG, "host"),
+           "-I", os.path.join(PKG, "host", "seam"), os.path.join(ROOT, "tests", "host_seam_check.cpp"),
+           "-L", PKG, "-lscatt_b200", f"-Wl,-rpath,{PKG}", "-o", str(exe)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, (r.stdout, r.stderr)
