@@ -30,7 +30,8 @@ analytic start and an independent LU recursion, the three-point Numerov
 identity on the back-propagated solution, K symmetry, S unitarity,
 eigenphases, matching-radius invariance, the asymptotic-fit checks, the
 setup rules, the per-channel length/velocity gauge identity, the channel
-potential and the real Gaunt coefficients to l = 50.
+potential and the real Gaunt coefficients to l = 50.  K is also held to
+exact phase shifts of a short-range well (tests/test_oracle_phase_shifts.py).
 
 oracle/adjoint.py is the gradient checker for the adjoint (the reference
 has none): the forward path restated in float64 torch and differentiated by
