@@ -78,3 +78,32 @@ def test_K_meets_the_exact_phase_shifts(runs):
         assert 1.8 < e1 / e2 < 2.2                                  # first order in dr
         assert abs(2.0 * K2[mu] - K1[mu] - target) < 2e-4           # Richardson
         assert abs(e2) < 0.02                                      # and close already at dr = 0.005
+
+
+def test_dipole_phase_and_time_delay_follow_delta():
+    """For one open channel D = conj((A - iB)^-1) d with d real, so arg D is
+    +delta (the two sign choices above cancel) and the time delay of the
+    default convention (oracle/observables.py, cross_section_delay.py) is the
+    Wigner delay d delta / dE.  The s-like initial state reaches l = 1, m = 0
+    in z only.  At dr = 0.005 both sit within the first-order grid error."""
+    from oracle import observables as OBS
+    dr, Nr = 0.005, 8001
+    r = np.arange(Nr) * dr
+    F = np.zeros((1, 1, Nr))
+    F[0, 0] = 1e-8 * 2.0 * np.exp(-r)
+    inp = ScanInputs(name="well", dr=dr, Nr=Nr, l_cont=2, atoms=np.zeros((0, 4)), psi_lm=F,
+                     orb_energies=np.array([-0.5]), n_occ=1, V_H=(math.sqrt(4.0 * math.pi) * U(r))[None, :])
+    st = O.make_setup(inp)
+    Es = [0.49, 0.5, 0.51]
+    res = [O.solve_energy(st, E_) for E_ in Es]
+    k = [math.sqrt(2.0 * E_) for E_ in Es]
+    mu = 2                                                    # l = 1, m = 0
+    D = [list(x.slices[2]["D"]) for x in res]                 # (L, z)
+    assert all(abs(d) <= 1e-12 * abs(row[mu]) for row in D for i, d in enumerate(row) if i != mu)
+    delta = exact_delta(1, k[1], 40.0)
+    assert abs(np.angle(D[1][mu]) - delta) < 0.01
+    h = 1e-4
+    ddelta_dE = (exact_delta(1, math.sqrt(2.0 * (Es[1] + h)), 40.0)
+                 - exact_delta(1, math.sqrt(2.0 * (Es[1] - h)), 40.0)) / (2.0 * h)
+    tau = OBS.time_delay(k, D)[1]
+    assert ddelta_dE > 0 and abs(tau - ddelta_dE) < 0.03 * ddelta_dE
