@@ -13,11 +13,22 @@ with dD/dE = (dD/dk) / k, dD/dk by second-order finite differences on the
 (possibly uneven) k grid (one-sided at the ends), and omega = E - E_HOMO
 (src/scatt/DipoleIO.cpp:285).  D is the orthogonalised reduced dipole
 (DipoleResult::D_reduced) of one slot; the six slots are (L,x) (L,y) (L,z)
-(V,x) (V,y) (V,z).
+(V,x) (V,y) (V,z).  Also, as cross_section_delay.py:270-430 computes them:
+
+    dphi_rms = sqrt( sum w dphi^2 / sum w ),  dphi = arg(D^V conj D^L),  w = |D^L| |D^V|
+    beta     = N_1 / sigma_tot - 1   (orientation-averaged asymmetry, linear polarisation)
+    sigma_tot = 1/3 int dOmega sum_q |D^(q)(k)|^2,   N_1 = int dOmega |sum_q D^(q)(k) k_q|^2,
+    D^(q)(k) = sum_lm d^(q)_lm Y^R_lm(k)
+
+with the integrals on a Gauss-Legendre (cos theta) x trapezoid (phi) grid,
+40 x 80 by default, which is exact while 2 (l_max + 1) < 80.
 """
 from __future__ import annotations
 
+import math
+
 import numpy as np
+from scipy.special import sph_harm_y
 
 C_AU = 137.036            # speed of light, atomic units
 AU_TO_AS = 24.18884       # atomic unit of time in attoseconds
@@ -60,6 +71,54 @@ def q_sigma(D_L, D_V, omega) -> np.ndarray:
     return np.divide(num, den, out=np.full_like(num, np.nan), where=den > 1e-30)
 
 
+def dphi_rms(D_L, D_V) -> np.ndarray:
+    """Weighted rms phase difference between the gauges, per energy
+    (cross_section_delay.py:270-275); D_L, D_V: (n_energy, n_channels)."""
+    D_L = np.asarray(D_L, dtype=np.complex128)
+    D_V = np.asarray(D_V, dtype=np.complex128)
+    dphi = np.angle(D_V * np.conj(D_L))
+    w = np.abs(D_L) * np.abs(D_V)
+    s_w = np.sum(w, axis=1)
+    s_w_phi2 = np.sum(w * dphi ** 2, axis=1)
+    return np.sqrt(np.divide(s_w_phi2, s_w, out=np.zeros_like(s_w_phi2), where=s_w > 1e-30))
+
+
+def real_ylm(l: int, m: int, theta, phi):
+    """Real spherical harmonic without the Condon-Shortley phase
+    (src/angular/Gaunt.hpp:171-181): x <-> m = +1, y <-> m = -1, z <-> m = 0."""
+    am = abs(m)
+    if m == 0:
+        return np.real(sph_harm_y(l, 0, theta, phi))
+    if m > 0:
+        return math.sqrt(2.0) * (-1.0) ** m * np.real(sph_harm_y(l, m, theta, phi))
+    return math.sqrt(2.0) * (-1.0) ** am * np.imag(sph_harm_y(l, am, theta, phi))
+
+
+def beta(D_x, D_y, D_z, mu_list=None, n_theta: int = 40, n_phi: int = 80) -> np.ndarray:
+    """Orientation-averaged asymmetry parameter per energy, in [-1, 2]
+    (cross_section_delay.py:350-430).  D_q: (n_energy, n_channels) dipoles of
+    the three polarisations; mu_list: the lm index of each channel (default
+    0 .. n_channels - 1)."""
+    D = [np.asarray(d, dtype=np.complex128) for d in (D_x, D_y, D_z)]
+    n_ch = D[0].shape[1]
+    mu_list = list(range(n_ch)) if mu_list is None else list(mu_list)
+    x, w = np.polynomial.legendre.leggauss(n_theta)
+    theta = np.arccos(x)
+    phi = np.arange(n_phi) * (2.0 * np.pi / n_phi)
+    TH, PH = np.meshgrid(theta, phi, indexing="ij")
+    Y = np.empty((n_ch, n_theta, n_phi))
+    for i, mu in enumerate(mu_list):
+        l = int(math.isqrt(mu))
+        Y[i] = real_ylm(l, mu - l * l - l, TH, PH)
+    weights = w[:, None] * (2.0 * np.pi / n_phi)
+    maps = [np.tensordot(d, Y, axes=([1], [0])) for d in D]          # (n_energy, n_theta, n_phi)
+    sigma_tot = np.sum((np.abs(maps[0]) ** 2 + np.abs(maps[1]) ** 2 + np.abs(maps[2]) ** 2)
+                       * weights, axis=(1, 2)) / 3.0
+    k_dot = maps[0] * (np.sin(TH) * np.cos(PH)) + maps[1] * (np.sin(TH) * np.sin(PH)) + maps[2] * np.cos(TH)
+    N1 = np.sum(np.abs(k_dot) ** 2 * weights, axis=(1, 2))
+    return np.divide(N1, sigma_tot, out=np.ones_like(N1), where=sigma_tot > 1e-30) - 1.0
+
+
 def scan_observables(results, e_homo: float) -> dict:
     """Cross sections, delays and q for every polarisation of a scan.
 
@@ -78,4 +137,7 @@ def scan_observables(results, e_homo: float) -> dict:
         DL = np.stack([r.D[p] for r in res])
         DV = np.stack([r.D[3 + p] for r in res])
         out[f"q_{pol}"] = q_sigma(DL, DV, omega)
+        out[f"dphi_rms_{pol}"] = dphi_rms(DL, DV)
+    for g, gauge in enumerate(("length", "velocity")):
+        out[f"beta_{gauge}"] = beta(*(np.stack([r.D[3 * g + p] for r in res]) for p in range(3)))
     return out

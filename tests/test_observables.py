@@ -49,3 +49,65 @@ def test_gauge_ratio_is_one_when_dv_equals_omega_dl():
     assert np.allclose(OBS.q_sigma(DL, DV, om), 1.0, rtol=1e-13)
     assert np.allclose(OBS.cross_section(k, DL, om, "length"), OBS.cross_section(k, DV, om, "velocity"),
                        rtol=1e-13)
+
+
+def _three_pols(n_e=2, l_max=3, seed=5):
+    rng = np.random.default_rng(seed)
+    n = (l_max + 1) ** 2
+    return [rng.standard_normal((n_e, n)) + 1j * rng.standard_normal((n_e, n)) for _ in range(3)]
+
+
+def test_dphi_rms_and_beta_match_the_oracle():
+    DL, DV, _ = _three_pols(3, 3, seed=6)
+    assert np.allclose(OBS.dphi_rms(DL, DV), OO.dphi_rms([list(r) for r in DL], [list(r) for r in DV]),
+                       rtol=1e-13, atol=0)
+    D = _three_pols(2, 2)
+    got = OBS.beta(*D, n_theta=12, n_phi=24)
+    ref = OO.beta(*[[list(r) for r in d] for d in D], n_theta=12, n_phi=24)
+    assert np.allclose(got, ref, rtol=1e-12, atol=1e-13)
+
+
+def test_beta_limits():
+    # atomic s -> p: D^(q) on the l = 1 channel along q gives beta = 2
+    D = [np.zeros((1, 4), complex) for _ in range(3)]
+    D[0][0, 3] = D[1][0, 1] = D[2][0, 2] = 0.7 - 0.2j          # (1, +1) = x, (1, -1) = y, (1, 0) = z
+    assert abs(OBS.beta(*D)[0] - 2.0) < 1e-13
+    # D^(q)(k) = (k x a)_q has no component along k: N_1 = 0, beta = -1
+    ax, ay, az = 0.3, -1.1, 0.8 + 0.4j
+    X, Y, Z = 3, 1, 2                                           # l = 1 channels along x, y, z
+    D = [np.zeros((1, 4), complex) for _ in range(3)]
+    D[0][0, Y], D[0][0, Z] = az, -ay                           # k_y a_z - k_z a_y
+    D[1][0, Z], D[1][0, X] = ax, -az                           # k_z a_x - k_x a_z
+    D[2][0, X], D[2][0, Y] = ay, -ax                           # k_x a_y - k_y a_x
+    assert abs(OBS.beta(*D)[0] + 1.0) < 1e-13
+    # and any amplitudes stay within [-1, 2]
+    b = OBS.beta(*_three_pols(50, 6, seed=7))
+    assert np.all(b >= -1.0 - 1e-12) and np.all(b <= 2.0 + 1e-12)
+
+
+def test_beta_quadrature_is_exact_below_its_degree():
+    """N_1 = (4 pi / 3) sum_lambda |sum_{q, mu} d^(q)_mu G(mu; 1 q; lambda)|^2 in
+    real Gaunt coefficients and sigma_tot = 1/3 sum |d|^2 (orthonormality):
+    the default 40 x 80 grid reproduces this closed form while 2 (l_max + 1) < 80."""
+    from oracle import angular
+    l_max = 6
+    D = _three_pols(2, l_max, seed=8)
+    n = (l_max + 1) ** 2
+    lms = [angular.idx_to_lm(i) for i in range(n)]
+    qs = (1, -1, 0)                                           # x, y, z
+    exact = []
+    for e in range(2):
+        sig = sum(np.sum(np.abs(d[e]) ** 2) for d in D) / 3.0
+        amp = {}
+        for qi, q in enumerate(qs):
+            for i, (l, m) in enumerate(lms):
+                for lam in (l - 1, l + 1):
+                    if lam < 0:
+                        continue
+                    for mlam in range(-lam, lam + 1):
+                        g = angular.gaunt_real(l, m, 1, q, lam, mlam)
+                        if g != 0.0:
+                            amp[(lam, mlam)] = amp.get((lam, mlam), 0.0) + D[qi][e, i] * g
+        N1 = 4.0 * np.pi / 3.0 * sum(abs(a) ** 2 for a in amp.values())
+        exact.append(N1 / sig - 1.0)
+    assert np.allclose(OBS.beta(*D), exact, rtol=1e-12, atol=1e-13)
