@@ -44,7 +44,8 @@ CHI_CUTOFF = 1e-15     # WavefunctionSetup.hpp:92
 # variant, LapackInverse.hpp:88-91 and :166-176).  The oracle follows the
 # Eigen build by default (BUILD = "eigen"); BUILD = "mkl" selects the MKL
 # routines.  The two builds differ from each other by O(eps * cond) per step;
-# on the synthetic configs that reaches ~2e-10 in K.
+# on the synthetic H2- and H2O-like inputs that reaches ~2e-10 in K, which is
+# the floor the GPU parity tolerances are set against.
 BUILD = "eigen"
 
 
