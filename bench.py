@@ -46,9 +46,9 @@ CONFIGS = {
 }
 
 
-# DRAM bytes (read + write) of one batched R^-1 inversion, summed over its
-# kernels from an ncu launch-list capture of the same call
-# (profiles/gj_inverse_n1046_b32.md); algorithmic minimum ~10.1 GB.
+# DRAM bytes (read + write) of one batched R^-1 inversion (order 1046, batch
+# 32), summed over its kernels in one ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum) of the same call; the algorithmic minimum is ~10.1 GB.
 INVERSE_TRAFFIC = {(1046, 32): 11.21e9}
 
 
