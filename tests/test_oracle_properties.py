@@ -102,3 +102,26 @@ def test_setup_rules(name):
     ir = 5
     ref = ir * inp.dr * psi[:inp.n_occ, :nl, ir]
     assert np.max(np.abs(st.chi_r[:, :nl, ir] - ref)) < 1e-14
+
+
+def test_orbital_truncation_only_crops():
+    """src/tests/test_orbital_truncation.cpp: orbitals stored on a cropped
+    grid (Nr_store < Nr, Nlm_store < the file's) give the same chi, and here
+    the same K and dipoles bit for bit, as long as the crop keeps
+    n_transition; a crop below it caps n_transition at Nr_store
+    (WavefunctionSetup.cpp:278-324)."""
+    import dataclasses
+    full = synth.h2o_like(Nr=1201, dr=0.05, l_cont=3, lmax_orb=6, n_orb=3)
+    st_full = O.make_setup(full)
+    n_tr = st_full.n_tr
+    assert n_tr < full.Nr
+    cropped = dataclasses.replace(full, psi_lm=np.ascontiguousarray(full.psi_lm[:, :st_full.n_lambda, :n_tr]))
+    st_c = O.make_setup(cropped)
+    assert st_c.n_tr == n_tr
+    assert np.array_equal(st_c.chi_r, st_full.chi_r) and np.array_equal(st_c.chi_init, st_full.chi_init)
+    a, b = O.solve_energy(st_full, 0.8), O.solve_energy(st_c, 0.8)
+    assert np.array_equal(a.K_kme, b.K_kme)
+    for s in range(6):
+        assert np.array_equal(a.slices[s]["D"], b.slices[s]["D"])
+    short = dataclasses.replace(full, psi_lm=np.ascontiguousarray(full.psi_lm[:, :, : n_tr - 50]))
+    assert O.make_setup(short).n_tr == n_tr - 50
