@@ -111,3 +111,29 @@ def test_beta_quadrature_is_exact_below_its_degree():
         N1 = 4.0 * np.pi / 3.0 * sum(abs(a) ** 2 for a in amp.values())
         exact.append(N1 / sig - 1.0)
     assert np.allclose(OBS.beta(*D), exact, rtol=1e-12, atol=1e-13)
+
+
+def test_scan_observables_on_solver_shaped_results():
+    """scan_observables reads .E and .D (six slots of N_psi dipoles) of the
+    solver's per-energy results, sorts them by energy and returns every
+    observable keyed by gauge and polarisation."""
+    from types import SimpleNamespace
+    rng = np.random.default_rng(9)
+    n_mu, Es = 9, [0.9, 0.5, 0.7, 0.6]
+    res = [SimpleNamespace(E=E, D=[rng.standard_normal(n_mu) + 1j * rng.standard_normal(n_mu) for _ in range(6)])
+           for E in Es]
+    obs = OBS.scan_observables(res, e_homo=-0.6)
+    order = np.argsort(Es)
+    k = np.sqrt(2.0 * np.array(Es)[order])
+    assert np.allclose(obs["k"], k)
+    for s, (gauge, pol) in enumerate(OBS.SLOTS):
+        D = np.stack([res[i].D[s] for i in order])
+        assert np.allclose(obs[f"sigma_{gauge}_{pol}"], OBS.cross_section(k, D, obs["omega"], gauge))
+        assert np.allclose(obs[f"tau_{gauge}_{pol}"], OBS.time_delay(k, D))
+    for p, pol in enumerate("xyz"):
+        DL = np.stack([res[i].D[p] for i in order])
+        DV = np.stack([res[i].D[3 + p] for i in order])
+        assert np.allclose(obs[f"dphi_rms_{pol}"], OBS.dphi_rms(DL, DV))
+    for g, gauge in enumerate(("length", "velocity")):
+        b = obs[f"beta_{gauge}"]
+        assert b.shape == (len(Es),) and np.all((b >= -1 - 1e-12) & (b <= 2 + 1e-12))
