@@ -1,5 +1,7 @@
-"""Cross sections and Wigner delays of a scan (host arithmetic on the solver's
-dipoles) against the oracle's loop restatement and an analytic phase."""
+"""Scan observables (host arithmetic on the solver's dipoles): cross
+sections, Wigner delays, the gauge ratio and phase spread, and the asymmetry
+parameter beta, against the oracle's loop restatement, an analytic phase,
+the beta limits and a closed form of beta in real Gaunt coefficients."""
 import numpy as np
 
 from oracle import observables as OO
