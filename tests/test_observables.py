@@ -139,3 +139,25 @@ def test_scan_observables_on_solver_shaped_results():
     for g, gauge in enumerate(("length", "velocity")):
         b = obs[f"beta_{gauge}"]
         assert b.shape == (len(Es),) and np.all((b >= -1 - 1e-12) & (b <= 2 + 1e-12))
+
+
+def test_against_the_reference_code():
+    """tests/golden/observables_vectors.json holds seeded dipoles and what the
+    reference's own postprocessing/cross_section_delay.py computed from them
+    (tests/golden/make_observables_golden.py): sigma, tau in both sign
+    conventions, q, dphi_rms and beta."""
+    import json
+    import os
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "observables_vectors.json")))
+    k, om = np.array(g["k"]), np.array(g["omega"])
+    D = [np.array(re) + 1j * np.array(im) for re, im in zip(g["D_re"], g["D_im"])]
+    for s, (gauge, pol) in enumerate(OBS.SLOTS):
+        assert np.allclose(OBS.cross_section(k, D[s], om, gauge), g[f"sigma_{gauge}_{pol}"], rtol=1e-14, atol=0)
+        assert np.allclose(OBS.time_delay(k, D[s]), g[f"tau_{gauge}_{pol}"], rtol=1e-13, atol=1e-15)
+        assert np.allclose(OBS.time_delay(k, D[s], with_minus=True), g[f"tau_minus_{gauge}_{pol}"],
+                           rtol=1e-13, atol=1e-15)
+    for p, pol in enumerate("xyz"):
+        assert np.allclose(OBS.q_sigma(D[p], D[3 + p], om), g[f"q_{pol}"], rtol=1e-14, atol=0)
+        assert np.allclose(OBS.dphi_rms(D[p], D[3 + p]), g[f"dphi_rms_{pol}"], rtol=1e-14, atol=0)
+    for i, gauge in enumerate(("length", "velocity")):
+        assert np.allclose(OBS.beta(D[3 * i], D[3 * i + 1], D[3 * i + 2]), g[f"beta_{gauge}"], rtol=1e-12, atol=1e-14)
