@@ -43,3 +43,28 @@ def test_compute_entry_points_fail_loudly_without_device():
                                             _lib.as_dptr(np.zeros_like(A)), 0, None)
     assert code == 7          # SCATT_ERR_NO_DEVICE: no CPU fallback
     assert b"no CUDA device" in _lib.lib().scatt_last_error()
+
+
+def test_every_compute_entry_point_reports_no_device():
+    """Without a CUDA device every compute entry point returns
+    SCATT_ERR_NO_DEVICE (7) with the library's message: there is no CPU
+    path behind any of them."""
+    if _lib.device_count() > 0:
+        return
+    L = _lib.lib()
+    A = np.ascontiguousarray(np.eye(4)[None])
+    out = np.zeros_like(A)
+    C = np.zeros((4, 4))
+    ms = np.zeros(1)
+    calls = {
+        "scatt_inverse_batched": lambda: L.scatt_inverse_batched(4, 1, _lib.as_dptr(A), _lib.as_dptr(out), 0, None),
+        "scatt_inverse_batched_noalloc": lambda: L.scatt_inverse_batched_noalloc(
+            4, 1, _lib.as_dptr(A), _lib.as_dptr(out), 0, None),
+        "scatt_dgemm": lambda: L.scatt_dgemm(0, 0, 4, 4, 4, 1.0, _lib.as_dptr(C), 4, _lib.as_dptr(C), 4, 0.0,
+                                             _lib.as_dptr(C), 4),
+        "scatt_bench_inverse": lambda: L.scatt_bench_inverse(8, 1, 1, _lib.as_dptr(ms)),
+        "scatt_ctx_create": lambda: L.scatt_ctx_create(0, ctypes.byref(ctypes.c_void_p())),
+    }
+    for name, call in calls.items():
+        assert call() == 7, name
+        assert b"no CUDA device" in L.scatt_last_error(), name
