@@ -68,3 +68,16 @@ def test_every_compute_entry_point_reports_no_device():
     for name, call in calls.items():
         assert call() == 7, name
         assert b"no CUDA device" in L.scatt_last_error(), name
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """The package has no fallback when the built library is absent: the
+    first use raises with the build instruction."""
+    monkeypatch.setattr(_lib, "_lib", None)
+    monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "libscatt_b200.so"))
+    try:
+        _lib.lib()
+    except _lib.ScattError as e:
+        assert "is missing" in str(e) and "build.py" in str(e)
+    else:
+        raise AssertionError("lib() returned without the library")
