@@ -645,3 +645,91 @@ def solve_energy(st: Setup, E: float, keep_rinv=False, keep_psi=False) -> Energy
     return EnergyResult(E, kme["K"], kme, aa, slices, b_overlap,
                         psi_keep=psi if keep_psi else {}, rinv=Rinv if keep_rinv else None,
                         shifts=counts)
+
+
+def solve_energy_lean(st: Setup, E: float, seg: int = 256, psi_dir: str | None = None) -> EnergyResult:
+    """solve_energy with bounded memory, for the full-size grids.
+
+    The same stage functions in the same order as solve_energy, so the same
+    arithmetic: the forward recurrence keeps Rinv only at segment ends (every
+    `seg` steps) and the backward sweep recomputes each segment's Sinv and
+    Rinv from its checkpoint before walking it downward, as the reference's
+    checkpointed stages do when R^-1 does not fit in memory
+    (ForwardRPropagator.cpp:244-382, BackPropagator.cpp:533-703).  psi over
+    [0, n_transition) -- 1.56 MB a point at l_cont = 20 -- goes to a
+    disk-backed array under psi_dir (a temporary directory by default).
+    """
+    import os
+    import tempfile
+    Nr, Nt, Np = st.Nr, st.Nt, st.n_mu
+    counts = {"A": 0, "S": 0}
+    ns = n_start(st)
+
+    def rinv_range(a, b, prev, cnt=None):
+        """Sinv(n), Rinv(n) for n in [a, b), from Rinv(a-1) = prev."""
+        S, R = {}, {}
+        for n in range(a, b):
+            S[n] = sinv_at(st, E, n, cnt)
+            if n < ns:
+                R[n] = analytic_init(st, E, n)
+            else:
+                R[n] = frp_step(st, n, S[n], prev)
+            prev = R[n]
+        return S, R
+
+    ck = {}                      # ck[a] = Rinv(a - 1), the state entering segment [a, a + seg)
+    prev = None
+    keep_match = None
+    n_match = Nr - 2
+    for a in range(0, Nr, seg):
+        b = min(Nr, a + seg)
+        ck[a] = prev
+        _, R = rinv_range(a, b, prev, counts)
+        prev = R[b - 1]
+        if a <= n_match < b:
+            keep_match = R[n_match]
+    kme = kme_extract(st, E, keep_match, n_match)
+    bc = psi_boundary(st, E, kme["K"])
+    N = Nr - 1
+    n_keep_hi = min(Nr - 1, max(1, st.n_tr - 1))
+    asym_lo = N - N_ASYM + 1
+    Dinv_N = dinv_at(st, N)
+    B_N = B_at(st, N)
+    f_N = -(Dinv_N[:, None] * (B_N.T @ bc))
+    h2_6 = st.dr * st.dr / 6.0
+    Z = np.zeros((Nt, Np))
+    Z[:Np] = bc + h2_6 * E * bc - h2_6 * V_at(st, N) @ bc + B_N @ f_N
+    tmp = tempfile.mkdtemp(dir=psi_dir)
+    store = np.lib.format.open_memmap(os.path.join(tmp, "psi.npy"), mode="w+",
+                                      dtype=np.float64, shape=(n_keep_hi + 1, Np, Np))
+    psi = {}
+
+    def keep(n, p):
+        if n <= n_keep_hi:
+            store[n] = p
+        if n >= asym_lo:
+            psi[n] = p.copy()
+
+    keep(N, bc)
+    starts = sorted(ck)
+    for a in reversed(starts):
+        b = min(Nr, a + seg)
+        lo_n, hi_n = a, min(b, N)           # the sweep visits n = N-1 .. 0
+        if lo_n >= hi_n:
+            continue
+        S, R = rinv_range(a, b, ck[a])
+        for n in range(hi_n - 1, lo_n - 1, -1):
+            Z = R[n] @ Z
+            Y = winv_apply(st, n, S[n], Z)
+            keep(n, Y[:Np])
+        del S, R
+    aa = aa_extract(st, E, psi)
+    n_hi = min(Nr, n_keep_hi + 1)
+    slices, b_overlap = dme_compute_six(st, aa["A"], aa["B"], lambda ir: store[ir], 0, n_hi)
+    del store
+    try:
+        os.remove(os.path.join(tmp, "psi.npy"))
+        os.rmdir(tmp)
+    except OSError:
+        pass
+    return EnergyResult(E, kme["K"], kme, aa, slices, b_overlap, shifts=counts)

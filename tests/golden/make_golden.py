@@ -5,15 +5,17 @@ Reads (text only, nothing is compiled or run):
   src/tests/test_gaunt.cpp               permutation-symmetry cases
   src/tests/test_freeparticle_dipole.cpp free-particle k list, grid and tolerances
 
-Run in a checkout that has the reference at REF (default /root/reference):
-    python tests/golden/make_golden.py [REF]
+Run with the path of a reference checkout as REF (required):
+    python tests/golden/make_golden.py REF
 """
 import json
 import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit(f"usage: python {sys.argv[0]} REFERENCE_CHECKOUT")
+REF = sys.argv[1]
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

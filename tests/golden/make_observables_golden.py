@@ -1,13 +1,13 @@
 """Golden vectors of the reference's own observables code
 (postprocessing/cross_section_delay.py), run on seeded dipoles.
 
-The reference module is imported from REF (default /root/reference) and
+The reference module is imported from REF (the required first argument) and
 its numerical functions run unmodified: sigma_from_dipole, time_delay (both
 sign conventions), q_sigma, dphi_rms and compute_beta.  Only its plotting
 uses matplotlib, which this image lacks, so a stand-in module with use()
 and pyplot is put into sys.modules before the import.
 
-    python tests/golden/make_observables_golden.py [REF]
+    python tests/golden/make_observables_golden.py REF
 """
 import json
 import os
@@ -16,7 +16,9 @@ import types
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit(f"usage: python {sys.argv[0]} REFERENCE_CHECKOUT")
+REF = sys.argv[1]
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
