@@ -1,24 +1,30 @@
 """Benchmark: FP64 scan energies/sec of the per-energy scattering path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config h2o_like|h2_like] [--batch B]
+                    [--config h2o_like|h2_like] [--slots S] [--groups G]
+                    [--graphs 0|1] [--autotune 0|1]
 
 Workload (default): the H2O-like system -- O + 2 H, five doubly occupied
 orbitals, l_cont = 20 (441 continuum + 605 exchange channels, N_t = 1046),
 dr = 0.005 bohr, 12001 radial points, momenta k = 0.05 .. 2.0 (200 energies).
 Inputs are seeded synthetic data of those shapes (no molecular file exists
-here).  A step is one batch of B energies taken in order from the k grid,
-solved end to end (Schur inverses, R-ratio recurrence, K, asymptotic fit,
-dipoles).  Under torchrun each rank takes its own contiguous block of the k
-grid (energies are independent: weak scaling, no data-path collective).
+here).  The energies stream through the library's scan (scatt_scan_*): S
+device slots in G phase groups started a fraction 1/G of the radial sweep
+apart; a step is one group finishing -- S/G energies solved end to end
+(Schur inverses, R-ratio recurrence, K, asymptotic fit, dipoles) while the
+other groups advance by 1/G of their sweep -- and the finished slots take the
+next energies of the k grid at once.  Under torchrun each rank streams its
+own contiguous block of the k grid (energies are independent: weak scaling,
+no data-path collective).
 
 value      energies/s of the whole job over the timed steps, device time
            (CUDA events on the library's stream), max over ranks;
-e2e        the same energies through the C ABI with host buffers (energies
-           in, every output back in host memory), host clock;
+e2e        the same steps through the C ABI with host buffers: energies
+           submitted from host memory, every output of the finished energies
+           read back into pinned host memory, host clock, max over ranks;
 roofline   the dominant kernel group -- the batched R^-1 inversion -- as
-           achieved FP64 TF/s against the cuBLAS DGEMM peak measured on this
-           GPU in the same run;
+           achieved FP64 TF/s (2 n^3 per matrix, over the sampled inversions)
+           against the cuBLAS DGEMM peak measured on this GPU in the same run;
 cpu_baseline  the oracle port timed on a bounded sample of the same workload
            on this host's cores, extrapolated to energies/s.
 """
@@ -40,16 +46,16 @@ import numpy as np  # noqa: E402
 
 CONFIGS = {
     "h2o_like": dict(builder="h2o_like", kw=dict(Nr=12001, dr=0.005, l_cont=20, lmax_orb=40, n_orb=5),
-                     ks=lambda: np.linspace(0.05, 2.0, 200), batch=32),
+                     ks=lambda: np.linspace(0.05, 2.0, 200), slots=32, groups=8, graphs=0),
     "h2_like": dict(builder="h2_like", kw=dict(Nr=4001, dr=0.01, l_cont=8),
-                    ks=lambda: np.arange(1, 21) * 0.1, batch=20),
+                    ks=lambda: np.arange(1, 21) * 0.1, slots=20, groups=4, graphs=1),
 }
 
 
-# DRAM bytes (read + write) of one batched R^-1 inversion (order 1046, batch
-# 32), summed over its kernels in one ncu capture (dram__bytes_read.sum +
-# dram__bytes_write.sum) of the same call; the algorithmic minimum is ~10.1 GB.
-INVERSE_TRAFFIC = {(1046, 32): 11.21e9}
+# DRAM bytes (read + write) per sampled R^-1 inversion of the scan, from one
+# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum summed over the
+# inversion's kernels), keyed by (config, slots, groups).
+INVERSE_TRAFFIC: dict = {}
 
 
 def dist_env():
@@ -173,14 +179,30 @@ def oracle_baseline(st, ks, budget_s=20.0):
     }
 
 
+def pinned_alloc(torch):
+    """Host output arrays in page-locked memory (device-to-host at full speed)."""
+    keep = []
+
+    def mk(shape, dtype=np.float64):
+        t = torch.empty(shape, dtype=torch.from_numpy(np.zeros(0, dtype=dtype)).dtype, pin_memory=True)
+        t.zero_()
+        keep.append(t)
+        return t.numpy()
+    return mk, keep
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="h2o_like", choices=list(CONFIGS))
-    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--slots", type=int, default=0)
+    ap.add_argument("--groups", type=int, default=0)
+    ap.add_argument("--graphs", type=int, default=-1, help="replay chunks from CUDA graphs (default: per config)")
+    ap.add_argument("--autotune", type=int, default=0,
+                    help="time the inverse's blockings for the workload's orders before the run")
     ap.add_argument("--cpu-budget", type=float, default=20.0,
                     help="seconds of oracle work per CPU sample (the reference arm takes one per step)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -189,8 +211,11 @@ def main():
     cfg = CONFIGS[a.config]
     from scatt_b200 import synth
     ks = cfg["ks"]()
-    B = a.batch or cfg["batch"]
-    workload = {"workload": a.config, **cfg["kw"], "energies": int(len(ks)), "batch_per_step": B,
+    slots = a.slots or cfg["slots"]
+    groups = a.groups or cfg["groups"]
+    graphs = cfg["graphs"] if a.graphs < 0 else a.graphs
+    workload = {"workload": a.config, **cfg["kw"], "energies": int(len(ks)), "slots": slots, "groups": groups,
+                "energies_per_step": slots // groups,
                 "seed": synth.SEED_BASE + (1 if a.config == "h2o_like" else 0)}
 
     if a.impl == "reference":
@@ -228,63 +253,83 @@ def main():
     # this rank's contiguous block of the k grid (cost-balanced; one l_cont here)
     from scatt_b200 import shard
     blocks = shard.partition(shard.energy_cost(np.full(len(ks), cfg["kw"]["l_cont"]), sol.Nf), ws)
-    mine = ks[blocks[rank]]
-    Es_all = 0.5 * mine ** 2
+    Es_all = 0.5 * ks[blocks[rank]] ** 2
+    if slots > len(Es_all):
+        raise SystemExit(f"--slots {slots} exceeds this rank's {len(Es_all)} energies")
+    gsize = slots // groups
+    cursor = [0]
 
-    def batch_of(step):
-        idx = [(step * B + i) % len(Es_all) for i in range(B)]
+    def next_energies(n):
+        idx = [(cursor[0] + i) % len(Es_all) for i in range(n)]
+        cursor[0] += n
         return Es_all[idx]
 
-    opts = S.default_opts(allow_closed_channels=1, max_batch=B, timing=1)
+    tuned = []
+    if a.autotune:
+        Nt = sol.Np + sol.Nf
+        for n in sorted({Nt, sol.Np}):
+            tuned.append(_lib.autotune_inverse(n, slots, device=local))
     peak = cuda_dgemm_peak(torch) if rank == 0 else None
+    alloc, _keep = pinned_alloc(torch)
+    opts = S.default_opts(allow_closed_channels=1, timing=1, use_graphs=graphs)
+    scan = sol.scan(slots=slots, groups=groups, opts=opts, alloc=alloc)
+    assert (scan.slots, scan.groups) == (slots, groups)
+    scan.submit(next_energies(slots))
     for w in range(a.warmup):
-        sol.solve(batch_of(w), opts=opts)
+        scan.submit(next_energies(gsize))
+        scan.step(results=False)
     torch.cuda.synchronize()
     if ws > 1:
         dist.barrier()
+    st0 = sol.last_stats()
     clocks = ClockSampler(local)
     clocks.start()
-    dev_s = 0.0
-    rinv_s = 0.0
-    rinv_calls = 0
-    launches = 0
+    n_done = 0
+    out_bytes = 0
     t_host = time.time()
     for k in range(a.steps):
-        sol.solve(batch_of(a.warmup + k), opts=opts)
-        st = sol.last_stats()
-        dev_s += st["device_s"]
-        rinv_s += st["rinv_s"]
-        rinv_calls += st["rinv_calls"]
-        launches += st["launches"]
+        scan.submit(next_energies(gsize))               # energies from host memory
+        n_done += len(scan.step(results=False))         # outputs back in pinned host memory
+        out_bytes += scan.last_out_bytes
     torch.cuda.synchronize()
     host_s = time.time() - t_host
     ck = clocks.stop()
+    st1 = sol.last_stats()
+    dev_s = st1["device_s"] - st0["device_s"]
+    rinv_s = st1["rinv_s"] - st0["rinv_s"]
+    rinv_flops = st1["rinv_flops"] - st0["rinv_flops"]
+    launches = st1["launches"] - st0["launches"]
     if ws > 1:
         dist.barrier()
         t = torch.tensor([dev_s, host_s], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dev_s, host_s = float(t[0]), float(t[1])
-    n_done = a.steps * B * ws
+        c = torch.tensor([n_done], dtype=torch.float64, device="cuda")
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        n_total = int(c[0])
+    else:
+        n_total = n_done
+    scan.close()
     if rank == 0:
         Nt = sol.Np + sol.Nf
-        flops_per_inv = 2.0 * Nt ** 3
-        achieved = (flops_per_inv * B) / (rinv_s / rinv_calls) / 1e12 if rinv_calls else None
-        out_bytes = B * 8 * (4 * sol.Np * sol.Np + sol.n_occ * sol.Np + 5 * 6 * sol.Np + 6 * sol.n_occ + 6
-                             + 2 * sol.Np + 16) + 4 * B
+        achieved = rinv_flops / rinv_s / 1e12 if rinv_s > 0 else None
         line = {
-            "metric": "FP64 scan energies/sec", "value": n_done / dev_s, "unit": "energies/s",
+            "metric": "FP64 scan energies/sec", "value": n_total / dev_s, "unit": "energies/s",
             "n_gpus": ws, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dev_s / a.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded H2O-like inputs of the benchmark shapes)",
-            "config": {**workload, "parallelism": f"energy-sharded x{ws}",
-                       "l2": "inputs larger than L2 (per-energy state > 126 MB)"},
-            "e2e": {"value": n_done / host_s, "unit": "energies/s", "h2d_bytes_per_step": 8 * B + 4 * B,
-                    "d2h_bytes_per_step": out_bytes},
+            "data": "synthetic (seeded H2O-like inputs of the benchmark shapes)"
+                    if a.config == "h2o_like" else "synthetic (seeded H2-like inputs of the benchmark shapes)",
+            "config": {**workload, "parallelism": f"energy-sharded x{ws}", "cuda_graphs": bool(graphs),
+                       "autotuned_inverses": tuned,
+                       "l2": "inputs larger than L2 (per-slot state of the scan > 126 MB)"},
+            "e2e": {"value": n_total / host_s, "unit": "energies/s", "h2d_bytes_per_step": 8 * gsize,
+                    "d2h_bytes_per_step": int(out_bytes / max(a.steps, 1))},
             "gpu_launches": int(launches),
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": (achieved / peak) if (achieved and peak) else None,
-                         "traffic": INVERSE_TRAFFIC.get((Nt, B)),
-                         "kernel": f"batched R^-1 (Gauss-Jordan, N_t={Nt}, batch {B}); "
+                         "traffic": INVERSE_TRAFFIC.get((a.config, slots, groups)),
+                         "kernel": f"batched R^-1 (Gauss-Jordan, N_t={Nt} in the exchange region, "
+                                   f"{sol.Np} outside; {slots} matrices a call); "
                                    "peak = cuBLAS DGEMM 8192^3 measured in this run (FP64 of measured)"},
             "clocks": ck,
             "setup_s": setup_s,

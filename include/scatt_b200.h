@@ -68,16 +68,20 @@ int scatt_inverse_batched(int n, int count, const double* A, double* out,
  * latency-bound caller that cannot accept the device-wide synchronisation of
  * cudaMalloc / cudaFree.  Every device buffer (matrix copies, ping-pong
  * buffers, pivot maps, panel windows, status words, entry table) is carved
- * from one static 64 MiB device array per device, held until exit by every
- * GPU that loads the library.
+ * from one static 64 MiB device array.  The array is reserved on a device
+ * when the library's module holding it loads there -- at the first use of
+ * this entry point under CUDA's default lazy module loading, at context
+ * creation under CUDA_MODULE_LOADING=EAGER -- and is held until the process
+ * exits.
  * Limits: n <= 1280, count <= 256, and
  * 8 count (3 n^2 + 128 n) + 4 count (4 n + 2) + 80 count bytes (each of
  * the nine pieces rounded up to 256) <= 64 MiB; larger requests return SCATT_ERR_SIZE before
  * any device work.  The first call on a device resolves the array's address
- * (cudaGetSymbolAddress) and should come before any stream capture.  Calls
- * that overlap in time on one device (several host threads) share the
- * array and race.  No counterpart in the reference (LapackInverse.hpp
- * allocates its workspace per call). */
+ * (cudaGetSymbolAddress) and creates the non-blocking stream the calls run
+ * on; it should come before any stream capture.  Calls do not synchronise
+ * with the caller's other streams, but return only after their host copies.
+ * Calls that overlap in time on one device (several host threads) share the
+ * array and race.  No counterpart in the reference. */
 int scatt_inverse_batched_noalloc(int n, int count, const double* A, double* out,
                                   int symmetrize, int* status);
 
@@ -175,8 +179,9 @@ typedef struct {
     int    allow_closed_channels; /* (0)     AsymptoticAmplitudes.hpp:72-102          */
     int    orthogonalize;         /* (1)     DipoleMatrixElement.hpp:104-148          */
     int    max_batch;             /* energies per device batch; 0 = as many as fit    */
-    int    use_graphs;            /* reserved, ignored: the radial step is launched
-                                     directly; graph replay is not implemented    */
+    int    use_graphs;            /* 1: each chunk of 8 radial steps is replayed
+                                     from a CUDA graph captured once per pattern
+                                     of stages (same results, fewer launches)    */
     int    diagnostics;           /* 1: S-matrix unitarity and eigenphases            */
     int    timing;                /* 1: CUDA-event timing of the solve (scatt_last_stats) */
 } scatt_solve_opts;
@@ -237,12 +242,47 @@ int scatt_solve_batch(scatt_ctx* ctx, int n_energy, const double* energies, cons
                       const scatt_solve_opts* opts, const scatt_outputs* outputs);
 /* Default policies (the reference's). */
 void scatt_default_opts(scatt_solve_opts* opts);
-/* Timing of the last scatt_solve_batch with opts.timing = 1 (device clock,
- * CUDA events on the library stream): out[0] device seconds of the whole
- * solve, out[1] seconds spent in the sampled R^-1 inversions, out[2] number
- * of sampled inversions, out[3] kernel launches issued, out[4] radial-sweep
- * seconds, out[5] post-processing seconds. */
-int scatt_last_stats(scatt_ctx* ctx, double* out6);
+
+/* ------------------------------------------------------ streaming scan
+ * The energy loop of the reference's driver (src/main.cpp:847-877, one
+ * run_one_energy per ik) as a conveyor: energies are queued and solved in
+ * `slots` device slots split into `groups` phase groups.  Every energy of a
+ * group is at the same radial step; groups start staggered by 1/groups of
+ * the radial sweep, so once the conveyor is full one group finishes every
+ * 1/groups of a sweep and its slots take the next queued energies at once.
+ * groups = 1 is the lock-step batch that scatt_solve_batch runs.
+ * Each energy's results equal scatt_solve_batch's for it.  A scan holds its
+ * device memory (slots sized for l_cont_max) until scatt_scan_close. */
+typedef struct scatt_scan scatt_scan;
+/* slots <= 0: as many as fit in 85% of free device memory;
+ * 1 <= groups <= 64 (clamped to slots); l_cont_max < 0: the uploaded
+ * scan's.  The scan keeps *opts as given. */
+int scatt_scan_open(scatt_ctx* ctx, const scatt_solve_opts* opts, int slots, int groups,
+                    int l_cont_max, scatt_scan** out);
+/* Queues energies (Hartree; l_cont NULL: the scan's l_cont_max); their
+ * submission indices continue from the previous submissions. */
+int scatt_scan_submit(scatt_scan* scan, int n, const double* energies, const int* l_cont);
+/* Runs the conveyor until at least one group finishes, then that group's
+ * post stages.  The finished energies' results go to rows 0 .. *n_done - 1
+ * of `outputs` (laid out as for scatt_solve_batch, capacity >= slots rows)
+ * and their submission indices to index_out (may be NULL).  *n_done = 0
+ * when nothing is queued or in flight.  Returns SCATT_OK or the first
+ * failing energy's status (outputs->status has each one's). */
+int scatt_scan_step(scatt_scan* scan, const scatt_outputs* outputs, int capacity, int* n_done,
+                    long long* index_out);
+/* Energies waiting in the queue and in flight in slots. */
+int scatt_scan_pending(scatt_scan* scan, int* queued, int* in_flight);
+/* Slot and group counts the scan was opened with. */
+int scatt_scan_shape(scatt_scan* scan, int* slots, int* groups);
+int scatt_scan_close(scatt_scan* scan);
+/* Timing of the last scatt_solve_batch with opts.timing = 1, or of every
+ * scatt_scan_step since the last scatt_scan_open (device clock, CUDA events
+ * on the library stream): out[0] device seconds, out[1] seconds spent in the
+ * sampled R^-1 inversions, out[2] number of sampled inversions, out[3] kernel
+ * launches issued, out[4] radial-sweep seconds, out[5] post-processing
+ * seconds, out[6] floating-point operations of the sampled inversions
+ * (2 n^3 per matrix of order n). */
+int scatt_last_stats(scatt_ctx* ctx, double* out7);
 
 #ifdef __cplusplus
 }

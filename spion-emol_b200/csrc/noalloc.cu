@@ -5,10 +5,16 @@
 // memory, and latency-bound callers that cannot take the device-wide
 // synchronisation of cudaMalloc / cudaFree.
 //
-// The scratch array is a module-level __device__ object.  This file is its
-// own CUDA module, so the array is only reserved on a device once this entry
-// point is first used there.  Its device address is taken once per device
-// with cudaGetSymbolAddress, with that device current.
+// The scratch array is a module-level __device__ object of this file's CUDA
+// module.  It is reserved on a device when that module is loaded there: at
+// the first use of this entry point under CUDA's default lazy module loading,
+// at context creation under CUDA_MODULE_LOADING=EAGER; either way it is held
+// until the process exits.  Its device address is taken once per device with
+// cudaGetSymbolAddress, with that device current.  The work runs on a
+// non-blocking stream created once per device, so a call does not
+// synchronise with the caller's work on other streams; its host copies are
+// from and to the caller's (pageable) buffers, so the call returns only when
+// they are done.
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -29,6 +35,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 
 std::mutex g_setup_mutex;
 void* g_scratch_addr[NOALLOC_MAX_DEVICES] = {};
+cudaStream_t g_stream[NOALLOC_MAX_DEVICES] = {};
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
@@ -73,8 +80,8 @@ __global__ void k_noalloc_entries(unsigned char* base, Carve c, int n, int count
                      st + 2 * b, n, n, n, P + (size_t)2 * n * 64 * b, sigt + (size_t)2 * n * b};
 }
 
-// Scratch address on the current device; resolved once per device.
-int scratch_address(unsigned char** out) {
+// Scratch address and stream of the current device; set up once per device.
+int scratch_address(unsigned char** out, cudaStream_t* stream) {
     int dev = -1;
     SCATT_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
@@ -94,7 +101,18 @@ int scratch_address(unsigned char** out) {
         }
         g_scratch_addr[dev] = p;
     }
+    if (!g_stream[dev]) {
+        cudaStream_t st = nullptr;
+        const cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();
+            set_last_error(std::string("scatt_inverse_batched_noalloc: cudaStreamCreate: ") + cudaGetErrorString(e));
+            return SCATT_ERR_CUDA;
+        }
+        g_stream[dev] = st;
+    }
     *out = static_cast<unsigned char*>(g_scratch_addr[dev]);
+    *stream = g_stream[dev];
     return SCATT_OK;
 }
 
@@ -125,9 +143,9 @@ int scatt_inverse_batched_noalloc(int n, int count, const double* A, double* out
     }
     SCATT_TRY(require_device());
     unsigned char* base = nullptr;
-    SCATT_TRY(scratch_address(&base));
+    cudaStream_t s = nullptr;
+    SCATT_TRY(scratch_address(&base, &s));
     const size_t nbytes = (size_t)n * n * count * sizeof(double);
-    cudaStream_t s = 0;
     // the status words (code, first failing column) must start at zero
     SCATT_CUDA_TRY(cudaMemsetAsync(base + c.st, 0, (size_t)2 * count * sizeof(int), s));
     SCATT_CUDA_TRY(cudaMemcpyAsync(base + c.A, A, nbytes, cudaMemcpyHostToDevice, s));

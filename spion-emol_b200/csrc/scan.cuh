@@ -28,6 +28,7 @@ struct ScanTables {
     int n_exp = 0;          // (2 l_max + 1)^2
     double alpha_pol = 0.0, r_c = 1.5;
     int pol_form = 0;
+    const double* dV = nullptr;   // optional caller device array added to V(n): [Nr][Np_max][Np_max]
     // potential: V_sigma(r_ir) [ir][sigma], Gaunt pair CSR
     DevBuf<double> vsig;
     int n_pairs = 0;
@@ -57,6 +58,7 @@ struct ScanTables {
 struct SolveStats {
     double device_s = 0.0, rinv_s = 0.0, sweep_s = 0.0, post_s = 0.0;
     double rinv_calls = 0.0;
+    double rinv_flops = 0.0;   // 2 n^3 summed over the matrices of the sampled inversions
     unsigned long long launches = 0;
 };
 

@@ -28,6 +28,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <deque>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -50,10 +52,46 @@ inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
 
 // ================================================================ step kernels
 
-// V(n): one thread per channel pair (mu' <= mu); Potentials.cpp:324-340.
-__global__ void k_build_V(BatchDev b, int n) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= b.n_pairs) return;
+// Radial step of slot d at position j of its group's current chunk, or -1
+// when the slot has none (empty slot, idle group, j past the chunk's end).
+__device__ __forceinline__ int step_of(const BatchDev& b, const EnergyDev& d, int j) {
+    if (!d.live) return -1;
+    const GroupDev& g = b.grp[d.grp];
+    return (g.n0 >= 0 && j < g.C) ? g.n0 + j : -1;
+}
+
+__device__ __forceinline__ size_t bslot(const BatchDev& b) { return (size_t)b.Np_max * (b.Nf > 0 ? b.Nf : 1); }
+__device__ __forceinline__ const double* V_of(const BatchDev& b, const EnergyDev& d, int j) {
+    return b.grp[d.grp].Vc + (size_t)j * b.Np_max * b.Np_max;
+}
+__device__ __forceinline__ const double* B_of(const BatchDev& b, const EnergyDev& d, int j) {
+    return b.grp[d.grp].Bc + (size_t)j * bslot(b);
+}
+__device__ __forceinline__ const double* Bs_of(const BatchDev& b, const EnergyDev& d, int j) {
+    return b.grp[d.grp].Bsc + (size_t)j * bslot(b);
+}
+__device__ __forceinline__ const double* Dinv_of(const BatchDev& b, const EnergyDev& d, int j) {
+    return b.grp[d.grp].Dinvc + (size_t)j * (b.Nf > 0 ? b.Nf : 1);
+}
+
+__device__ __forceinline__ double vpol_at(const BatchDev& b, double r) {
+    double vpol = 0.0;
+    if (b.alpha_pol != 0.0 && r >= 1.0e-6) {
+        if (b.pol_form == 0) {
+            const double u = r / b.r_c;
+            const double u6 = u * u * u * u * u * u;
+            const double damp = 1.0 - exp(-u6);
+            vpol = -0.5 * b.alpha_pol * (damp * damp) / (r * r * r * r);
+        } else {
+            const double s = r * r + b.r_c * b.r_c;
+            vpol = -b.alpha_pol / (2.0 * (s * s));
+        }
+    }
+    return vpol;
+}
+
+// V(n) pair p (row <= col of the upper triangle); Potentials.cpp:324-340.
+__device__ __forceinline__ void build_V_pair(const BatchDev& b, int p, int n, double* V) {
     const int row = b.pair_row[p], col = b.pair_col[p];
     const double r = n * b.dr;
     double v = 0.0;
@@ -61,31 +99,39 @@ __global__ void k_build_V(BatchDev b, int n) {
         const double* vs = b.vsig + (size_t)n * b.n_exp;
         for (int k = b.pair_ptr[p]; k < b.pair_ptr[p + 1]; ++k) v += b.pair_G[k] * vs[b.pair_sig[k]];
         if (row == col) {
-            double vpol = 0.0;
-            if (b.alpha_pol != 0.0 && r >= 1.0e-6) {
-                if (b.pol_form == 0) {
-                    const double u = r / b.r_c;
-                    const double u6 = u * u * u * u * u * u;
-                    const double damp = 1.0 - exp(-u6);
-                    vpol = -0.5 * b.alpha_pol * (damp * damp) / (r * r * r * r);
-                } else {
-                    const double s = r * r + b.r_c * b.r_c;
-                    vpol = -b.alpha_pol / (2.0 * (s * s));
-                }
-            }
             const int l = b.l_of_mu[row];
             const double inv_r2 = 1.0 / (r * r);
-            v = (v + vpol) + l * (l + 1.0) * 0.5 * inv_r2;
+            v = (v + vpol_at(b, r)) + l * (l + 1.0) * 0.5 * inv_r2;
         }
     }
-    b.V[row + (size_t)col * b.Np_max] = v;
-    b.V[col + (size_t)row * b.Np_max] = v;
+    if (b.dV) v += b.dV[(size_t)n * b.Np_max * b.Np_max + row + (size_t)col * b.Np_max];
+    V[row + (size_t)col * b.Np_max] = v;
+    V[col + (size_t)row * b.Np_max] = v;
 }
 
-// diagonal of V(n) only (for the analytic start of the recurrence)
-__global__ void k_vdiag(BatchDev b, int n, double* out) {
+// V of every group's chunk: grid (pairs, groups, SCHUR_CHUNK), one thread per
+// channel pair (mu' <= mu).
+__global__ void k_build_V(BatchDev b) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const GroupDev& g = b.grp[blockIdx.y];
+    const int j = blockIdx.z;
+    if (p >= b.n_pairs || g.n0 < 0 || j >= g.C) return;
+    build_V_pair(b, p, g.n0 + j, g.Vc + (size_t)j * b.Np_max * b.Np_max);
+}
+
+// V(n) into one given buffer (post stages).
+__global__ void k_build_V_at(BatchDev b, int n, double* V) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < b.n_pairs) build_V_pair(b, p, n, V);
+}
+
+// diagonal of V(n + 1) for the groups whose step n = n0 + j is inside the
+// analytic start of the recurrence: grid (channels, groups).
+__global__ void k_vdiag(BatchDev b, int j) {
     const int mu = blockIdx.x * blockDim.x + threadIdx.x;
-    if (mu >= b.Np_max) return;
+    const GroupDev& g = b.grp[blockIdx.y];
+    if (mu >= b.Np_max || g.n0 < 0 || j >= g.C || g.n0 + j >= b.n_start) return;
+    const int n = g.n0 + j + 1;
     // pair index of (mu, mu) in the row-major upper triangle
     const long p = (long)mu * b.Np_max - ((long)mu * (mu - 1)) / 2;
     const double r = n * b.dr;
@@ -93,23 +139,12 @@ __global__ void k_vdiag(BatchDev b, int n, double* out) {
     if (r > 1e-14) {
         const double* vs = b.vsig + (size_t)n * b.n_exp;
         for (int k = b.pair_ptr[p]; k < b.pair_ptr[p + 1]; ++k) v += b.pair_G[k] * vs[b.pair_sig[k]];
-        double vpol = 0.0;
-        if (b.alpha_pol != 0.0 && r >= 1.0e-6) {
-            if (b.pol_form == 0) {
-                const double u = r / b.r_c;
-                const double u6 = u * u * u * u * u * u;
-                const double damp = 1.0 - exp(-u6);
-                vpol = -0.5 * b.alpha_pol * (damp * damp) / (r * r * r * r);
-            } else {
-                const double s = r * r + b.r_c * b.r_c;
-                vpol = -b.alpha_pol / (2.0 * (s * s));
-            }
-        }
         const int l = b.l_of_mu[mu];
         const double inv_r2 = 1.0 / (r * r);
-        v = (v + vpol) + l * (l + 1.0) * 0.5 * inv_r2;
+        v = (v + vpol_at(b, r)) + l * (l + 1.0) * 0.5 * inv_r2;
     }
-    out[mu] = v;
+    if (b.dV) v += b.dV[(size_t)n * b.Np_max * b.Np_max + mu + (size_t)mu * b.Np_max];
+    g.vdiag1[mu] = v;
 }
 
 __device__ __forceinline__ double dinv_of(const BatchDev& b, int l, int n) {
@@ -122,11 +157,12 @@ __device__ __forceinline__ double dinv_of(const BatchDev& b, int l, int n) {
     return 1.0 / Df;
 }
 
-// B(n) = h^2/12 * (2 sqrt(2 pi) / r) * sum_lambda G chi, r = n dr (ExchangeCoupling.cpp:65-136)
-__global__ void k_build_B(BatchDev b, int n) {
-    const int row = blockIdx.x * blockDim.x + threadIdx.x;     // mu * n_sigma + sigma
+// B(n) = h^2/12 * (2 sqrt(2 pi) / r) * sum_lambda G chi, r = n dr, one
+// thread per row mu * n_sigma + sigma; Bs = B D^-1 (ExchangeCoupling.cpp:65-136).
+__device__ __forceinline__ void build_B_row(const BatchDev& b, int row, int n, double* B, double* Bs,
+                                            double* Dinv) {
     const int rows = b.Np_max * b.n_sigma;
-    if (row < b.Nf) b.Dinv[row] = dinv_of(b, b.l_sigma[row % b.n_sigma], n);
+    if (row < b.Nf) Dinv[row] = dinv_of(b, b.l_sigma[row % b.n_sigma], n);
     if (row >= rows) return;
     const int mu = row / b.n_sigma, sigma = row % b.n_sigma;
     const double r = n * b.dr;
@@ -146,67 +182,124 @@ __global__ void k_build_B(BatchDev b, int n) {
     for (int i = 0; i < no && i < 64; ++i) {
         const int f = i * b.n_sigma + sigma;
         const double Bv = on ? b.h2_12 * (factor * acc[i]) : 0.0;
-        b.B[mu + (size_t)f * b.Np_max] = Bv;
-        b.Bs[mu + (size_t)f * b.Np_max] = Bv * dinv_of(b, b.l_sigma[sigma], n);
+        B[mu + (size_t)f * b.Np_max] = Bv;
+        Bs[mu + (size_t)f * b.Np_max] = Bv * dinv_of(b, b.l_sigma[sigma], n);
     }
 }
 
-// Sinv of step n: the window store inside the asymptotic window, else the
-// chunk slot of step n.
-__device__ __forceinline__ double* sinv_at(const BatchDev& b, const EnergyDev& d, int n) {
+// B, Bs, D^-1 of every group's chunk: grid (rows, groups, SCHUR_CHUNK).
+__global__ void k_build_B(BatchDev b) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    const GroupDev& g = b.grp[blockIdx.y];
+    const int j = blockIdx.z;
+    if (g.n0 < 0 || j >= g.C) return;
+    const size_t sl = bslot(b);
+    build_B_row(b, row, g.n0 + j, g.Bc + j * sl, g.Bsc + j * sl, g.Dinvc + (size_t)j * (b.Nf > 0 ? b.Nf : 1));
+}
+
+// B(n), Bs(n), D^-1(n) into given buffers (post stages).
+__global__ void k_build_B_at(BatchDev b, int n, double* B, double* Bs, double* Dinv) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    build_B_row(b, row, n, B, Bs, Dinv);
+}
+
+__device__ __forceinline__ bool in_seg(const EnergyDev& d, int n) { return n >= d.seg_lo && n < d.seg_hi; }
+
+// Sinv of step n at chunk position j: the segment store, the asymptotic
+// window store, or the chunk slot j.
+__device__ __forceinline__ double* sinv_at(const BatchDev& b, const EnergyDev& d, int n, int j) {
     const size_t np2 = (size_t)d.Np * d.Np;
-    return n >= b.n_s ? d.tailS + (size_t)(n - b.n_s) * np2 : d.Sinv + (size_t)(n - b.cn0) * np2;
+    if (in_seg(d, n)) return d.segS + (size_t)(n - d.seg_lo) * np2;
+    return n >= b.n_s ? d.tailS + (size_t)(n - b.n_s) * np2 : d.Sinv + (size_t)j * np2;
+}
+
+// Rinv(n): the segment store, the asymptotic window store, or the ping-pong pair.
+__device__ __forceinline__ double* rinv_at(const BatchDev& b, const EnergyDev& d, int n) {
+    const size_t nt2 = (size_t)d.Nt * d.Nt;
+    if (in_seg(d, n)) return d.segR + (size_t)(n - d.seg_lo) * nt2;
+    return n >= b.n_s ? d.tailR + (size_t)(n - b.n_s) * nt2 : ((n & 1) ? d.Rinv1 : d.Rinv0);
+}
+
+// G(n-1)^T, accumulated into H(n)^T during step n (K x N_t, ld K).
+__device__ __forceinline__ double* gacc_at(const BatchDev& b, const EnergyDev& d, int n) {
+    if (in_seg(d, n)) return d.segH + (size_t)(n - d.seg_lo) * b.Krows * d.Nt;
+    return (n & 1) ? d.G1 : d.G0;
 }
 
 // Entries of one chunk's Schur GEMM and inverse, index j * count + e.
-__global__ void k_prepare_schur(BatchDev b, int C) {
+// Steps outside a slot's chunk get empty entries (M = 0, n = 0), which the
+// GEMM and inverse kernels skip; so do steps past n_transition for the GEMM.
+__global__ void k_prepare_schur(BatchDev b) {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= b.count * C) return;
+    if (idx >= b.count * SCHUR_CHUNK) return;
     const int j = idx / b.count, e = idx % b.count;
     EnergyDev& d = b.ed[e];
+    const int n = step_of(b, d, j);
     const int Np = d.Np, Nf = b.Nf;
-    const size_t np2 = (size_t)Np * Np, sl = (size_t)b.Np_max * Nf;
+    const size_t np2 = (size_t)Np * Np;
     double* S = d.S + j * np2;
+    const GemmEntry none{nullptr, nullptr, nullptr, 0, 0, 0, 1, 1, 1, 0.0, 1.0};
+    if (n < 0) {
+        b.gmS[idx] = none;
+        b.gjS[idx] = GjEntry{S, S, S, d.sigS, d.ridS, d.stS + 4 * j, 0, 1, 1, d.PS, d.sgS};
+        return;
+    }
+    const bool exch = n < b.n_tr && Nf > 0;
     // Bs B^T = B D^-1 B^T and A are symmetric: lower tiles only, mirrored
-    b.gmS[idx] = GemmEntry{b.Bsc + j * sl, b.Bc + j * sl, S, Np, Np, Nf, b.Np_max, b.Np_max, Np, -1.0, 1.0, 1};
-    b.gjS[idx] = GjEntry{S, d.Sw + j * np2, sinv_at(b, d, b.cn0 + j), d.sigS + (size_t)j * Np,
+    b.gmS[idx] = exch ? GemmEntry{Bs_of(b, d, j), B_of(b, d, j), S, Np, Np, Nf, b.Np_max, b.Np_max, Np, -1.0, 1.0, 1}
+                      : none;
+    b.gjS[idx] = GjEntry{S, d.Sw + j * np2, sinv_at(b, d, n, j), d.sigS + (size_t)j * Np,
                          d.ridS + (size_t)j * Np, d.stS + 4 * j, Np, Np, Np,
                          d.PS + (size_t)j * 4 * 64 * Np, d.sgS + (size_t)j * 4 * Np};
 }
 
-// Fills the per-step GEMM / GJ entry arrays (pointer bookkeeping only).
-__global__ void k_prepare(BatchDev b, int n) {
+// Fills the per-step GEMM / GJ entry arrays of chunk position j (pointer
+// bookkeeping only); entries a slot does not take this step are empty.
+__global__ void k_prepare(BatchDev b, int j) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= b.count) return;
     EnergyDev& d = b.ed[e];
+    const int n = step_of(b, d, j);
+    const GemmEntry none{nullptr, nullptr, nullptr, 0, 0, 0, 1, 1, 1, 0.0, 1.0};
+    if (n < 0) {
+        b.gmT[e] = b.gmF[e] = b.gmG1[e] = b.gmG2[e] = b.gmG3[e] = none;
+        b.gjR[e] = GjEntry{d.Ra, d.Rw, d.Ra, d.sigR, d.ridR, d.stR, 0, 1, 1, d.PR, d.sgR};
+        return;
+    }
     const int Np = d.Np, Nt = d.Nt, Nf = b.Nf, K = b.Krows;
-    const bool tail = n >= b.n_s;
-    double* sinv = sinv_at(b, d, n);
-    double* rinv = tail ? d.tailR + (size_t)(n - b.n_s) * Nt * Nt : ((n & 1) ? d.Rinv1 : d.Rinv0);
-    double* gcur = (n & 1) ? d.G1 : d.G0;
-    double* gnext = (n & 1) ? d.G0 : d.G1;
+    const bool exch = n < b.n_tr && Nf > 0;
+    const bool sweep = n <= b.N - 1;
+    double* sinv = sinv_at(b, d, n, j);
+    double* rinv = rinv_at(b, d, n);
+    double* gcur = gacc_at(b, d, n);
+    double* gnext = gacc_at(b, d, n + 1);
+    const double* Bs = Bs_of(b, d, j);
     const double* Cn = (n < b.n_pts) ? b.Ctab + (size_t)n * K * b.Np_max : nullptr;
-    b.gmT[e] = GemmEntry{sinv, b.Bs, d.T, Np, Nf, Np, Np, b.Np_max, Np, 1.0, 0.0};
+    b.gmT[e] = exch ? GemmEntry{sinv, Bs, d.T, Np, Nf, Np, Np, b.Np_max, Np, 1.0, 0.0} : none;
     // F = Bs^T Sinv Bs is symmetric: lower tiles only, mirrored
-    b.gmF[e] = GemmEntry{b.Bs, d.T, d.F, Nf, Nf, Np, b.Np_max, Np, Nf, 1.0, 0.0, 1};
-    b.gmG1[e] = GemmEntry{Cn, sinv, gcur, K, Np, Np, K, Np, K, 1.0, 1.0};
-    b.gmG2[e] = GemmEntry{Cn, d.T, gcur + (size_t)Np * K, K, Nf, Np, K, Np, K, -1.0, 1.0};
-    b.gmG3[e] = GemmEntry{gcur, rinv, gnext, K, Nt, Nt, K, Nt, K, 1.0, 0.0};
-    b.gjR[e] = GjEntry{d.Ra, d.Rw, rinv, d.sigR, d.ridR, d.stR, Nt, Nt, Nt, d.PR, d.sgR};
+    b.gmF[e] = exch ? GemmEntry{Bs, d.T, d.F, Nf, Nf, Np, b.Np_max, Np, Nf, 1.0, 0.0, 1} : none;
+    b.gmG1[e] = (sweep && Cn) ? GemmEntry{Cn, sinv, gcur, K, Np, Np, K, Np, K, 1.0, 1.0} : none;
+    b.gmG2[e] = (sweep && Cn && exch) ? GemmEntry{Cn, d.T, gcur + (size_t)Np * K, K, Nf, Np, K, Np, K, -1.0, 1.0}
+                                      : none;
+    b.gmG3[e] = sweep ? GemmEntry{gcur, rinv, gnext, K, Nt, Nt, K, Nt, K, 1.0, 0.0} : none;
+    b.gjR[e] = GjEntry{d.Ra, d.Rw, rinv, d.sigR, d.ridR, d.stR, n >= b.n_start ? Nt : 0, Nt, Nt, d.PR, d.sgR};
 }
 
-// A = (1 + h^2 E / 6) I - h^2/6 V(n)  into Schur slot j (SchurInverter.cpp:253-261)
-__global__ void k_init_S(BatchDev b, int j) {
-    const int e = blockIdx.y;
+// A = (1 + h^2 E / 6) I - h^2/6 V(n) into Schur slot j (SchurInverter.cpp:253-261);
+// grid (x, slots, SCHUR_CHUNK).
+__global__ void k_init_S(BatchDev b) {
+    const int e = blockIdx.y, j = blockIdx.z;
     const EnergyDev& d = b.ed[e];
+    if (step_of(b, d, j) < 0) return;
     const int Np = d.Np;
     const long total = (long)Np * Np;
     double* S = d.S + (size_t)j * total;
+    const double* V = V_of(b, d, j);
     for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
          idx += (long)gridDim.x * blockDim.x) {
         const int i = (int)(idx % Np), jc = (int)(idx / Np);
         const double diag = (i == jc) ? d.c : 0.0;
-        S[idx] = diag - b.h2_6 * b.V[i + (size_t)jc * b.Np_max];
+        S[idx] = diag - b.h2_6 * V[i + (size_t)jc * b.Np_max];
     }
 }
 
@@ -228,12 +321,15 @@ __device__ double block_min(double v, double* red) {
 // Johnson stability shift (SchurInverter.cpp:30-59): Gershgorin lower bound
 // first; when inconclusive the exact smallest eigenvalue c + lambda_min(M),
 // with lambda_min(M) precomputed per n (the matrix differs from M only by
-// c I).  which = 0: A (also records delta_A), 1: S = A_shifted - Bs B^T.
-__global__ void k_stab(BatchDev b, int n, int which) {
-    const int e = blockIdx.x;
+// c I).  which = 0: A (also records delta_A), 1: S = A_shifted - Bs B^T
+// (exchange steps only).  Grid (slots, SCHUR_CHUNK); steps n >= stab_n skip.
+__global__ void k_stab(BatchDev b, int which) {
+    const int e = blockIdx.x, slot = blockIdx.y;
     EnergyDev& d = b.ed[e];
+    const int n = step_of(b, d, slot);
+    if (n < 0 || n >= b.stab_n) return;
+    if (which == 1 && !(n < b.n_tr && b.Nf > 0)) return;
     const int Np = d.Np;
-    const int slot = n - b.cn0;
     double* S = d.S + (size_t)slot * Np * Np;
     __shared__ double red[33];
     double g = INFINITY;
@@ -254,6 +350,7 @@ __global__ void k_stab(BatchDev b, int n, int which) {
             if (which == 0) d.shiftsA += 1; else d.shiftsS += 1;
         }
         if (which == 0) d.deltaAc[slot] = delta;
+        if (d.stabd) d.stabd[2 * n + which] = delta;
         red[0] = delta;
     }
     __syncthreads();
@@ -262,64 +359,67 @@ __global__ void k_stab(BatchDev b, int n, int which) {
         for (int i = threadIdx.x; i < Np; i += blockDim.x) S[i + (size_t)i * Np] += delta;
 }
 
-// R = 12 W^-1 - 10 I - Rinv_prev, W^-1 = [[Sinv, -T], [-T^T, D^-1 + F]]
-__global__ void k_assemble_R(BatchDev b, int n) {
+// R = 12 W^-1 - 10 I - Rinv_prev, W^-1 = [[Sinv, -T], [-T^T, D^-1 + F]];
+// slots whose step is inside the analytic start skip.
+__global__ void k_assemble_R(BatchDev b, int j) {
     const int e = blockIdx.y;
     const EnergyDev& d = b.ed[e];
+    const int n = step_of(b, d, j);
+    if (n < b.n_start) return;                 // also n < 0
     const int Np = d.Np, Nt = d.Nt, Nf = b.Nf;
     const bool exch = n < b.n_tr;
-    const bool tail = n >= b.n_s;
-    const double* sinv = sinv_at(b, d, n);
-    const int pm = n - 1;
-    const double* prev = (pm >= b.n_s) ? d.tailR + (size_t)(pm - b.n_s) * Nt * Nt
-                                       : ((pm & 1) ? d.Rinv1 : d.Rinv0);
+    const double* sinv = sinv_at(b, d, n, j);
+    const double* Dinv = Dinv_of(b, d, j);
+    const double* prev = rinv_at(b, d, n - 1);
     const long total = (long)Nt * Nt;
     for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
          idx += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(idx % Nt), j = (int)(idx / Nt);
+        const int i = (int)(idx % Nt), jc = (int)(idx / Nt);
         double w;
-        if (i < Np && j < Np) w = sinv[i + (size_t)j * Np];
-        else if (i < Np) w = exch ? -d.T[i + (size_t)(j - Np) * Np] : 0.0;
-        else if (j < Np) w = exch ? -d.T[j + (size_t)(i - Np) * Np] : 0.0;
+        if (i < Np && jc < Np) w = sinv[i + (size_t)jc * Np];
+        else if (i < Np) w = exch ? -d.T[i + (size_t)(jc - Np) * Np] : 0.0;
+        else if (jc < Np) w = exch ? -d.T[jc + (size_t)(i - Np) * Np] : 0.0;
         else {
-            const int fi = i - Np, fj = j - Np;
-            w = (fi == fj) ? b.Dinv[fi] : 0.0;
+            const int fi = i - Np, fj = jc - Np;
+            w = (fi == fj) ? Dinv[fi] : 0.0;
             if (exch) w += d.F[fi + (size_t)fj * Nf];
         }
-        const double u = 12.0 * w - ((i == j) ? 10.0 : 0.0);
+        const double u = 12.0 * w - ((i == jc) ? 10.0 : 0.0);
         d.Ra[idx] = u - prev[idx];
     }
 }
 
 // Analytic diagonal Rinv for 1 <= n < n_start, 0 at n = 0
 // (ForwardRPropagator.cpp:78-134): zero fill, then k_analytic_R_diag.
-__global__ void k_analytic_R(BatchDev b, int n) {
+__global__ void k_analytic_R(BatchDev b, int j) {
     const int e = blockIdx.y;
     const EnergyDev& d = b.ed[e];
-    const int Nt = d.Nt;
-    const bool tail = n >= b.n_s;
-    double* out = tail ? d.tailR + (size_t)(n - b.n_s) * Nt * Nt : ((n & 1) ? d.Rinv1 : d.Rinv0);
-    const long total = (long)Nt * Nt;
+    const int n = step_of(b, d, j);
+    if (n < 0 || n >= b.n_start) return;
+    double* out = rinv_at(b, d, n);
+    const long total = (long)d.Nt * d.Nt;
     for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
          idx += (long)gridDim.x * blockDim.x)
         out[idx] = 0.0;
 }
 
-__global__ void k_analytic_R_diag(BatchDev b, int n) {
+__global__ void k_analytic_R_diag(BatchDev b, int j) {
     const int e = blockIdx.y;
     const EnergyDev& d = b.ed[e];
+    const int n = step_of(b, d, j);
+    if (n <= 0 || n >= b.n_start) return;
     const int Np = d.Np, Nt = d.Nt;
-    if (n <= 0) return;
-    const bool tail = n >= b.n_s;
-    double* out = tail ? d.tailR + (size_t)(n - b.n_s) * Nt * Nt : ((n & 1) ? d.Rinv1 : d.Rinv0);
+    double* out = rinv_at(b, d, n);
+    const double* V = V_of(b, d, j);
+    const double* vdiag1 = b.grp[d.grp].vdiag1;
     const double h = b.dr;
     const double rn = b.dr + n * h, rn1 = b.dr + (n + 1) * h;
     for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < Nt; m += gridDim.x * blockDim.x) {
         double val = 0.0;
         if (m < Np) {
             const int l = b.l_of_mu[m];
-            const double Mn = 1.0 + b.h2_6 * (d.E - b.V[m + (size_t)m * b.Np_max]);
-            const double Mn1 = 1.0 + b.h2_6 * (d.E - b.vdiag1[m]);
+            const double Mn = 1.0 + b.h2_6 * (d.E - V[m + (size_t)m * b.Np_max]);
+            const double Mn1 = 1.0 + b.h2_6 * (d.E - vdiag1[m]);
             const double yn = riccati_j(l, d.k * rn);
             const double yn1 = riccati_j(l, d.k * rn1);
             const double den = Mn1 * yn1;
@@ -342,16 +442,39 @@ __global__ void k_analytic_R_diag(BatchDev b, int n) {
     }
 }
 
-// sticky per-energy error: first failing inversion (step, code)
-__global__ void k_collect(BatchDev b, int n, int which) {
+// sticky per-slot error: first failing inversion (step, code); which = 0:
+// the Schur inverse of chunk position j, 1: the R^-1 of position j.
+__global__ void k_collect(BatchDev b, int j, int which) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= b.count) return;
     EnergyDev& d = b.ed[e];
-    const int st = which ? d.stR[0] : d.stS[4 * (n - b.cn0)];
+    const int n = step_of(b, d, j);
+    if (n < 0 || (which == 1 && n < b.n_start)) return;
+    const int st = which ? d.stR[0] : d.stS[4 * j];
     if (st != 0 && d.err_code == 0) {
         d.err_code = (st == DEV_SINGULAR) ? SCATT_ERR_SINGULAR : SCATT_ERR_NONFINITE;
         d.err_step = n;
     }
+}
+
+// End of a chunk: every running group moves on by its chunk's length; a
+// group whose chunk reached the stop step stops (n0 = -1).
+__global__ void k_advance(BatchDev b) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= b.ngroups) return;
+    GroupDev& G = b.grp[g];
+    if (G.n0 < 0) return;
+    const int n0 = G.n0 + G.C;
+    if (n0 >= b.n_stop) { G.n0 = -1; G.C = 0; return; }
+    G.n0 = n0;
+    G.C = min(SCHUR_CHUNK, b.n_stop - n0);
+}
+
+// Start (n0 >= 0) or stop (n0 = -1) one group between chunks.
+__global__ void k_set_group(BatchDev b, int g, int n0) {
+    GroupDev& G = b.grp[g];
+    G.n0 = n0;
+    G.C = n0 < 0 ? 0 : min(SCHUR_CHUNK, b.n_stop - n0);
 }
 
 
@@ -974,22 +1097,15 @@ int upload_static(Context& ctx, const scatt_scan_desc& D) {
     return SCATT_OK;
 }
 
-// ---------------------------------------------------------------- batch
-struct Batch {
-    BatchDev b{};
-    std::vector<EnergyDev> ed;
-    DevBuf<EnergyDev> d_ed;
-    DevBuf<double> arena;
-    DevBuf<int> iarena;
-    DevBuf<double> V, vdiag1, B, Bs, Dinv;
-    DevBuf<GemmEntry> gm;
-    DevBuf<GjEntry> gj;
-};
+namespace {
 
-int make_shared(const ScanTables& t, const scatt_solve_opts& o, Batch& bt) {
-    BatchDev& b = bt.b;
+// ---------------------------------------------------------------- scan constants
+// Grid rules shared by every energy of a scan (SolverParams, the fit window,
+// n_start), with the static tables' device pointers.
+int make_consts(const ScanTables& t, const scatt_solve_opts& o, BatchDev& b) {
     b.Nr = t.Nr;
     b.N = t.Nr - 1;
+    b.n_stop = t.Nr;
     b.n_tr = t.n_tr;
     const int n_keep_hi = std::min(t.Nr - 1, std::max(1, t.n_tr - 1));
     b.n_pts = std::min(t.Nr, n_keep_hi + 1);
@@ -1029,6 +1145,7 @@ int make_shared(const ScanTables& t, const scatt_solve_opts& o, Batch& bt) {
     b.alpha_pol = t.alpha_pol;
     b.r_c = t.r_c;
     b.pol_form = t.pol_form;
+    b.dV = t.dV;
     b.vsig = t.vsig.p;
     b.n_exp = t.n_exp;
     b.n_pairs = t.n_pairs;
@@ -1039,24 +1156,27 @@ int make_shared(const ScanTables& t, const scatt_solve_opts& o, Batch& bt) {
     b.Ctab = t.Ctab.p;
     b.l_of_mu = t.d_l_of_mu.p;
     b.l_sigma = t.d_l_sigma.p;
-    SCATT_TRY(bt.V.alloc((size_t)SCHUR_CHUNK * t.Np_max * t.Np_max));
-    SCATT_TRY(bt.vdiag1.alloc(t.Np_max));
-    SCATT_TRY(bt.B.alloc((size_t)SCHUR_CHUNK * t.Np_max * std::max(1, t.Nf)));
-    SCATT_TRY(bt.Bs.alloc((size_t)SCHUR_CHUNK * t.Np_max * std::max(1, t.Nf)));
-    SCATT_TRY(bt.Dinv.alloc((size_t)SCHUR_CHUNK * std::max(1, t.Nf)));
-    b.Vc = bt.V.p; b.Bc = bt.B.p; b.Bsc = bt.Bs.p; b.Dinvc = bt.Dinv.p;
-    b.V = bt.V.p; b.vdiag1 = bt.vdiag1.p; b.B = bt.B.p; b.Bs = bt.Bs.p; b.Dinv = bt.Dinv.p;
-    b.cn0 = 0;
     return SCATT_OK;
 }
 
-void launch_VB(const BatchDev& b, int n, cudaStream_t s) {
-    k_build_V<<<cdiv(b.n_pairs, TPB), TPB, 0, s>>>(b, n);
-    SCATT_COUNT_LAUNCH(1);
-    const int rows = std::max(b.Np_max * b.n_sigma, b.Nf);
-    k_build_B<<<cdiv(rows, 128), 128, 0, s>>>(b, n);
-    SCATT_COUNT_LAUNCH(1);
-}
+// V(n), B(n), Bs(n), D^-1(n) into one set of buffers (post stages, setup).
+struct VBAt {
+    DevBuf<double> V, B, Bs, Dinv;
+    int alloc(const BatchDev& b) {
+        SCATT_TRY(V.alloc((size_t)b.Np_max * b.Np_max));
+        SCATT_TRY(B.alloc((size_t)b.Np_max * std::max(1, b.Nf)));
+        SCATT_TRY(Bs.alloc((size_t)b.Np_max * std::max(1, b.Nf)));
+        SCATT_TRY(Dinv.alloc(std::max(1, b.Nf)));
+        return SCATT_OK;
+    }
+    void build(const BatchDev& b, int n, cudaStream_t s) {
+        k_build_V_at<<<cdiv(b.n_pairs, TPB), TPB, 0, s>>>(b, n, V.p);
+        SCATT_COUNT_LAUNCH(1);
+        const int rows = std::max(b.Np_max * b.n_sigma, b.Nf);
+        k_build_B_at<<<cdiv(rows, 128), 128, 0, s>>>(b, n, B.p, Bs.p, Dinv.p);
+        SCATT_COUNT_LAUNCH(1);
+    }
+};
 
 // lambda_min(-h^2/6 V(n)) and lambda_min(-h^2/6 V(n) - Bs B^T) for n < stab_n (per Np)
 int ensure_stab(Context& ctx, const scatt_solve_opts& o, int l_cont, const double** lmA, const double** lmS,
@@ -1073,12 +1193,14 @@ int ensure_stab(Context& ctx, const scatt_solve_opts& o, int l_cont, const doubl
             *lmS = keep.back().p;
             return SCATT_OK;
         }
-    Batch bt;
-    SCATT_TRY(make_shared(t, o, bt));
+    BatchDev b{};
+    SCATT_TRY(make_consts(t, o, b));
     const int Np = (l_cont + 1) * (l_cont + 1);
     const int ns = std::min(o.stab_n_max, t.Nr);
     std::vector<double> lA(std::max(ns, 1), 0.0), lS(std::max(ns, 1), 0.0);
     if (ns > 0) {
+        VBAt vb;
+        SCATT_TRY(vb.alloc(b));
         DevBuf<double> MA, MS, d, e, wk, outA, outS;
         SCATT_TRY(MA.alloc((size_t)ns * Np * Np));
         SCATT_TRY(MS.alloc((size_t)ns * Np * Np));
@@ -1089,13 +1211,13 @@ int ensure_stab(Context& ctx, const scatt_solve_opts& o, int l_cont, const doubl
         SCATT_TRY(outS.alloc(ns));
         Launcher L{s};
         for (int n = 0; n < ns; ++n) {
-            launch_VB(bt.b, n, s);
-            k_neg_hV<<<64, TPB, 0, s>>>(bt.b.V, t.Np_max, bt.b.h2_6, MA.p + (size_t)n * Np * Np, Np);
+            vb.build(b, n, s);
+            k_neg_hV<<<64, TPB, 0, s>>>(vb.V.p, t.Np_max, b.h2_6, MA.p + (size_t)n * Np * Np, Np);
             SCATT_COUNT_LAUNCH(1);
             SCATT_CUDA_TRY(cudaMemcpyAsync(MS.p + (size_t)n * Np * Np, MA.p + (size_t)n * Np * Np,
                                            (size_t)Np * Np * sizeof(double), cudaMemcpyDeviceToDevice, s));
             if (n < t.n_tr && t.Nf > 0) {
-                std::vector<GemmEntry> g{GemmEntry{bt.b.Bs, bt.b.B, MS.p + (size_t)n * Np * Np, Np, Np, t.Nf,
+                std::vector<GemmEntry> g{GemmEntry{vb.Bs.p, vb.B.p, MS.p + (size_t)n * Np * Np, Np, Np, t.Nf,
                                                    t.Np_max, t.Np_max, Np, -1.0, 1.0}};
                 SCATT_TRY(L.gemm(g, 0, 1));
             }
@@ -1124,277 +1246,502 @@ int ensure_stab(Context& ctx, const scatt_solve_opts& o, int l_cont, const doubl
     return SCATT_OK;
 }
 
-size_t energy_bytes(const BatchDev& b, int Np, int Nt, int nslots) {
+// Device doubles of one slot sized for (Np, Nt): the chunk's Schur slots,
+// the W^-1 blocks, the R ping-pong buffers, the dipole rows, the asymptotic
+// window store and the inverse's panel windows (every piece 256-byte aligned).
+size_t slot_doubles(const BatchDev& b, int Np, int Nt) {
+    const int nslots = b.N - b.n_s + 1;
+    auto al = [](size_t c) { return (c + 31) & ~size_t(31); };
     const size_t np2 = (size_t)Np * Np, nt2 = (size_t)Nt * Nt;
-    size_t d = 3 * SCHUR_CHUNK * np2 + (size_t)Np * b.Nf + (size_t)b.Nf * b.Nf + 4 * nt2 +
-               2 * (size_t)b.Krows * Nt;
-    d += (size_t)nslots * (nt2 + 2 * np2);
-    d += 4 * (size_t)64 * (SCHUR_CHUNK * (size_t)Np + Nt);   // two-level panel windows (two sets)
-    d += 16 * 32;                                    // every buffer starts on a 256-byte boundary
-    return d * sizeof(double);
+    return 3 * al(SCHUR_CHUNK * np2) + al((size_t)Np * b.Nf) + al((size_t)b.Nf * b.Nf) + 4 * al(nt2) +
+           2 * al((size_t)b.Krows * Nt) + al((size_t)nslots * nt2) + 2 * al((size_t)nslots * np2) +
+           al((size_t)SCHUR_CHUNK * 4 * 64 * Np) + al((size_t)4 * 64 * Nt);
 }
-
-
-namespace {
-
-struct Post {        // per-energy post-processing buffers
+size_t slot_ints(int Np, int Nt) { return SCHUR_CHUNK * (6 * (size_t)Np + 4) + 6 * (size_t)Nt + 4; }
+// Device doubles of one group's chunk arrays (V, B, Bs, D^-1 of SCHUR_CHUNK steps, V(n+1) diagonal).
+size_t group_doubles(const BatchDev& b) {
+    auto al = [](size_t c) { return (c + 31) & ~size_t(31); };
+    const size_t sl = (size_t)b.Np_max * std::max(1, b.Nf);
+    return al(SCHUR_CHUNK * (size_t)b.Np_max * b.Np_max) + 2 * al(SCHUR_CHUNK * sl) +
+           al(SCHUR_CHUNK * (size_t)std::max(1, b.Nf)) + al(b.Np_max);
+}
+// Device doubles of one energy's post-stage buffers.
+size_t post_doubles(const BatchDev& b, int Np, int Nt, int l_cont, int nfit, int n_occ) {
+    const size_t np2 = (size_t)Np * Np;
+    return 6 * Np + 14 * np2 + (size_t)b.Nf * Np + 2 * (size_t)Nt * Np + 12 * np2 +
+           2 * (size_t)(l_cont + 1) * nfit + 8 * (size_t)(l_cont + 1) + 2 * np2 + (size_t)b.Krows * Np +
+           24 * (size_t)Np + 2 * (size_t)n_occ * Np + 8 * (size_t)Np + 2 * np2 + 64;
+}
+// ---------------------------------------------------------------- scan
+struct PostBufs {        // per-energy post-processing buffers
     double *tab, *Amat, *Bmat, *Bw, *Binv, *Kraw, *K, *psibc, *VP, *Bf, *fN, *Z0, *Z1, *rhs;
-    double *Q, *Qw, *Qinv, *aatab, *aaM, *aared, *Aaa, *Baa, *Aw, *Ainv, *Kaa, *dall;
-    double *Dre, *Dim, *Drre, *Drim, *ore, *oim, *ew_d, *ew_e, *ew_w, *eigK, *eigA, *Kc;
+    double *Q, *Qw, *Qinv, *aatab, *aaM, *aared, *Aaa, *Baa, *Aw, *Ainv, *Kc, *dall;
+    double *Dre, *Dim, *Drre, *Drim, *ore, *oim, *ew_d, *ew_e, *ew_w, *eigK, *eigA;
     int *sig, *rid, *st;
 };
 
-int gemm_dev(Batch& bt, GemmEntry* ents, int count, const std::vector<EnergyDev>& ed, int which,
-             int opA, int opB, cudaStream_t s) {
-    int mM = 0, mN = 0;
-    for (auto& d : ed) {
-        const int Np = d.Np, Nt = d.Nt, Nf = bt.b.Nf, K = bt.b.Krows;
-        int M = 0, N = 0;
-        switch (which) {
-            case 0: M = Np; N = Np; break;       // S
-            case 1: M = Np; N = Nf; break;       // T
-            case 2: M = Nf; N = Nf; break;       // F
-            case 3: M = K; N = Np; break;        // G1
-            case 4: M = K; N = Nf; break;        // G2
-            case 5: M = K; N = Nt; break;        // G3
-        }
-        mM = std::max(mM, M);
-        mN = std::max(mN, N);
+struct Job {
+    double E;
+    int l_cont;
+    long index;       // submission index
+};
+
+// CUDA events created once per scan and destroyed with it, so no early
+// return leaks one.
+struct EventPool {
+    std::vector<cudaEvent_t> ev;
+    size_t used = 0;
+    ~EventPool() {
+        for (auto e : ev) cudaEventDestroy(e);
     }
-    return gemm_batched(ents, count, mM, mN, opA, opB, s);
+    int get(cudaEvent_t* out) {
+        if (used == ev.size()) {
+            cudaEvent_t e;
+            SCATT_CUDA_TRY(cudaEventCreate(&e));
+            ev.push_back(e);
+        }
+        *out = ev[used++];
+        return SCATT_OK;
+    }
+    void reset() { used = 0; }
+};
+
+}  // namespace
+
+// A scan: `slots` energies in flight in `ngroups` phase groups; energies
+// wait in a queue and enter a group whenever the group is free.
+struct Scan {
+    Context* ctx = nullptr;
+    scatt_solve_opts o{};
+    BatchDev b{};
+    int slots = 0, G = 1, gs = 1;
+    int l_cap = 0, Np_cap = 0, Nt_cap = 0;
+    int chunks_per_sweep = 0;
+    std::vector<EnergyDev> ed;          // host copy of the slot state (pointers fixed at open)
+    std::vector<GroupDev> grp;          // host mirror of the group state
+    std::vector<long> job_of;           // submission index held by each slot (-1 empty)
+    std::vector<long> start_chunk;      // first chunk at which each idle group may start
+    std::deque<Job> queue;
+    long chunk = 0;
+    long submitted = 0;
+    DevBuf<EnergyDev> d_ed;
+    DevBuf<GroupDev> d_grp;
+    DevBuf<double> arena, garena, parena;
+    DevBuf<int> iarena, pia;
+    DevBuf<GemmEntry> gm;
+    DevBuf<GjEntry> gj;
+    VBAt vb;                            // V/B at one step for the post stages
+    std::vector<PostBufs> P;            // gs energies
+    std::vector<DevBuf<double>> keep;   // stability spectra per l_cont
+    std::vector<std::pair<int, std::pair<const double*, const double*>>> stab_ptr;
+    EventPool events;
+    Launcher L{nullptr};
+    int nfit = 0, ne_fit = 0;
+    struct Graph {
+        cudaGraphExec_t exec;
+        unsigned long long launches;    // kernels per replay
+    };
+    std::map<std::pair<uint64_t, int>, Graph> graphs;   // (stage pattern, stop step) -> replay
+    Scan() = default;
+    Scan(const Scan&) = delete;
+    Scan& operator=(const Scan&) = delete;
+    ~Scan() {
+        for (auto& g : graphs) cudaGraphExecDestroy(g.second.exec);
+    }
+};
+
+namespace {
+
+int gemm_slots(Scan& sc, GemmEntry* ents, int count, int which, int opA, int opB) {
+    const int Np = sc.Np_cap, Nt = sc.Nt_cap, Nf = sc.b.Nf, K = sc.b.Krows;
+    int M = 0, N = 0;
+    switch (which) {
+        case 0: M = Np; N = Np; break;       // S
+        case 1: M = Np; N = Nf; break;       // T
+        case 2: M = Nf; N = Nf; break;       // F
+        case 3: M = K; N = Np; break;        // G1
+        case 4: M = K; N = Nf; break;        // G2
+        case 5: M = K; N = Nt; break;        // G3
+    }
+    return gemm_batched(ents, count, M, N, opA, opB, sc.ctx->stream);
 }
 
-int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* E, const int* lc,
-              const scatt_outputs* out, int offset) {
+int stab_for(Scan& sc, int l_cont, const double** lmA, const double** lmS) {
+    for (auto& p : sc.stab_ptr)
+        if (p.first == l_cont) {
+            *lmA = p.second.first;
+            *lmS = p.second.second;
+            return SCATT_OK;
+        }
+    SCATT_TRY(ensure_stab(*sc.ctx, sc.o, l_cont, lmA, lmS, sc.keep));
+    sc.stab_ptr.push_back({l_cont, {*lmA, *lmS}});
+    return SCATT_OK;
+}
+
+int scan_open(Context& ctx, const scatt_solve_opts& o, int slots, int ngroups, int l_cap, Scan& sc) {
     ScanTables& t = *ctx.tab;
     cudaStream_t s = ctx.stream;
-    Batch bt;
-    SCATT_TRY(make_shared(t, o, bt));
-    BatchDev& b = bt.b;
-    b.count = count;
-    const int N = b.N;
-    const int nslots = N - b.n_s + 1;
-    const int K = b.Krows, Nf = b.Nf;
-    std::vector<DevBuf<double>> keep;
-    // ---- per-energy sizes and arena
-    bt.ed.resize(count);
-    size_t total = 0;
-    std::vector<size_t> off(count);
-    for (int e = 0; e < count; ++e) {
-        EnergyDev& d = bt.ed[e];
-        std::memset(&d, 0, sizeof(d));
-        d.E = E[e];
-        d.c = 1.0 + b.h2_6 * E[e];
-        d.k = std::sqrt(2.0 * E[e]);
-        d.l_cont = lc ? lc[e] : t.l_max;
-        d.Np = (d.l_cont + 1) * (d.l_cont + 1);
-        d.Nt = d.Np + Nf;
-        off[e] = total;
-        total += (energy_bytes(b, d.Np, d.Nt, nslots) / sizeof(double) + 31) & ~size_t(31);
-        SCATT_TRY(ensure_stab(ctx, o, d.l_cont, &d.lmA, &d.lmS, keep));
+    if (slots < 1 || ngroups < 1 || ngroups > MAX_GROUPS || ngroups > slots || l_cap < 0 || l_cap > t.l_max) {
+        set_last_error("scatt_scan_open: need 1 <= groups <= min(slots, " + std::to_string(MAX_GROUPS) +
+                       ") and 0 <= l_cont_max <= the uploaded scan's");
+        return SCATT_ERR_ARG;
     }
-    SCATT_TRY(bt.arena.alloc(total));
-    size_t itot = 0;
-    for (auto& d : bt.ed) itot += SCHUR_CHUNK * (6 * (size_t)d.Np + 4) + 6 * (size_t)d.Nt + 4;
-    SCATT_TRY(bt.iarena.alloc(itot));
-    SCATT_CUDA_TRY(cudaMemsetAsync(bt.iarena.p, 0, itot * sizeof(int), s));
-    size_t ip = 0;
-    for (int e = 0; e < count; ++e) {
-        EnergyDev& d = bt.ed[e];
-        const size_t np2 = (size_t)d.Np * d.Np, nt2 = (size_t)d.Nt * d.Nt;
-        double* p = bt.arena.p + off[e];
+    sc.ctx = &ctx;
+    sc.o = o;
+    sc.L.s = s;
+    BatchDev& b = sc.b;
+    SCATT_TRY(make_consts(t, o, b));
+    sc.slots = slots;
+    sc.G = ngroups;
+    sc.gs = (slots + ngroups - 1) / ngroups;
+    sc.l_cap = l_cap;
+    sc.Np_cap = (l_cap + 1) * (l_cap + 1);
+    sc.Nt_cap = sc.Np_cap + b.Nf;
+    sc.chunks_per_sweep = (b.N + 1 + SCHUR_CHUNK - 1) / SCHUR_CHUNK;
+    sc.ne_fit = std::min(t.Nr - 1 - 3, b.N);
+    sc.nfit = sc.ne_fit - b.n_s + 1;
+    b.count = slots;
+    b.ngroups = ngroups;
+    const int K = b.Krows, Nf = b.Nf;
+    // ---- slot arena
+    const size_t per = slot_doubles(b, sc.Np_cap, sc.Nt_cap);
+    SCATT_TRY(sc.arena.alloc(per * slots));
+    SCATT_TRY(sc.iarena.alloc(slot_ints(sc.Np_cap, sc.Nt_cap) * slots));
+    SCATT_CUDA_TRY(cudaMemsetAsync(sc.iarena.p, 0, sc.iarena.n * sizeof(int), s));
+    sc.ed.assign(slots, EnergyDev{});
+    sc.job_of.assign(slots, -1);
+    for (int e = 0; e < slots; ++e) {
+        EnergyDev& d = sc.ed[e];
+        std::memset(&d, 0, sizeof(d));
+        const size_t np2 = (size_t)sc.Np_cap * sc.Np_cap, nt2 = (size_t)sc.Nt_cap * sc.Nt_cap;
+        const int nslots = b.N - b.n_s + 1;
+        double* p = sc.arena.p + per * e;
         // 256-byte aligned pieces (the inverse kernels copy 16-byte row pairs)
         auto take = [&p](size_t cnt) { double* r = p; p += (cnt + 31) & ~size_t(31); return r; };
         d.S = take(SCHUR_CHUNK * np2);
         d.Sw = take(SCHUR_CHUNK * np2);
         d.Sinv = take(SCHUR_CHUNK * np2);
-        d.T = take((size_t)d.Np * Nf);
+        d.T = take((size_t)sc.Np_cap * Nf);
         d.F = take((size_t)Nf * Nf);
         d.Ra = take(nt2);
         d.Rw = take(nt2);
         d.Rinv0 = take(nt2);
         d.Rinv1 = take(nt2);
-        d.G0 = take((size_t)K * d.Nt);
-        d.G1 = take((size_t)K * d.Nt);
+        d.G0 = take((size_t)K * sc.Nt_cap);
+        d.G1 = take((size_t)K * sc.Nt_cap);
         d.tailR = take((size_t)nslots * nt2);
         d.tailS = take((size_t)nslots * np2);
         d.psiT = take((size_t)nslots * np2);
-        d.PS = take((size_t)SCHUR_CHUNK * 4 * 64 * d.Np);
-        d.PR = take((size_t)4 * 64 * d.Nt);
-        int* q = bt.iarena.p + ip;
-        d.sigS = q; q += SCHUR_CHUNK * d.Np;
-        d.ridS = q; q += SCHUR_CHUNK * d.Np;
-        d.sigR = q; q += d.Nt;
-        d.ridR = q; q += d.Nt;
+        d.PS = take((size_t)SCHUR_CHUNK * 4 * 64 * sc.Np_cap);
+        d.PR = take((size_t)4 * 64 * sc.Nt_cap);
+        int* q = sc.iarena.p + slot_ints(sc.Np_cap, sc.Nt_cap) * e;
+        const int Np = sc.Np_cap, Nt = sc.Nt_cap;
+        d.sigS = q; q += SCHUR_CHUNK * Np;
+        d.ridS = q; q += SCHUR_CHUNK * Np;
+        d.sigR = q; q += Nt;
+        d.ridR = q; q += Nt;
         d.stS = q; q += SCHUR_CHUNK * 4;
         d.stR = q; q += 4;
-        d.sgS = q; q += SCHUR_CHUNK * 4 * d.Np;
-        d.sgR = q; q += 4 * d.Nt;
-        ip += SCHUR_CHUNK * (6 * (size_t)d.Np + 4) + 6 * (size_t)d.Nt + 4;
-        SCATT_CUDA_TRY(cudaMemsetAsync(d.G0, 0, (size_t)K * d.Nt * sizeof(double), s));
+        d.sgS = q; q += SCHUR_CHUNK * 4 * Np;
+        d.sgR = q; q += 4 * Nt;
+        d.grp = e / sc.gs;
+        d.live = 0;
     }
-    SCATT_TRY(upload_vec(bt.d_ed, bt.ed, s));
-    b.ed = bt.d_ed.p;
-    SCATT_TRY(bt.gm.alloc((5 + SCHUR_CHUNK) * (size_t)count));
-    SCATT_TRY(bt.gj.alloc((1 + SCHUR_CHUNK) * (size_t)count));
-    b.gmT = bt.gm.p; b.gmF = bt.gm.p + count;
-    b.gmG1 = bt.gm.p + 2 * count; b.gmG2 = bt.gm.p + 3 * count; b.gmG3 = bt.gm.p + 4 * count;
-    b.gmS = bt.gm.p + 5 * count;                  // SCHUR_CHUNK x count
-    b.gjR = bt.gj.p; b.gjS = bt.gj.p + count;     // gjS: SCHUR_CHUNK x count
-    int maxNp = 0, maxNt = 0;
-    for (auto& d : bt.ed) { maxNp = std::max(maxNp, d.Np); maxNt = std::max(maxNt, d.Nt); }
-
-    // ================================================================ radial sweep
-    const dim3 eg(64, count);
-    const unsigned long long launches0 = launch_counter();
-    cudaEvent_t ev_begin = nullptr, ev_sweep = nullptr, ev_end = nullptr;
-    std::vector<cudaEvent_t> rev;           // sampled R^-1 inversions: pairs
-    const int sample_every = 16;
-    if (o.timing) {
-        cudaEventCreate(&ev_begin);
-        cudaEventCreate(&ev_sweep);
-        cudaEventCreate(&ev_end);
-        cudaEventRecord(ev_begin, s);
-    }
-    // BatchDev with the per-step buffers pointing at chunk slot j
-    auto slot = [&](int n0, int j) {
-        BatchDev bj = b;
+    SCATT_TRY(upload_vec(sc.d_ed, sc.ed, s));
+    b.ed = sc.d_ed.p;
+    // ---- group chunk arrays
+    const size_t gper = group_doubles(b);
+    SCATT_TRY(sc.garena.alloc(gper * ngroups));
+    sc.grp.assign(ngroups, GroupDev{});
+    for (int g = 0; g < ngroups; ++g) {
+        GroupDev& G = sc.grp[g];
+        double* p = sc.garena.p + gper * g;
+        auto take = [&p](size_t cnt) { double* r = p; p += (cnt + 31) & ~size_t(31); return r; };
         const size_t sl = (size_t)b.Np_max * std::max(1, Nf);
-        bj.V = b.Vc + (size_t)j * b.Np_max * b.Np_max;
-        bj.B = b.Bc + (size_t)j * sl;
-        bj.Bs = b.Bsc + (size_t)j * sl;
-        bj.Dinv = b.Dinvc + (size_t)j * std::max(1, Nf);
-        bj.cn0 = n0;
-        return bj;
-    };
-    for (int n0 = 0; n0 <= N; n0 += SCHUR_CHUNK) {
-        const int C = std::min(SCHUR_CHUNK, N + 1 - n0);
-        // ---- Schur complements of the chunk's steps: A(n), S(n) = A - Bs B^T, one batched inverse
-        for (int j = 0; j < C; ++j) {
-            const int n = n0 + j;
-            const BatchDev bj = slot(n0, j);
-            launch_VB(bj, n, s);
-            k_init_S<<<eg, TPB, 0, s>>>(bj, j);
-            SCATT_COUNT_LAUNCH(1);
-            if (n < b.stab_n) { k_stab<<<count, TPB, 0, s>>>(bj, n, 0); SCATT_COUNT_LAUNCH(1); }
-        }
-        {
-            BatchDev bc = b;
-            bc.cn0 = n0;
-            k_prepare_schur<<<cdiv(count * C, 128), 128, 0, s>>>(bc, C);
-            SCATT_COUNT_LAUNCH(1);
-        }
-        // the exchange steps of a chunk are its leading ones (n < n_tr)
-        const int Cx = (Nf > 0) ? std::max(0, std::min(C, b.n_tr - n0)) : 0;
-        if (Cx > 0) SCATT_TRY(gemm_dev(bt, b.gmS, count * Cx, bt.ed, 0, 0, 1, s));
-        for (int j = 0; j < Cx; ++j)
-            if (n0 + j < b.stab_n) { k_stab<<<count, TPB, 0, s>>>(slot(n0, j), n0 + j, 1); SCATT_COUNT_LAUNCH(1); }
-        SCATT_TRY(gj_inverse_selected(b.gjS, count * C, maxNp, true, s, true));
-        // ---- the R-ratio recurrence over the chunk's steps
-        for (int j = 0; j < C; ++j) {
-            const int n = n0 + j;
-            const BatchDev bj = slot(n0, j);
-            k_prepare<<<cdiv(count, 128), 128, 0, s>>>(bj, n);
-            SCATT_COUNT_LAUNCH(1);
-            if (n < b.n_start) { k_vdiag<<<cdiv(b.Np_max, 128), 128, 0, s>>>(bj, n + 1, b.vdiag1); SCATT_COUNT_LAUNCH(1); }
-            k_collect<<<cdiv(count, 128), 128, 0, s>>>(bj, n, 0);
-            SCATT_COUNT_LAUNCH(1);
-            const bool exch = n < b.n_tr && Nf > 0;
-            if (exch) {
-                SCATT_TRY(gemm_dev(bt, b.gmT, count, bt.ed, 1, 0, 0, s));
-                SCATT_TRY(gemm_dev(bt, b.gmF, count, bt.ed, 2, 1, 0, s));
-            }
-            if (n < b.n_start) {
-                k_analytic_R<<<eg, TPB, 0, s>>>(bj, n);
-                SCATT_COUNT_LAUNCH(1);
-                k_analytic_R_diag<<<dim3(4, count), TPB, 0, s>>>(bj, n);
-                SCATT_COUNT_LAUNCH(1);
-            } else {
-                k_assemble_R<<<eg, TPB, 0, s>>>(bj, n);
-                SCATT_COUNT_LAUNCH(1);
-                const bool sample = o.timing && (n % sample_every == 0);
-                if (sample) {
-                    cudaEvent_t a0, a1;
-                    cudaEventCreate(&a0);
-                    cudaEventCreate(&a1);
-                    rev.push_back(a0);
-                    rev.push_back(a1);
-                    cudaEventRecord(a0, s);
-                }
-                SCATT_TRY(gj_inverse_selected(b.gjR, count, maxNt, true, s, true));
-                if (sample) cudaEventRecord(rev.back(), s);
-                k_collect<<<cdiv(count, 128), 128, 0, s>>>(bj, n, 1);
-                SCATT_COUNT_LAUNCH(1);
-            }
-            if (n <= N - 1) {
-                if (n < b.n_pts) SCATT_TRY(gemm_dev(bt, b.gmG1, count, bt.ed, 3, 0, 0, s));
-                if (n < b.n_pts && exch) SCATT_TRY(gemm_dev(bt, b.gmG2, count, bt.ed, 4, 0, 0, s));
-                SCATT_TRY(gemm_dev(bt, b.gmG3, count, bt.ed, 5, 0, 0, s));
-            }
-        }
+        G.n0 = -1;
+        G.C = 0;
+        G.Vc = take(SCHUR_CHUNK * (size_t)b.Np_max * b.Np_max);
+        G.Bc = take(SCHUR_CHUNK * sl);
+        G.Bsc = take(SCHUR_CHUNK * sl);
+        G.Dinvc = take(SCHUR_CHUNK * (size_t)std::max(1, Nf));
+        G.vdiag1 = take(b.Np_max);
     }
-    SCATT_CUDA_TRY(cudaGetLastError());
-    if (o.timing) cudaEventRecord(ev_sweep, s);
-    SCATT_CUDA_TRY(cudaStreamSynchronize(s));
-    // read back per-energy error/shift counters
-    std::vector<EnergyDev> edh(count);
-    SCATT_CUDA_TRY(cudaMemcpy(edh.data(), bt.d_ed.p, count * sizeof(EnergyDev), cudaMemcpyDeviceToHost));
-
-    // ================================================================ post stages
-    const int ne_fit = std::min(t.Nr - 1 - 3, N);
-    const int nfit = ne_fit - b.n_s + 1;
-    std::vector<Post> P(count);
-    DevBuf<double> parena;
-    DevBuf<int> pia;
+    SCATT_TRY(upload_vec(sc.d_grp, sc.grp, s));
+    b.grp = sc.d_grp.p;
+    // staggered starts: group g first starts g / G of a sweep after group 0
+    sc.start_chunk.assign(ngroups, 0);
+    for (int g = 0; g < ngroups; ++g) sc.start_chunk[g] = (long)g * sc.chunks_per_sweep / ngroups;
+    // ---- entry arrays
+    SCATT_TRY(sc.gm.alloc((5 + SCHUR_CHUNK) * (size_t)slots));
+    SCATT_TRY(sc.gj.alloc((1 + SCHUR_CHUNK) * (size_t)slots));
+    b.gmT = sc.gm.p; b.gmF = sc.gm.p + slots;
+    b.gmG1 = sc.gm.p + 2 * slots; b.gmG2 = sc.gm.p + 3 * slots; b.gmG3 = sc.gm.p + 4 * slots;
+    b.gmS = sc.gm.p + 5 * slots;                   // SCHUR_CHUNK x slots
+    b.gjR = sc.gj.p; b.gjS = sc.gj.p + slots;      // gjS: SCHUR_CHUNK x slots
+    // ---- post-stage buffers for one group
+    SCATT_TRY(sc.vb.alloc(b));
     {
-        size_t tot = 0, itot2 = 0;
-        for (auto& d : bt.ed) {
-            const size_t np2 = (size_t)d.Np * d.Np;
-            tot += 6 * d.Np + 14 * np2 + (size_t)Nf * d.Np + 2 * (size_t)d.Nt * d.Np + 12 * np2 +
-                   2 * (size_t)(d.l_cont + 1) * nfit + 8 * (size_t)(d.l_cont + 1) + 2 * np2 + (size_t)K * d.Np +
-                   (6 * 4 + 2 * 2 * 0) * (size_t)d.Np + 2 * (size_t)t.n_occ * d.Np + 8 * (size_t)d.Np + 2 * np2 + 64;
-            itot2 += 4 * (size_t)d.Np + 8;
-        }
-        SCATT_TRY(parena.alloc(tot));
-        SCATT_TRY(pia.alloc(itot2));
-        double* p = parena.p;
-        int* q = pia.p;
-        for (int e = 0; e < count; ++e) {
-            const EnergyDev& d = bt.ed[e];
-            const size_t np2 = (size_t)d.Np * d.Np;
-            Post& x = P[e];
-            x.tab = p; p += 6 * d.Np;
+        const int Np = sc.Np_cap, Nt = sc.Nt_cap;
+        const size_t pd = post_doubles(b, Np, Nt, l_cap, sc.nfit, t.n_occ);
+        SCATT_TRY(sc.parena.alloc(pd * sc.gs));
+        SCATT_TRY(sc.pia.alloc((4 * (size_t)Np + 8) * sc.gs));
+        sc.P.assign(sc.gs, PostBufs{});
+        const size_t np2 = (size_t)Np * Np;
+        for (int i = 0; i < sc.gs; ++i) {
+            double* p = sc.parena.p + pd * i;
+            int* q = sc.pia.p + (4 * (size_t)Np + 8) * i;
+            PostBufs& x = sc.P[i];
+            x.tab = p; p += 6 * Np;
             x.Amat = p; p += np2; x.Bmat = p; p += np2; x.Bw = p; p += np2; x.Binv = p; p += np2;
             x.Kraw = p; p += np2; x.K = p; p += np2; x.psibc = p; p += np2; x.VP = p; p += np2;
             x.Bf = p; p += np2; x.rhs = p; p += np2; x.Aaa = p; p += np2; x.Baa = p; p += np2;
             x.Aw = p; p += np2; x.Ainv = p; p += np2;
-            x.fN = p; p += (size_t)Nf * d.Np;
-            x.Z0 = p; p += (size_t)d.Nt * d.Np; x.Z1 = p; p += (size_t)d.Nt * d.Np;
+            x.fN = p; p += (size_t)Nf * Np;
+            x.Z0 = p; p += (size_t)Nt * Np; x.Z1 = p; p += (size_t)Nt * Np;
             x.Q = p; p += 4 * np2; x.Qw = p; p += 4 * np2; x.Qinv = p; p += 4 * np2;
-            x.aatab = p; p += 2 * (size_t)(d.l_cont + 1) * nfit;
-            x.aaM = p; p += 8 * (size_t)(d.l_cont + 1);
+            x.aatab = p; p += 2 * (size_t)(l_cap + 1) * sc.nfit;
+            x.aaM = p; p += 8 * (size_t)(l_cap + 1);
             x.aared = p; p += 2 * np2;
-            x.dall = p; p += (size_t)K * d.Np;
-            x.Dre = p; p += 6 * (size_t)d.Np; x.Dim = p; p += 6 * (size_t)d.Np;
-            x.Drre = p; p += 6 * (size_t)d.Np; x.Drim = p; p += 6 * (size_t)d.Np;
-            x.ore = p; p += (size_t)t.n_occ * d.Np; x.oim = p; p += (size_t)t.n_occ * d.Np;
-            x.ew_d = p; p += 2 * (size_t)d.Np; x.ew_e = p; p += 2 * (size_t)d.Np; x.ew_w = p; p += 2 * (size_t)d.Np;
-            x.eigK = p; p += (size_t)d.Np; x.eigA = p; p += (size_t)d.Np;
+            x.dall = p; p += (size_t)K * Np;
+            x.Dre = p; p += 6 * (size_t)Np; x.Dim = p; p += 6 * (size_t)Np;
+            x.Drre = p; p += 6 * (size_t)Np; x.Drim = p; p += 6 * (size_t)Np;
+            x.ore = p; p += (size_t)t.n_occ * Np; x.oim = p; p += (size_t)t.n_occ * Np;
+            x.ew_d = p; p += 2 * (size_t)Np; x.ew_e = p; p += 2 * (size_t)Np; x.ew_w = p; p += 2 * (size_t)Np;
+            x.eigK = p; p += (size_t)Np; x.eigA = p; p += (size_t)Np;
             x.Kc = p; p += 2 * np2;
-            x.sig = q; q += 2 * d.Np; x.rid = q; q += 2 * d.Np; x.st = q; q += 8;
+            x.sig = q; q += 2 * Np; x.rid = q; q += 2 * Np; x.st = q; q += 8;
         }
     }
-    Launcher L{s};
-    std::vector<int> status(count, SCATT_OK);
-    for (int e = 0; e < count; ++e)
+    SCATT_CUDA_TRY(cudaStreamSynchronize(s));
+    return SCATT_OK;
+}
+
+// Moves queued energies into the free slots of group g and starts the group
+// at n = 0 (no-op when the queue is empty).
+int load_group(Scan& sc, int g) {
+    if (sc.queue.empty()) return SCATT_OK;
+    cudaStream_t s = sc.ctx->stream;
+    const int e0 = g * sc.gs, e1 = std::min(sc.slots, e0 + sc.gs);
+    const BatchDev& b = sc.b;
+    for (int e = e0; e < e1; ++e) {
+        EnergyDev& d = sc.ed[e];
+        if (sc.queue.empty()) {
+            d.live = 0;
+            sc.job_of[e] = -1;
+            continue;
+        }
+        const Job j = sc.queue.front();
+        sc.queue.pop_front();
+        d.E = j.E;
+        d.c = 1.0 + b.h2_6 * j.E;
+        d.k = std::sqrt(2.0 * j.E);
+        d.l_cont = j.l_cont;
+        d.Np = (j.l_cont + 1) * (j.l_cont + 1);
+        d.Nt = d.Np + b.Nf;
+        d.shiftsA = d.shiftsS = 0;
+        d.deltaA = 0.0;
+        for (double& x : d.deltaAc) x = 0.0;
+        d.err_code = d.err_step = 0;
+        d.live = 1;
+        SCATT_TRY(stab_for(sc, j.l_cont, &d.lmA, &d.lmS));
+        sc.job_of[e] = j.index;
+        SCATT_CUDA_TRY(cudaMemsetAsync(d.G0, 0, (size_t)b.Krows * d.Nt * sizeof(double), s));
+    }
+    // a pageable copy: the host copy may change as soon as the call returns
+    SCATT_CUDA_TRY(cudaMemcpyAsync(sc.d_ed.p + e0, sc.ed.data() + e0, (size_t)(e1 - e0) * sizeof(EnergyDev),
+                                   cudaMemcpyHostToDevice, s));
+    k_set_group<<<1, 1, 0, s>>>(sc.b, g, 0);
+    SCATT_COUNT_LAUNCH(1);
+    sc.grp[g].n0 = 0;
+    sc.grp[g].C = std::min(SCHUR_CHUNK, b.n_stop);
+    return SCATT_OK;
+}
+
+struct ChunkTiming {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> rinv;   // sampled R^-1 inversions
+    double flops = 0.0;                                       // 2 n^3 over their matrices
+};
+
+// One chunk of SCHUR_CHUNK radial steps for every running group.  With
+// opts.use_graphs the chunk's launches are replayed from a CUDA graph: every
+// kernel reads its radial step from the device-resident group state and its
+// entries from device-side preparation, so one captured graph serves every
+// chunk whose running groups need the same stages at each chunk position.
+int run_chunk(Scan& sc, ChunkTiming* tm) {
+    BatchDev& b = sc.b;
+    cudaStream_t s = sc.ctx->stream;
+    const int count = sc.slots, G = sc.G, Nf = b.Nf;
+    // what the running groups need at each chunk position (host mirror)
+    bool step[SCHUR_CHUNK] = {}, exch[SCHUR_CHUNK] = {}, start[SCHUR_CHUNK] = {}, rinv[SCHUR_CHUNK] = {};
+    bool sweep[SCHUR_CHUNK] = {}, pts[SCHUR_CHUNK] = {};
+    bool stab = false, stab_x = false, any_exch = false;
+    int live_rinv[SCHUR_CHUNK] = {};
+    std::vector<int> live_in(G, 0);
+    for (int e = 0; e < count; ++e) live_in[sc.ed[e].grp] += sc.ed[e].live;
+    for (int g = 0; g < G; ++g) {
+        const GroupDev& gr = sc.grp[g];
+        if (gr.n0 < 0) continue;
+        for (int j = 0; j < gr.C; ++j) {
+            const int n = gr.n0 + j;
+            step[j] = true;
+            const bool x = n < b.n_tr && Nf > 0;
+            exch[j] |= x;
+            any_exch |= x;
+            start[j] |= n < b.n_start;
+            if (n >= b.n_start) { rinv[j] = true; live_rinv[j] += live_in[g]; }
+            sweep[j] |= n <= b.N - 1;
+            pts[j] |= n < b.n_pts && n <= b.N - 1;
+            stab |= n < b.stab_n;
+            stab_x |= n < b.stab_n && x;
+        }
+    }
+    // one R^-1 call in two chunks is timed (one in 16 under graphs) while every slot takes part
+    const bool sample_chunk = tm && rinv[0] && live_rinv[0] == count &&
+                              (sc.chunk % (sc.o.use_graphs ? 16 : 2) == 0);
+    auto issue = [&]() -> int {
+        // ---- Schur complements of the chunk's steps: A(n), S(n) = A - Bs B^T, one batched inverse
+        k_build_V<<<dim3(cdiv(b.n_pairs, TPB), G, SCHUR_CHUNK), TPB, 0, s>>>(b);
+        SCATT_COUNT_LAUNCH(1);
+        {
+            const int rows = std::max(b.Np_max * b.n_sigma, b.Nf);
+            k_build_B<<<dim3(cdiv(rows, 128), G, SCHUR_CHUNK), 128, 0, s>>>(b);
+            SCATT_COUNT_LAUNCH(1);
+        }
+        k_init_S<<<dim3(64, count, SCHUR_CHUNK), TPB, 0, s>>>(b);
+        SCATT_COUNT_LAUNCH(1);
+        if (stab) { k_stab<<<dim3(count, SCHUR_CHUNK), TPB, 0, s>>>(b, 0); SCATT_COUNT_LAUNCH(1); }
+        k_prepare_schur<<<cdiv(count * SCHUR_CHUNK, 128), 128, 0, s>>>(b);
+        SCATT_COUNT_LAUNCH(1);
+        if (any_exch) SCATT_TRY(gemm_slots(sc, b.gmS, count * SCHUR_CHUNK, 0, 0, 1));
+        if (stab_x) { k_stab<<<dim3(count, SCHUR_CHUNK), TPB, 0, s>>>(b, 1); SCATT_COUNT_LAUNCH(1); }
+        SCATT_TRY(gj_inverse_selected(b.gjS, count * SCHUR_CHUNK, sc.Np_cap, true, s, true));
+        // ---- the R-ratio recurrence over the chunk's steps
+        const dim3 eg(64, count);
+        for (int j = 0; j < SCHUR_CHUNK; ++j) {
+            if (!step[j]) continue;
+            k_prepare<<<cdiv(count, 128), 128, 0, s>>>(b, j);
+            SCATT_COUNT_LAUNCH(1);
+            if (start[j]) { k_vdiag<<<dim3(cdiv(b.Np_max, 128), G), 128, 0, s>>>(b, j); SCATT_COUNT_LAUNCH(1); }
+            k_collect<<<cdiv(count, 128), 128, 0, s>>>(b, j, 0);
+            SCATT_COUNT_LAUNCH(1);
+            if (exch[j]) {
+                SCATT_TRY(gemm_slots(sc, b.gmT, count, 1, 0, 0));
+                SCATT_TRY(gemm_slots(sc, b.gmF, count, 2, 1, 0));
+            }
+            if (start[j]) {
+                k_analytic_R<<<eg, TPB, 0, s>>>(b, j);
+                SCATT_COUNT_LAUNCH(1);
+                k_analytic_R_diag<<<dim3(4, count), TPB, 0, s>>>(b, j);
+                SCATT_COUNT_LAUNCH(1);
+            }
+            if (rinv[j]) {
+                k_assemble_R<<<eg, TPB, 0, s>>>(b, j);
+                SCATT_COUNT_LAUNCH(1);
+                const bool sample = sample_chunk && j == 0;
+                cudaEvent_t a0 = nullptr, a1 = nullptr;
+                if (sample) {
+                    SCATT_TRY(sc.events.get(&a0));
+                    SCATT_TRY(sc.events.get(&a1));
+                    SCATT_CUDA_TRY(cudaEventRecord(a0, s));
+                }
+                SCATT_TRY(gj_inverse_selected(b.gjR, count, sc.Nt_cap, true, s, true));
+                if (sample) {
+                    SCATT_CUDA_TRY(cudaEventRecord(a1, s));
+                    tm->rinv.push_back({a0, a1});
+                    for (int e = 0; e < count; ++e) {
+                        const GroupDev& gr = sc.grp[sc.ed[e].grp];
+                        const double n = (gr.n0 < b.n_tr && Nf > 0) ? sc.ed[e].Nt : sc.ed[e].Np;
+                        tm->flops += 2.0 * n * n * n;
+                    }
+                }
+                k_collect<<<cdiv(count, 128), 128, 0, s>>>(b, j, 1);
+                SCATT_COUNT_LAUNCH(1);
+            }
+            if (sweep[j]) {
+                if (pts[j]) SCATT_TRY(gemm_slots(sc, b.gmG1, count, 3, 0, 0));
+                if (pts[j] && exch[j]) SCATT_TRY(gemm_slots(sc, b.gmG2, count, 4, 0, 0));
+                SCATT_TRY(gemm_slots(sc, b.gmG3, count, 5, 0, 0));
+            }
+        }
+        k_advance<<<1, MAX_GROUPS, 0, s>>>(b);
+        SCATT_COUNT_LAUNCH(1);
+        return SCATT_CUDA_TRY_RET(cudaGetLastError());
+    };
+    uint64_t key = (stab ? 1u : 0u) | (stab_x ? 2u : 0u) | (any_exch ? 4u : 0u);
+    for (int j = 0; j < SCHUR_CHUNK; ++j) {
+        const uint64_t bits = (step[j] ? 1u : 0u) | (exch[j] ? 2u : 0u) | (start[j] ? 4u : 0u) |
+                              (rinv[j] ? 8u : 0u) | (sweep[j] ? 16u : 0u) | (pts[j] ? 32u : 0u);
+        key |= bits << (3 + 6 * j);
+    }
+    if (sc.o.use_graphs && !sample_chunk && sc.chunk > 0) {
+        const auto gk = std::make_pair(key, b.n_stop);
+        auto it = sc.graphs.find(gk);
+        if (it == sc.graphs.end()) {
+            SCATT_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            const unsigned long long l0 = launch_counter();
+            const int st = issue();
+            cudaGraph_t g = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(s, &g);
+            const unsigned long long nl = launch_counter() - l0;
+            launch_counter().fetch_sub(nl);          // captured, not launched
+            if (st != SCATT_OK) { if (g) cudaGraphDestroy(g); return st; }
+            if (ce != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_status(ce, "cudaStreamEndCapture"); }
+            cudaGraphExec_t ex = nullptr;
+            const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess) return cuda_status(ie, "cudaGraphInstantiate");
+            it = sc.graphs.emplace(gk, Scan::Graph{ex, nl}).first;
+        }
+        SCATT_CUDA_TRY(cudaGraphLaunch(it->second.exec, s));
+        SCATT_COUNT_LAUNCH(it->second.launches);
+    } else {
+        SCATT_TRY(issue());
+    }
+    for (auto& gr : sc.grp) {
+        if (gr.n0 < 0) continue;
+        const int n0 = gr.n0 + gr.C;
+        if (n0 >= b.n_stop) { gr.n0 = -2; gr.C = 0; }      // finished: post stages pending
+        else { gr.n0 = n0; gr.C = std::min(SCHUR_CHUNK, b.n_stop - n0); }
+    }
+    ++sc.chunk;
+    return SCATT_OK;
+}
+
+// Post stages of the slots `sel` of one group, whose sweep has reached N:
+// K extraction, the outer boundary value, the backward sweep over the
+// asymptotic window, the amplitude fit and the dipoles.  Outputs go to rows
+// `rows` of `out`.  A failed energy (singular pivot, closed channel) leaves
+// its status in out->status and the first one in *first_status / *first_msg.
+int post_slots(Scan& sc, const std::vector<int>& sel, const std::vector<long>& rows, const scatt_outputs* out,
+               int* first_status, std::string* first_msg) {
+    ScanTables& t = *sc.ctx->tab;
+    const scatt_solve_opts& o = sc.o;
+    cudaStream_t s = sc.ctx->stream;
+    BatchDev& b = sc.b;
+    const int cnt = (int)sel.size();
+    if (cnt == 0) return SCATT_OK;
+    const int N = b.N, K = b.Krows, Nf = b.Nf;
+    const int ne_fit = sc.ne_fit, nfit = sc.nfit;
+    auto ED = [&](int i) -> const EnergyDev& { return sc.ed[sel[i]]; };
+    std::vector<PostBufs>& P = sc.P;
+    Launcher& L = sc.L;
+    int maxNp = 0;
+    for (int e = 0; e < cnt; ++e) maxNp = std::max(maxNp, ED(e).Np);
+    // the slots' device counters: stability shifts and the first failing step
+    std::vector<EnergyDev> edh(cnt);
+    SCATT_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int e = 0; e < cnt; ++e)
+        SCATT_CUDA_TRY(cudaMemcpy(&edh[e], sc.d_ed.p + sel[e], sizeof(EnergyDev), cudaMemcpyDeviceToHost));
+    std::vector<int> status(cnt, SCATT_OK);
+    for (int e = 0; e < cnt; ++e)
         if (edh[e].err_code) status[e] = edh[e].err_code;
 
     // ---- KMatrixExtractor (KMatrixExtractor.cpp:75-198), n_match = Nr - 2
     {
         std::vector<CopyEntry> cp;
         std::vector<GjEntry> gj;
-        for (int e = 0; e < count; ++e) {
-            const EnergyDev& d = bt.ed[e];
+        for (int e = 0; e < cnt; ++e) {
+            const EnergyDev& d = ED(e);
             const double* rin = d.tailR + (size_t)(N - 1 - b.n_s) * d.Nt * d.Nt;
             cp.push_back(CopyEntry{rin, d.Ra, d.Nt, d.Nt, d.Nt, d.Nt, 1.0});
             gj.push_back(GjEntry{d.Ra, d.Rw, d.Rinv0, d.sigR, d.ridR, d.stR, d.Nt, d.Nt, d.Nt});
@@ -1402,27 +1749,27 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         SCATT_TRY(L.copy(cp));
         SCATT_TRY(L.gj(gj, false));
         // coupling norms
-        std::vector<const double*> Rp(count);
-        std::vector<int> np(count), nt(count);
-        for (int e = 0; e < count; ++e) { Rp[e] = bt.ed[e].Rinv0; np[e] = bt.ed[e].Np; nt[e] = bt.ed[e].Nt; }
+        std::vector<const double*> Rp(cnt);
+        std::vector<int> np(cnt), nt(cnt);
+        for (int e = 0; e < cnt; ++e) { Rp[e] = ED(e).Rinv0; np[e] = ED(e).Np; nt[e] = ED(e).Nt; }
         DevBuf<const double*> dRp;
         DevBuf<int> dnp, dnt;
         DevBuf<double> dnorm;
         SCATT_TRY(upload_vec(dRp, Rp, s));
         SCATT_TRY(upload_vec(dnp, np, s));
         SCATT_TRY(upload_vec(dnt, nt, s));
-        SCATT_TRY(dnorm.alloc(2 * (size_t)count));
-        k_block_norms<<<count, TPB, 0, s>>>(dRp.p, dnp.p, dnt.p, dnorm.p);
+        SCATT_TRY(dnorm.alloc(2 * (size_t)cnt));
+        k_block_norms<<<cnt, TPB, 0, s>>>(dRp.p, dnp.p, dnt.p, dnorm.p);
         SCATT_COUNT_LAUNCH(1);
-        std::vector<double> norms(2 * count);
+        std::vector<double> norms(2 * cnt);
         SCATT_CUDA_TRY(cudaMemcpyAsync(norms.data(), dnorm.p, norms.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
         SCATT_CUDA_TRY(cudaStreamSynchronize(s));
         std::vector<CopyEntry> c2, c3;
         std::vector<GjEntry> g2;
         std::vector<GemmEntry> m1, m2;
-        std::vector<int> coupled(count, 0);
-        for (int e = 0; e < count; ++e) {
-            const EnergyDev& d = bt.ed[e];
+        std::vector<int> coupled(cnt, 0);
+        for (int e = 0; e < cnt; ++e) {
+            const EnergyDev& d = ED(e);
             const int Np = d.Np, Nt = d.Nt;
             // S_schur starts as R_psi_psi
             c2.push_back(CopyEntry{d.Rinv0, d.Sw, Np, Np, Nt, Np, 1.0});
@@ -1441,23 +1788,23 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         SCATT_TRY(L.gemm(m1, 0, 0));
         SCATT_TRY(L.gemm(m2, 0, 0));
         std::vector<KmeEntry> ke;
-        for (int e = 0; e < count; ++e) {
-            const EnergyDev& d = bt.ed[e];
+        for (int e = 0; e < cnt; ++e) {
+            const EnergyDev& d = ED(e);
             ke.push_back(KmeEntry{d.Sw, P[e].Amat, P[e].Bmat, P[e].tab, d.Np, d.k});
         }
         DevBuf<KmeEntry> dke;
         SCATT_TRY(upload_vec(dke, ke, s));
-        k_kme_tab<<<dim3(cdiv(maxNp, 128), count), 128, 0, s>>>(dke.p, t.d_l_of_mu.p, t.dr, t.Nr);
+        k_kme_tab<<<dim3(cdiv(maxNp, 128), cnt), 128, 0, s>>>(dke.p, t.d_l_of_mu.p, t.dr, t.Nr);
         SCATT_COUNT_LAUNCH(1);
-        k_kme_mats<<<dim3(64, count), TPB, 0, s>>>(dke.p);
+        k_kme_mats<<<dim3(64, cnt), TPB, 0, s>>>(dke.p);
         SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaGetLastError());
         // K = B_mat^-1 A_mat (the reference solves with partial-pivot LU)
         std::vector<CopyEntry> c4;
         std::vector<GjEntry> g4;
         std::vector<GemmEntry> m4;
-        for (int e = 0; e < count; ++e) {
-            const int Np = bt.ed[e].Np;
+        for (int e = 0; e < cnt; ++e) {
+            const int Np = ED(e).Np;
             c4.push_back(CopyEntry{P[e].Bmat, P[e].Bw, Np, Np, Np, Np, 1.0});
             g4.push_back(GjEntry{P[e].Bw, P[e].Kc, P[e].Binv, P[e].sig, P[e].rid, P[e].st, Np, Np, Np});
             m4.push_back(GemmEntry{P[e].Binv, P[e].Amat, P[e].Kraw, Np, Np, Np, Np, Np, Np, 1.0, 0.0});
@@ -1465,32 +1812,31 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         SCATT_TRY(L.copy(c4));
         SCATT_TRY(L.gj(g4, false));
         SCATT_TRY(L.gemm(m4, 0, 0));
-        std::vector<const double*> kr(count);
-        std::vector<double*> ko(count), pb(count);
-        for (int e = 0; e < count; ++e) { kr[e] = P[e].Kraw; ko[e] = P[e].K; pb[e] = P[e].psibc; }
+        std::vector<const double*> kr(cnt);
+        std::vector<double*> ko(cnt), pb(cnt);
+        for (int e = 0; e < cnt; ++e) { kr[e] = P[e].Kraw; ko[e] = P[e].K; pb[e] = P[e].psibc; }
         DevBuf<const double*> dkr;
         DevBuf<double*> dko, dpb;
         SCATT_TRY(upload_vec(dkr, kr, s));
         SCATT_TRY(upload_vec(dko, ko, s));
         SCATT_TRY(upload_vec(dpb, pb, s));
-        k_kme_final<<<dim3(64, count), TPB, 0, s>>>(dke.p, dkr.p, dko.p, dpb.p);
+        k_kme_final<<<dim3(64, cnt), TPB, 0, s>>>(dke.p, dkr.p, dko.p, dpb.p);
         SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaGetLastError());
         SCATT_CUDA_TRY(cudaStreamSynchronize(s));
-        for (int e = 0; e < count; ++e) bt.ed[e].shiftsA = coupled[e];   // reuse slot for schur flag below
-        for (int e = 0; e < count; ++e) edh[e].deltaA = coupled[e] ? 0.0 : 1.0;
+        for (int e = 0; e < cnt; ++e) edh[e].deltaA = coupled[e] ? 0.0 : 1.0;
     }
 
     // ---- outer boundary Z_N (BackPropagator.cpp:127-197) and the dipole contraction
-    launch_VB(b, N, s);
+    sc.vb.build(b, N, s);
     {
         std::vector<GemmEntry> mv, mf, mb;
-        for (int e = 0; e < count; ++e) {
-            const EnergyDev& d = bt.ed[e];
+        for (int e = 0; e < cnt; ++e) {
+            const EnergyDev& d = ED(e);
             const int Np = d.Np;
-            mv.push_back(GemmEntry{b.V, P[e].psibc, P[e].VP, Np, Np, Np, b.Np_max, Np, Np, b.h2_6, 0.0});
+            mv.push_back(GemmEntry{sc.vb.V.p, P[e].psibc, P[e].VP, Np, Np, Np, b.Np_max, Np, Np, b.h2_6, 0.0});
             if (N < b.n_tr && Nf > 0) {
-                mf.push_back(GemmEntry{b.B, P[e].psibc, P[e].fN, Nf, Np, Np, b.Np_max, Np, Nf, 1.0, 0.0});
+                mf.push_back(GemmEntry{sc.vb.B.p, P[e].psibc, P[e].fN, Nf, Np, Np, b.Np_max, Np, Nf, 1.0, 0.0});
             }
         }
         SCATT_TRY(L.gemm(mv, 0, 0));
@@ -1499,27 +1845,27 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
             // f_N = -D^-1 (B^T psi): scale rows by -Dinv through a copy-with-scale per f row is
             // not expressible as one CopyEntry; do it with a tiny GEMM-free kernel via Bs^T:
             // B_N f_N = B_N (-(D^-1 B^T psi)) = -(Bs_N)(B_N^T psi) with Bs = B D^-1.
-            for (int e = 0; e < count; ++e) {
-                const int Np = bt.ed[e].Np;
-                mb.push_back(GemmEntry{b.Bs, P[e].fN, P[e].Bf, Np, Np, Nf, b.Np_max, Nf, Np, -1.0, 0.0});
+            for (int e = 0; e < cnt; ++e) {
+                const int Np = ED(e).Np;
+                mb.push_back(GemmEntry{sc.vb.Bs.p, P[e].fN, P[e].Bf, Np, Np, Nf, b.Np_max, Nf, Np, -1.0, 0.0});
             }
             SCATT_TRY(L.gemm(mb, 0, 0));
         }
         std::vector<ZEntry> ze;
-        for (int e = 0; e < count; ++e) {
-            const EnergyDev& d = bt.ed[e];
+        for (int e = 0; e < cnt; ++e) {
+            const EnergyDev& d = ED(e);
             ze.push_back(ZEntry{P[e].psibc, P[e].VP, mb.empty() ? nullptr : P[e].Bf, P[e].Z0, d.Np, d.Nt,
                                 b.h2_6 * d.E});
         }
         DevBuf<ZEntry> dze;
         SCATT_TRY(upload_vec(dze, ze, s));
-        k_build_Z<<<dim3(64, count), TPB, 0, s>>>(dze.p);
+        k_build_Z<<<dim3(64, cnt), TPB, 0, s>>>(dze.p);
         SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaGetLastError());
         // d_all = G_{N-1} Z_N (+ C_N psi_N when N is inside the dipole window)
         std::vector<GemmEntry> md, mc;
-        for (int e = 0; e < count; ++e) {
-            const EnergyDev& d = bt.ed[e];
+        for (int e = 0; e < cnt; ++e) {
+            const EnergyDev& d = ED(e);
             const double* Gf = (N & 1) ? d.G1 : d.G0;
             md.push_back(GemmEntry{Gf, P[e].Z0, P[e].dall, K, d.Np, d.Nt, K, d.Nt, K, 1.0, 0.0});
             if (N < b.n_pts)
@@ -1533,27 +1879,27 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
     // ---- backward sweep over the asymptotic window (BackPropagator.cpp:603-703)
     {
         std::vector<CopyEntry> c0;
-        for (int e = 0; e < count; ++e) {
-            const EnergyDev& d = bt.ed[e];
+        for (int e = 0; e < cnt; ++e) {
+            const EnergyDev& d = ED(e);
             c0.push_back(CopyEntry{P[e].psibc, d.psiT + (size_t)(N - b.n_s) * d.Np * d.Np, d.Np, d.Np, d.Np, d.Np, 1.0});
         }
         SCATT_TRY(L.copy(c0));
-        std::vector<double*> zc(count), zn(count);
-        for (int e = 0; e < count; ++e) { zc[e] = P[e].Z0; zn[e] = P[e].Z1; }
+        std::vector<double*> zc(cnt), zn(cnt);
+        for (int e = 0; e < cnt; ++e) { zc[e] = P[e].Z0; zn[e] = P[e].Z1; }
         for (int n = N - 1; n >= b.n_s; --n) {
             const bool exch = n < b.n_tr && Nf > 0;
-            if (exch) launch_VB(b, n, s);
+            if (exch) sc.vb.build(b, n, s);
             std::vector<GemmEntry> mz, mr, mp;
             std::vector<CopyEntry> cr;
-            for (int e = 0; e < count; ++e) {
-                const EnergyDev& d = bt.ed[e];
+            for (int e = 0; e < cnt; ++e) {
+                const EnergyDev& d = ED(e);
                 const int Np = d.Np, Nt = d.Nt;
                 const size_t slot = (size_t)(n - b.n_s);
                 mz.push_back(GemmEntry{d.tailR + slot * Nt * Nt, zc[e], zn[e], Nt, Np, Nt, Nt, Nt, Nt, 1.0, 0.0});
                 const double* sinv = d.tailS + slot * Np * Np;
                 if (exch) {
                     cr.push_back(CopyEntry{zn[e], P[e].rhs, Np, Np, Nt, Np, 1.0});
-                    mr.push_back(GemmEntry{b.Bs, zn[e] + Np, P[e].rhs, Np, Np, Nf, b.Np_max, Nt, Np, -1.0, 1.0});
+                    mr.push_back(GemmEntry{sc.vb.Bs.p, zn[e] + Np, P[e].rhs, Np, Np, Nf, b.Np_max, Nt, Np, -1.0, 1.0});
                     mp.push_back(GemmEntry{sinv, P[e].rhs, d.psiT + slot * Np * Np, Np, Np, Np, Np, Np, Np, 1.0, 0.0});
                 } else {
                     mp.push_back(GemmEntry{sinv, zn[e], d.psiT + slot * Np * Np, Np, Np, Np, Np, Nt, Np, 1.0, 0.0});
@@ -1568,42 +1914,42 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
     }
 
     // ---- AsymptoticAmplitudes (AsymptoticAmplitudes.cpp:64-359)
-    std::vector<double> aared(2 * count), aasym(2 * count);
-    std::vector<int> nclosed(count, 0);
+    std::vector<double> aared(2 * cnt), aasym(2 * cnt);
+    std::vector<int> nclosed(cnt, 0);
     {
         std::vector<AaEntry> ae;
         int maxl = 0;
-        for (int e = 0; e < count; ++e) {
-            const EnergyDev& d = bt.ed[e];
+        for (int e = 0; e < cnt; ++e) {
+            const EnergyDev& d = ED(e);
             ae.push_back(AaEntry{d.psiT, P[e].aatab, P[e].aaM, P[e].Aaa, P[e].Baa, P[e].aared, d.Np, d.l_cont, d.k});
             maxl = std::max(maxl, d.l_cont);
         }
         DevBuf<AaEntry> dae;
         SCATT_TRY(upload_vec(dae, ae, s));
-        k_aa_tab<<<dim3(64, count), TPB, 0, s>>>(dae.p, b.n_s, nfit, t.dr);
+        k_aa_tab<<<dim3(64, cnt), TPB, 0, s>>>(dae.p, b.n_s, nfit, t.dr);
         SCATT_COUNT_LAUNCH(1);
-        k_aa_normal<<<dim3(cdiv(maxl + 1, 64), count), 64, 0, s>>>(dae.p, nfit);
+        k_aa_normal<<<dim3(cdiv(maxl + 1, 64), cnt), 64, 0, s>>>(dae.p, nfit);
         SCATT_COUNT_LAUNCH(1);
-        k_aa_fit<<<dim3(64, count), TPB, 0, s>>>(dae.p, t.d_l_of_mu.p, nfit);
+        k_aa_fit<<<dim3(64, cnt), TPB, 0, s>>>(dae.p, t.d_l_of_mu.p, nfit);
         SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaGetLastError());
-        std::vector<const double*> rp(count);
-        std::vector<int> rc(count);
-        for (int e = 0; e < count; ++e) { rp[e] = P[e].aared; rc[e] = bt.ed[e].Np * bt.ed[e].Np; }
+        std::vector<const double*> rp(cnt);
+        std::vector<int> rc(cnt);
+        for (int e = 0; e < cnt; ++e) { rp[e] = P[e].aared; rc[e] = ED(e).Np * ED(e).Np; }
         DevBuf<const double*> drp;
         DevBuf<int> drc;
         DevBuf<double> dout;
         SCATT_TRY(upload_vec(drp, rp, s));
         SCATT_TRY(upload_vec(drc, rc, s));
-        SCATT_TRY(dout.alloc(2 * (size_t)count));
-        k_max_pairs<<<count, TPB, 0, s>>>(drp.p, drc.p, dout.p);
+        SCATT_TRY(dout.alloc(2 * (size_t)cnt));
+        k_max_pairs<<<cnt, TPB, 0, s>>>(drp.p, drc.p, dout.p);
         SCATT_COUNT_LAUNCH(1);
-        SCATT_CUDA_TRY(cudaMemcpyAsync(aared.data(), dout.p, 2 * count * sizeof(double), cudaMemcpyDeviceToHost, s));
+        SCATT_CUDA_TRY(cudaMemcpyAsync(aared.data(), dout.p, 2 * cnt * sizeof(double), cudaMemcpyDeviceToHost, s));
         SCATT_CUDA_TRY(cudaStreamSynchronize(s));
-        for (int e = 0; e < count; ++e) {
-            std::vector<double> M(8 * (size_t)(bt.ed[e].l_cont + 1));
+        for (int e = 0; e < cnt; ++e) {
+            std::vector<double> M(8 * (size_t)(ED(e).l_cont + 1));
             SCATT_CUDA_TRY(cudaMemcpy(M.data(), P[e].aaM, M.size() * sizeof(double), cudaMemcpyDeviceToHost));
-            for (int l = 0; l <= bt.ed[e].l_cont; ++l)
+            for (int l = 0; l <= ED(e).l_cont; ++l)
                 if (M[8 * l + 4] != 0.0) ++nclosed[e];
             if (nclosed[e] > 0 && !o.allow_closed_channels && status[e] == SCATT_OK) status[e] = SCATT_ERR_CLOSED_CHANNEL;
         }
@@ -1611,8 +1957,8 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         std::vector<CopyEntry> ca;
         std::vector<GjEntry> ga;
         std::vector<GemmEntry> mk;
-        for (int e = 0; e < count; ++e) {
-            const int Np = bt.ed[e].Np;
+        for (int e = 0; e < cnt; ++e) {
+            const int Np = ED(e).Np;
             ca.push_back(CopyEntry{P[e].Aaa, P[e].Aw, Np, Np, Np, Np, 1.0});
             ga.push_back(GjEntry{P[e].Aw, P[e].Kc, P[e].Ainv, P[e].sig, P[e].rid, P[e].st, Np, Np, Np});
             mk.push_back(GemmEntry{P[e].Baa, P[e].Ainv, P[e].Kc + (size_t)Np * Np, Np, Np, Np, Np, Np, Np, 1.0, 0.0});
@@ -1620,12 +1966,12 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         SCATT_TRY(L.copy(ca));
         SCATT_TRY(L.gj(ga, false));
         SCATT_TRY(L.gemm(mk, 0, 0));
-        std::vector<const double*> kp(count), ap(count);
-        std::vector<int> npv(count);
-        for (int e = 0; e < count; ++e) {
-            kp[e] = P[e].Kc + (size_t)bt.ed[e].Np * bt.ed[e].Np;
+        std::vector<const double*> kp(cnt), ap(cnt);
+        std::vector<int> npv(cnt);
+        for (int e = 0; e < cnt; ++e) {
+            kp[e] = P[e].Kc + (size_t)ED(e).Np * ED(e).Np;
             ap[e] = P[e].Aaa;
-            npv[e] = bt.ed[e].Np;
+            npv[e] = ED(e).Np;
         }
         DevBuf<const double*> dkp, dap;
         DevBuf<int> dnpv;
@@ -1633,27 +1979,27 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         SCATT_TRY(upload_vec(dkp, kp, s));
         SCATT_TRY(upload_vec(dap, ap, s));
         SCATT_TRY(upload_vec(dnpv, npv, s));
-        SCATT_TRY(dsk.alloc(2 * (size_t)count));
-        SCATT_TRY(dsa.alloc(2 * (size_t)count));
-        k_sym_err<<<count, TPB, 0, s>>>(dkp.p, dnpv.p, dsk.p);
+        SCATT_TRY(dsk.alloc(2 * (size_t)cnt));
+        SCATT_TRY(dsa.alloc(2 * (size_t)cnt));
+        k_sym_err<<<cnt, TPB, 0, s>>>(dkp.p, dnpv.p, dsk.p);
         SCATT_COUNT_LAUNCH(1);
-        k_sym_err<<<count, TPB, 0, s>>>(dap.p, dnpv.p, dsa.p);
+        k_sym_err<<<cnt, TPB, 0, s>>>(dap.p, dnpv.p, dsa.p);
         SCATT_COUNT_LAUNCH(1);
-        std::vector<double> sk(2 * count), sa(2 * count);
+        std::vector<double> sk(2 * cnt), sa(2 * cnt);
         SCATT_CUDA_TRY(cudaMemcpyAsync(sk.data(), dsk.p, sk.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
         SCATT_CUDA_TRY(cudaMemcpyAsync(sa.data(), dsa.p, sa.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
         SCATT_CUDA_TRY(cudaStreamSynchronize(s));
-        for (int e = 0; e < count; ++e) { aasym[2 * e] = sk[2 * e]; aasym[2 * e + 1] = sa[2 * e + 1]; }
+        for (int e = 0; e < cnt; ++e) { aasym[2 * e] = sk[2 * e]; aasym[2 * e + 1] = sa[2 * e + 1]; }
     }
 
     // ---- DipoleMatrixElement finalisation (DipoleMatrixElement.cpp:673-947)
     {
-        std::vector<const double*> ap(count), bp;
-        std::vector<double*> qp(count);
-        std::vector<int> npv(count);
-        bp.resize(count);
-        for (int e = 0; e < count; ++e) {
-            ap[e] = P[e].Aaa; bp[e] = P[e].Baa; qp[e] = P[e].Q; npv[e] = bt.ed[e].Np;
+        std::vector<const double*> ap(cnt), bp;
+        std::vector<double*> qp(cnt);
+        std::vector<int> npv(cnt);
+        bp.resize(cnt);
+        for (int e = 0; e < cnt; ++e) {
+            ap[e] = P[e].Aaa; bp[e] = P[e].Baa; qp[e] = P[e].Q; npv[e] = ED(e).Np;
         }
         DevBuf<const double*> dap, dbp;
         DevBuf<double*> dqp;
@@ -1662,12 +2008,12 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         SCATT_TRY(upload_vec(dbp, bp, s));
         SCATT_TRY(upload_vec(dqp, qp, s));
         SCATT_TRY(upload_vec(dnp, npv, s));
-        k_embed<<<dim3(64, count), TPB, 0, s>>>(dap.p, dbp.p, dqp.p, dnp.p);
+        k_embed<<<dim3(64, cnt), TPB, 0, s>>>(dap.p, dbp.p, dqp.p, dnp.p);
         SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaGetLastError());
         std::vector<GjEntry> gq;
-        for (int e = 0; e < count; ++e) {
-            const int n2 = 2 * bt.ed[e].Np;
+        for (int e = 0; e < cnt; ++e) {
+            const int n2 = 2 * ED(e).Np;
             gq.push_back(GjEntry{P[e].Q, P[e].Qw, P[e].Qinv, P[e].sig, P[e].rid, P[e].st, n2, n2, n2});
         }
         SCATT_TRY(L.gj(gq, false));
@@ -1675,26 +2021,26 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         SCATT_TRY(upload_vec(ddc, t.d_corr, s));
         SCATT_TRY(upload_vec(dsp, t.spin, s));
         std::vector<DmeEntry> de;
-        for (int e = 0; e < count; ++e)
+        for (int e = 0; e < cnt; ++e)
             de.push_back(DmeEntry{P[e].Qinv, P[e].dall, ddc.p, dsp.p, P[e].Dre, P[e].Dim, P[e].Drre, P[e].Drim,
-                                  P[e].ore, P[e].oim, bt.ed[e].Np, K, t.n_occ});
+                                  P[e].ore, P[e].oim, ED(e).Np, K, t.n_occ});
         DevBuf<DmeEntry> dde;
         SCATT_TRY(upload_vec(dde, de, s));
-        k_dme_o<<<dim3(64, count), TPB, 0, s>>>(dde.p);
+        k_dme_o<<<dim3(64, cnt), TPB, 0, s>>>(dde.p);
         SCATT_COUNT_LAUNCH(1);
-        k_dme_D<<<dim3(16, count), TPB, 0, s>>>(dde.p, o.orthogonalize);
+        k_dme_D<<<dim3(16, cnt), TPB, 0, s>>>(dde.p, o.orthogonalize);
         SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaGetLastError());
         SCATT_CUDA_TRY(cudaStreamSynchronize(s));
     }
 
     // ---- eigenphases (diagnostics)
-    std::vector<std::vector<double>> eigk(count), eiga(count);
+    std::vector<std::vector<double>> eigk(cnt), eiga(cnt);
     if (o.diagnostics) {
         std::vector<CopyEntry> cc;
         std::vector<EigEntry> ee;
-        for (int e = 0; e < count; ++e) {
-            const int Np = bt.ed[e].Np;
+        for (int e = 0; e < cnt; ++e) {
+            const int Np = ED(e).Np;
             cc.push_back(CopyEntry{P[e].K, P[e].Amat, Np, Np, Np, Np, 1.0});
             cc.push_back(CopyEntry{P[e].Kc + (size_t)Np * Np, P[e].Bmat, Np, Np, Np, Np, 1.0});
             ee.push_back(EigEntry{P[e].Amat, Np, Np, P[e].ew_d, P[e].ew_e, P[e].ew_w, P[e].eigK});
@@ -1705,8 +2051,8 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         SCATT_TRY(upload_vec(dee, ee, s));
         SCATT_TRY(sym_eigvals_batched(dee.p, (int)ee.size(), maxNp, 0, s));
         SCATT_CUDA_TRY(cudaStreamSynchronize(s));
-        for (int e = 0; e < count; ++e) {
-            const int Np = bt.ed[e].Np;
+        for (int e = 0; e < cnt; ++e) {
+            const int Np = ED(e).Np;
             eigk[e].resize(Np);
             eiga[e].resize(Np);
             SCATT_CUDA_TRY(cudaMemcpy(eigk[e].data(), P[e].eigK, Np * sizeof(double), cudaMemcpyDeviceToHost));
@@ -1714,43 +2060,11 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         }
     }
 
-    if (o.timing) {
-        cudaEventRecord(ev_end, s);
-        cudaEventSynchronize(ev_end);
-        float ms_all = 0.f, ms_sweep = 0.f;
-        cudaEventElapsedTime(&ms_all, ev_begin, ev_end);
-        cudaEventElapsedTime(&ms_sweep, ev_begin, ev_sweep);
-        double rs = 0.0;
-        for (size_t i = 0; i + 1 < rev.size(); i += 2) {
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, rev[i], rev[i + 1]);
-            rs += ms * 1e-3;
-            cudaEventDestroy(rev[i]);
-            cudaEventDestroy(rev[i + 1]);
-        }
-        ctx.stats.device_s += ms_all * 1e-3;
-        ctx.stats.sweep_s += ms_sweep * 1e-3;
-        ctx.stats.post_s += (ms_all - ms_sweep) * 1e-3;
-        ctx.stats.rinv_s += rs;
-        ctx.stats.rinv_calls += rev.size() / 2;
-        cudaEventDestroy(ev_begin);
-        cudaEventDestroy(ev_sweep);
-        cudaEventDestroy(ev_end);
-    }
-    ctx.stats.launches += launch_counter() - launches0;
-
     // ================================================================ outputs
     const int Npm = t.Np_max;
-    auto dl_mat = [&](double* host, int e, const double* dev, int rows, int cols, int ldd) -> int {
-        if (!host) return SCATT_OK;
-        double* h = host + (size_t)(offset + e) * Npm * (ldd == Npm ? cols : 1) * 0;
-        (void)h;
-        return SCATT_OK;
-    };
-    (void)dl_mat;
-    for (int e = 0; e < count; ++e) {
-        const EnergyDev& d = bt.ed[e];
-        const int Np = d.Np, ge = offset + e;
+    for (int e = 0; e < cnt; ++e) {
+        const EnergyDev& d = ED(e);
+        const int Np = d.Np, ge = rows[e];
         auto mat = [&](double* host, const double* dev) -> int {
             if (!host) return SCATT_OK;
             double* h = host + (size_t)ge * Npm * Npm;
@@ -1827,20 +2141,171 @@ int run_batch(Context& ctx, const scatt_solve_opts& o, int count, const double* 
         }
         if (out->status) out->status[ge] = status[e];
     }
-    for (int e = 0; e < count; ++e)
-        if (status[e] != SCATT_OK) {
+    for (int e = 0; e < cnt; ++e)
+        if (status[e] != SCATT_OK && *first_status == SCATT_OK) {
+            *first_status = status[e];
             if (status[e] == SCATT_ERR_CLOSED_CHANNEL)
-                set_last_error("AsymptoticAmplitudes: singular normal matrix (closed channel) at energy " +
-                               std::to_string(offset + e) + "; set allow_closed_channels");
+                *first_msg = "AsymptoticAmplitudes: singular normal matrix (closed channel) at energy " +
+                             std::to_string(rows[e]) + "; set allow_closed_channels";
             else
-                set_last_error("singular or non-finite pivot at energy " + std::to_string(offset + e) +
-                               ", radial step " + std::to_string(edh[e].err_step));
-            return status[e];
+                *first_msg = "singular or non-finite pivot at energy " + std::to_string(rows[e]) + ", radial step " +
+                             std::to_string(edh[e].err_step);
         }
     return SCATT_OK;
 }
 
+// Runs chunks until at least one group has finished its sweep, then its
+// post stages.  out_row(slot, i) gives the output row of the i-th finished
+// energy (held by `slot`).  *n_done receives the number of finished energies
+// (0: nothing was in flight and the queue is empty); done_jobs lists their
+// submission indices.
+template <class RowOf>
+int scan_advance(Scan& sc, const scatt_outputs* out, RowOf out_row, int* n_done, std::vector<long>* done_jobs,
+                 int* first_status, std::string* first_msg) {
+    cudaStream_t s = sc.ctx->stream;
+    *n_done = 0;
+    SolveStats& stats = sc.ctx->stats;
+    const unsigned long long launches0 = launch_counter();
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp = nullptr;
+    ChunkTiming tm;
+    sc.events.reset();
+    if (sc.o.timing) {
+        SCATT_TRY(sc.events.get(&ev0));
+        SCATT_TRY(sc.events.get(&ev1));
+        SCATT_TRY(sc.events.get(&evp));
+        SCATT_CUDA_TRY(cudaEventRecord(ev0, s));
+    }
+    std::vector<int> finished;
+    for (;;) {
+        // idle groups whose turn has come take queued energies
+        for (int g = 0; g < sc.G; ++g)
+            if (sc.grp[g].n0 == -1 && sc.chunk >= sc.start_chunk[g] && !sc.queue.empty())
+                SCATT_TRY(load_group(sc, g));
+        bool running = false, waiting = false;
+        for (int g = 0; g < sc.G; ++g) {
+            running |= sc.grp[g].n0 >= 0;
+            waiting |= sc.grp[g].n0 == -1 && sc.chunk < sc.start_chunk[g];
+        }
+        if (!running) {
+            if (sc.queue.empty() || !waiting) break;
+            // nothing runs until the next staggered start: start it now
+            long next = -1;
+            for (int g = 0; g < sc.G; ++g)
+                if (sc.grp[g].n0 == -1 && (next < 0 || sc.start_chunk[g] < next)) next = sc.start_chunk[g];
+            sc.chunk = std::max(sc.chunk, next);
+            continue;
+        }
+        SCATT_TRY(run_chunk(sc, sc.o.timing ? &tm : nullptr));
+        for (int g = 0; g < sc.G; ++g)
+            if (sc.grp[g].n0 == -2) finished.push_back(g);
+        if (!finished.empty()) break;
+    }
+    if (sc.o.timing) SCATT_CUDA_TRY(cudaEventRecord(evp, s));
+    for (int g : finished) {
+        std::vector<int> sel;
+        std::vector<long> rows;
+        for (int e = g * sc.gs; e < std::min(sc.slots, (g + 1) * sc.gs); ++e)
+            if (sc.ed[e].live) {
+                sel.push_back(e);
+                rows.push_back(out_row(e, *n_done + (int)sel.size() - 1));
+            }
+        SCATT_TRY(post_slots(sc, sel, rows, out, first_status, first_msg));
+        for (int e : sel) {
+            if (done_jobs) done_jobs->push_back(sc.job_of[e]);
+            sc.ed[e].live = 0;
+            sc.job_of[e] = -1;
+        }
+        *n_done += (int)sel.size();
+        sc.grp[g].n0 = -1;                    // k_advance already stopped it on the device
+        sc.start_chunk[g] = sc.chunk;         // refill at once: the group keeps its phase
+    }
+    if (sc.o.timing) {
+        SCATT_CUDA_TRY(cudaEventRecord(ev1, s));
+        SCATT_CUDA_TRY(cudaEventSynchronize(ev1));
+        float ms_all = 0.f, ms_sweep = 0.f;
+        SCATT_CUDA_TRY(cudaEventElapsedTime(&ms_all, ev0, ev1));
+        SCATT_CUDA_TRY(cudaEventElapsedTime(&ms_sweep, ev0, evp));
+        double rs = 0.0;
+        for (auto& pr : tm.rinv) {
+            float ms = 0.f;
+            SCATT_CUDA_TRY(cudaEventElapsedTime(&ms, pr.first, pr.second));
+            rs += ms * 1e-3;
+        }
+        stats.device_s += ms_all * 1e-3;
+        stats.sweep_s += ms_sweep * 1e-3;
+        stats.post_s += (ms_all - ms_sweep) * 1e-3;
+        stats.rinv_s += rs;
+        stats.rinv_calls += (double)tm.rinv.size();
+        stats.rinv_flops += tm.flops;
+    }
+    stats.launches += launch_counter() - launches0;
+    return SCATT_OK;
+}
+
+int check_energies(const ScanTables& t, int n, const double* E, const int* lc, const char* who) {
+    for (int e = 0; e < n; ++e) {
+        if (!(E[e] > 0.0)) {
+            set_last_error("KMatrixExtractor: energy must be > 0 for scattering");
+            return SCATT_ERR_ARG;
+        }
+        const int l = lc ? lc[e] : t.l_max;
+        if (l < 0 || l > t.l_max || std::min(l, 10) != t.l_x) {
+            set_last_error(std::string(who) + ": l_cont " + std::to_string(l) +
+                           " is outside the uploaded scan or changes the exchange cutoff min(l_cont, 10)");
+            return SCATT_ERR_ARG;
+        }
+    }
+    return SCATT_OK;
+}
+
+// Slots that fit in 85% of the free device memory at continuum cutoff l_cap
+// with `groups` phase groups (at least 1).
+int slots_that_fit(Context& ctx, const scatt_solve_opts& o, int l_cap, int groups, int* out) {
+    const ScanTables& t = *ctx.tab;
+    BatchDev b{};
+    SCATT_TRY(make_consts(t, o, b));
+    size_t freeb = 0, totb = 0;
+    SCATT_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+    const int Np = (l_cap + 1) * (l_cap + 1), Nt = Np + t.Nf;
+    const int nfit = std::min(t.Nr - 1 - 3, b.N) - b.n_s + 1;
+    const size_t per = 8 * (slot_doubles(b, Np, Nt) + post_doubles(b, Np, Nt, l_cap, nfit, t.n_occ)) +
+                       4 * slot_ints(Np, Nt);
+    const size_t fixed = 8 * group_doubles(b) * (size_t)groups + (64u << 20);
+    const size_t avail = (size_t)(0.85 * freeb) > fixed ? (size_t)(0.85 * freeb) - fixed : 0;
+    *out = (int)std::max<size_t>(1, avail / std::max<size_t>(per, 1));
+    return SCATT_OK;
+}
+
 }  // namespace
+
+int solve_batch(Context& ctx, const scatt_solve_opts& o, int n_energy, const double* E, const int* lc,
+                const scatt_outputs* out) {
+    const ScanTables& t = *ctx.tab;
+    SCATT_TRY(check_energies(t, n_energy, E, lc, "scatt_solve_batch"));
+    if (n_energy == 0) return SCATT_OK;
+    int l_cap = 0;
+    for (int e = 0; e < n_energy; ++e) l_cap = std::max(l_cap, lc ? lc[e] : t.l_max);
+    int fit = 1;
+    SCATT_TRY(slots_that_fit(ctx, o, l_cap, 1, &fit));
+    int slots = std::min(n_energy, o.max_batch > 0 ? o.max_batch : n_energy);
+    slots = std::max(1, std::min(slots, fit));
+    // lock-step batches: one phase group, refilled when the whole batch is done
+    Scan sc;
+    SCATT_TRY(scan_open(ctx, o, slots, 1, l_cap, sc));
+    for (int e = 0; e < n_energy; ++e) sc.queue.push_back(Job{E[e], lc ? lc[e] : t.l_max, e});
+    sc.submitted = n_energy;
+    ctx.stats = SolveStats{};
+    int first = SCATT_OK;
+    std::string msg;
+    for (;;) {
+        int done = 0;
+        SCATT_TRY(scan_advance(sc, out, [&](int slot, int) { return sc.job_of[slot]; }, &done, nullptr, &first, &msg));
+        if (done == 0) break;
+    }
+    if (first != SCATT_OK) set_last_error(msg);
+    return first;
+}
+
 }  // namespace scatt
 
 // ================================================================ C ABI
@@ -1848,6 +2313,11 @@ using namespace scatt;
 
 struct scatt_ctx {
     Context c;
+};
+
+struct scatt_scan {
+    scatt_ctx* ctx = nullptr;
+    Scan s;
 };
 
 extern "C" {
@@ -1866,15 +2336,16 @@ void scatt_default_opts(scatt_solve_opts* o) {
     o->timing = 0;
 }
 
-int scatt_last_stats(scatt_ctx* ctx, double* out6) {
-    if (!ctx || !out6) return SCATT_ERR_ARG;
+int scatt_last_stats(scatt_ctx* ctx, double* out7) {
+    if (!ctx || !out7) return SCATT_ERR_ARG;
     const SolveStats& st = ctx->c.stats;
-    out6[0] = st.device_s;
-    out6[1] = st.rinv_s;
-    out6[2] = st.rinv_calls;
-    out6[3] = (double)st.launches;
-    out6[4] = st.sweep_s;
-    out6[5] = st.post_s;
+    out7[0] = st.device_s;
+    out7[1] = st.rinv_s;
+    out7[2] = st.rinv_calls;
+    out7[3] = (double)st.launches;
+    out7[4] = st.sweep_s;
+    out7[5] = st.post_s;
+    out7[6] = st.rinv_flops;
     return SCATT_OK;
 }
 
@@ -1934,49 +2405,101 @@ int scatt_solve_batch(scatt_ctx* ctx, int n_energy, const double* energies, cons
     SCATT_CUDA_TRY(cudaSetDevice(ctx->c.device));
     scatt_solve_opts o;
     if (opts) o = *opts; else scatt_default_opts(&o);
+    return solve_batch(ctx->c, o, n_energy, energies, l_cont, outputs);
+}
+
+int scatt_scan_open(scatt_ctx* ctx, const scatt_solve_opts* opts, int slots, int groups, int l_cont_max,
+                    scatt_scan** out) {
+    if (!ctx || !out) return SCATT_ERR_ARG;
+    *out = nullptr;
+    if (!ctx->c.tab || !ctx->c.tab->ready) {
+        set_last_error("scatt_scan_open: call scatt_upload_static first");
+        return SCATT_ERR_STATE;
+    }
+    SCATT_CUDA_TRY(cudaSetDevice(ctx->c.device));
+    scatt_solve_opts o;
+    if (opts) o = *opts; else scatt_default_opts(&o);
     const ScanTables& t = *ctx->c.tab;
-    for (int e = 0; e < n_energy; ++e) {
-        if (!(energies[e] > 0.0)) {
-            set_last_error("KMatrixExtractor: energy must be > 0 for scattering");
-            return SCATT_ERR_ARG;
-        }
-        const int lc = l_cont ? l_cont[e] : t.l_max;
-        if (lc < 0 || lc > t.l_max || std::min(lc, 10) != t.l_x) {
-            set_last_error("scatt_solve_batch: l_cont " + std::to_string(lc) +
-                           " is outside the uploaded scan or changes the exchange cutoff min(l_cont, 10)");
-            return SCATT_ERR_ARG;
-        }
+    const int l_cap = l_cont_max < 0 ? t.l_max : l_cont_max;
+    if (l_cap > t.l_max || std::min(l_cap, 10) != t.l_x) {
+        set_last_error("scatt_scan_open: l_cont_max is outside the uploaded scan");
+        return SCATT_ERR_ARG;
     }
-    // batch size: as many energies as fit in 85% of free device memory
-    size_t freeb = 0, totb = 0;
-    SCATT_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
-    int bmax = o.max_batch > 0 ? o.max_batch : n_energy;
-    {
-        Batch probe;
-        if (make_shared(t, o, probe) == SCATT_OK) {
-            const int nslots = probe.b.N - probe.b.n_s + 1;
-            const int Np = t.Np_max, Nt = Np + t.Nf;
-            const size_t per = energy_bytes(probe.b, Np, Nt, nslots) + 40 * (size_t)Np * Np * 8 +
-                               4 * (size_t)Nt * Np * 8;
-            const int fit = (int)std::max<size_t>(1, (size_t)(0.85 * freeb) / std::max<size_t>(per, 1));
-            bmax = std::min(bmax, fit);
-        }
+    if (groups < 1 || groups > MAX_GROUPS) {
+        set_last_error("scatt_scan_open: groups must be in [1, " + std::to_string(MAX_GROUPS) + "]");
+        return SCATT_ERR_ARG;
     }
-    bmax = std::max(1, bmax);
+    if (slots <= 0) SCATT_TRY(slots_that_fit(ctx->c, o, l_cap, groups, &slots));
+    if (groups > slots) groups = slots;
+    auto* h = new scatt_scan();
+    h->ctx = ctx;
+    const int st = scan_open(ctx->c, o, slots, groups, l_cap, h->s);
+    if (st != SCATT_OK) {
+        delete h;
+        return st;
+    }
     ctx->c.stats = SolveStats{};
-    int first_err = SCATT_OK;
-    std::string first_msg;
-    for (int e0 = 0; e0 < n_energy; e0 += bmax) {
-        const int cnt = std::min(bmax, n_energy - e0);
-        const int st = run_batch(ctx->c, o, cnt, energies + e0, l_cont ? l_cont + e0 : nullptr, outputs, e0);
-        if (st != SCATT_OK && first_err == SCATT_OK) {
-            first_err = st;
-            first_msg = scatt_last_error();
-            if (st == SCATT_ERR_CUDA || st == SCATT_ERR_OOM || st == SCATT_ERR_ARG || st == SCATT_ERR_FIT_WINDOW) break;
+    *out = h;
+    return SCATT_OK;
+}
+
+int scatt_scan_submit(scatt_scan* sc, int n, const double* energies, const int* l_cont) {
+    if (!sc || n < 0 || (n > 0 && !energies)) return SCATT_ERR_ARG;
+    const ScanTables& t = *sc->ctx->c.tab;
+    SCATT_TRY(check_energies(t, n, energies, l_cont, "scatt_scan_submit"));
+    for (int e = 0; e < n; ++e)
+        if ((l_cont ? l_cont[e] : sc->s.l_cap) > sc->s.l_cap) {
+            set_last_error("scatt_scan_submit: l_cont above the scan's l_cont_max");
+            return SCATT_ERR_ARG;
         }
+    for (int e = 0; e < n; ++e)
+        sc->s.queue.push_back(Job{energies[e], l_cont ? l_cont[e] : sc->s.l_cap, sc->s.submitted++});
+    return SCATT_OK;
+}
+
+int scatt_scan_step(scatt_scan* sc, const scatt_outputs* outputs, int capacity, int* n_done,
+                    long long* index_out) {
+    if (!sc || !outputs || !n_done) return SCATT_ERR_ARG;
+    *n_done = 0;
+    if (capacity < sc->s.slots) {
+        set_last_error("scatt_scan_step: output capacity below the scan's slot count");
+        return SCATT_ERR_ARG;
     }
-    if (first_err != SCATT_OK) set_last_error(first_msg);
-    return first_err;
+    SCATT_CUDA_TRY(cudaSetDevice(sc->ctx->c.device));
+    int first = SCATT_OK;
+    std::string msg;
+    std::vector<long> jobs;
+    SCATT_TRY(scan_advance(sc->s, outputs, [](int, int i) { return (long)i; }, n_done, &jobs, &first, &msg));
+    if (index_out)
+        for (size_t i = 0; i < jobs.size(); ++i) index_out[i] = jobs[i];
+    if (first != SCATT_OK) set_last_error(msg);
+    return first;
+}
+
+int scatt_scan_pending(scatt_scan* sc, int* queued, int* in_flight) {
+    if (!sc) return SCATT_ERR_ARG;
+    if (queued) *queued = (int)sc->s.queue.size();
+    if (in_flight) {
+        int f = 0;
+        for (auto& d : sc->s.ed) f += d.live;
+        *in_flight = f;
+    }
+    return SCATT_OK;
+}
+
+int scatt_scan_shape(scatt_scan* sc, int* slots, int* groups) {
+    if (!sc) return SCATT_ERR_ARG;
+    if (slots) *slots = sc->s.slots;
+    if (groups) *groups = sc->s.G;
+    return SCATT_OK;
+}
+
+int scatt_scan_close(scatt_scan* sc) {
+    if (!sc) return SCATT_OK;
+    cudaSetDevice(sc->ctx->c.device);
+    cudaStreamSynchronize(sc->ctx->c.stream);
+    delete sc;
+    return SCATT_OK;
 }
 
 }  // extern "C"

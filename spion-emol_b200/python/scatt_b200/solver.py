@@ -6,6 +6,10 @@ uploaded once (scatt_upload_static), then any number of energies are solved
 (scatt_solve_batch).  Results come back as numpy arrays named after the
 reference's result structs (ScatteringResult, AmplitudeResult,
 DipoleResult).
+
+``Scan`` (ScanSolver.scan) is the streaming form of the same solve: energies
+are queued, run in phase-staggered slot groups, and come back as each group
+finishes (scatt_scan_open / submit / step / close).
 """
 from __future__ import annotations
 
@@ -63,6 +67,13 @@ def _bind():
     L.scatt_default_opts.argtypes = [C.POINTER(SolveOpts)]
     L.scatt_default_opts.restype = None
     L.scatt_last_stats.argtypes = [C.c_void_p, dptr]
+    L.scatt_scan_open.argtypes = [C.c_void_p, C.POINTER(SolveOpts), C.c_int, C.c_int, C.c_int,
+                                  C.POINTER(C.c_void_p)]
+    L.scatt_scan_submit.argtypes = [C.c_void_p, C.c_int, dptr, iptr]
+    L.scatt_scan_step.argtypes = [C.c_void_p, C.POINTER(Outputs), C.c_int, iptr, C.POINTER(C.c_longlong)]
+    L.scatt_scan_pending.argtypes = [C.c_void_p, iptr, iptr]
+    L.scatt_scan_shape.argtypes = [C.c_void_p, iptr, iptr]
+    L.scatt_scan_close.argtypes = [C.c_void_p]
     _bound = True
 
 
@@ -122,11 +133,14 @@ class ScanSolver:
         d.alpha_pol, d.pol_form, d.r_c = inp.alpha_pol, inp.pol_form, inp.r_c
         d.n_transition = n_transition
         d.chi_cutoff = 1e-15
+        self._upload(d)
+
+    def _upload(self, d):
         check(lib().scatt_upload_static(self._ctx, C.byref(d)))
         info = np.zeros(5, dtype=np.int32)
         check(lib().scatt_scan_info(self._ctx, info.ctypes.data_as(iptr)))
         self.n_transition, self.Np, self.Nf, self.n_lambda, self.n_sigma = (int(x) for x in info)
-        self.n_occ = inp.n_occ
+        self.n_occ = d.n_occ
 
     def close(self):
         if self._ctx:
@@ -140,49 +154,141 @@ class ScanSolver:
             pass
 
     def last_stats(self) -> dict:
-        """Device timing of the last solve (needs opts.timing = 1)."""
-        v = np.zeros(6)
+        """Device timing of the last solve, or of the open scan's steps so far
+        (needs opts.timing = 1)."""
+        v = np.zeros(7)
         check(lib().scatt_last_stats(self._ctx, as_dptr(v)))
         return {"device_s": v[0], "rinv_s": v[1], "rinv_calls": int(v[2]), "launches": int(v[3]),
-                "sweep_s": v[4], "post_s": v[5]}
+                "sweep_s": v[4], "post_s": v[5], "rinv_flops": v[6]}
 
     def solve(self, energies, l_cont=None, opts: SolveOpts | None = None, raise_on_error=True):
         E = np.ascontiguousarray(energies, dtype=np.float64).reshape(-1)
         nE = E.size
-        Np, no = self.Np, self.n_occ
         lc = None
         if l_cont is not None:
             lc = np.ascontiguousarray(np.broadcast_to(np.asarray(l_cont, dtype=np.int32), (nE,)))
-        arr = {
-            "K_kme": np.zeros((nE, Np, Np)), "A": np.zeros((nE, Np, Np)), "B": np.zeros((nE, Np, Np)),
-            "K_aa": np.zeros((nE, Np, Np)), "b_overlap": np.zeros((nE, no, Np)),
-            "D_re": np.zeros((nE, 6, Np)), "D_im": np.zeros((nE, 6, Np)), "Draw_re": np.zeros((nE, 6, Np)),
-            "Draw_im": np.zeros((nE, 6, Np)), "d_raw": np.zeros((nE, 6, Np)), "d_corr": np.zeros((nE, 6, no)),
-            "partial_sigma": np.zeros((nE, 6)), "eig_kme": np.zeros((nE, Np)), "eig_aa": np.zeros((nE, Np)),
-            "diag": np.zeros((nE, NDIAG)),
-        }
-        status = np.zeros(nE, dtype=np.int32)
-        out = Outputs()
-        for k, v in arr.items():
-            setattr(out, k, as_dptr(v))
-        out.status = status.ctypes.data_as(iptr)
+        arr, status, out = output_arrays(nE, self.Np, self.n_occ)
         o = opts if opts is not None else default_opts()
         code = lib().scatt_solve_batch(self._ctx, nE, as_dptr(E),
                                        lc.ctypes.data_as(iptr) if lc is not None else None,
                                        C.byref(o), C.byref(out))
         if code != 0 and raise_on_error:
             check(code)
-        res = []
-        for e in range(nE):
-            n = (int(lc[e]) + 1) ** 2 if lc is not None else Np
-            # matrices come back column-major: transpose the C-order view
-            mat = lambda a: a[e].T[:n, :n]
-            res.append(EnergyResult(
-                E=float(E[e]), K_kme=mat(arr["K_kme"]), A=mat(arr["A"]), B=mat(arr["B"]),
-                K_aa=mat(arr["K_aa"]), b_overlap=arr["b_overlap"][e].T[:n, :],
-                D=(arr["D_re"][e] + 1j * arr["D_im"][e])[:, :n],
-                D_raw=(arr["Draw_re"][e] + 1j * arr["Draw_im"][e])[:, :n],
-                d_raw=arr["d_raw"][e][:, :n], d_corr=arr["d_corr"][e], partial_sigma=arr["partial_sigma"][e],
-                eig_kme=arr["eig_kme"][e][:n], eig_aa=arr["eig_aa"][e][:n],
-                diag={k: arr["diag"][e][i] for i, k in enumerate(DIAG)}, status=int(status[e])))
-        return res
+        return [result_of(arr, status, e, float(E[e]), int(lc[e]) if lc is not None else None, self.Np)
+                for e in range(nE)]
+
+    def scan(self, slots: int = 0, groups: int = 1, l_cont_max: int | None = None,
+             opts: SolveOpts | None = None, alloc=None) -> "Scan":
+        """A streaming scan over this solver's static inputs (see Scan)."""
+        return Scan(self, slots, groups, l_cont_max, opts, alloc)
+
+
+def output_arrays(nE, Np, no, alloc=None):
+    """Host output arrays for nE energies and the scatt_outputs pointing at
+    them; alloc(shape, dtype) may supply the memory (e.g. pinned)."""
+    mk = alloc or (lambda shape, dtype=np.float64: np.zeros(shape, dtype=dtype))
+    arr = {
+        "K_kme": mk((nE, Np, Np)), "A": mk((nE, Np, Np)), "B": mk((nE, Np, Np)),
+        "K_aa": mk((nE, Np, Np)), "b_overlap": mk((nE, no, Np)),
+        "D_re": mk((nE, 6, Np)), "D_im": mk((nE, 6, Np)), "Draw_re": mk((nE, 6, Np)),
+        "Draw_im": mk((nE, 6, Np)), "d_raw": mk((nE, 6, Np)), "d_corr": mk((nE, 6, no)),
+        "partial_sigma": mk((nE, 6)), "eig_kme": mk((nE, Np)), "eig_aa": mk((nE, Np)),
+        "diag": mk((nE, NDIAG)),
+    }
+    status = mk((nE,), np.int32)
+    out = Outputs()
+    for k, v in arr.items():
+        setattr(out, k, as_dptr(v))
+    out.status = status.ctypes.data_as(iptr)
+    return arr, status, out
+
+
+def output_bytes(arr, status, rows: int) -> int:
+    """Bytes of `rows` energies' outputs (what a device-to-host read moves)."""
+    return int(sum(v[:rows].nbytes for v in arr.values()) + status[:rows].nbytes)
+
+
+def result_of(arr, status, e, E, l_cont, Np) -> EnergyResult:
+    n = (l_cont + 1) ** 2 if l_cont is not None else Np
+    # matrices come back column-major: transpose the C-order view (copies, so
+    # a result outlives the buffer's next use)
+    mat = lambda a: np.array(a[e].T[:n, :n])
+    return EnergyResult(
+        E=E, K_kme=mat(arr["K_kme"]), A=mat(arr["A"]), B=mat(arr["B"]),
+        K_aa=mat(arr["K_aa"]), b_overlap=np.array(arr["b_overlap"][e].T[:n, :]),
+        D=(arr["D_re"][e] + 1j * arr["D_im"][e])[:, :n],
+        D_raw=(arr["Draw_re"][e] + 1j * arr["Draw_im"][e])[:, :n],
+        d_raw=np.array(arr["d_raw"][e][:, :n]), d_corr=np.array(arr["d_corr"][e]),
+        partial_sigma=np.array(arr["partial_sigma"][e]),
+        eig_kme=np.array(arr["eig_kme"][e][:n]), eig_aa=np.array(arr["eig_aa"][e][:n]),
+        diag={k: float(arr["diag"][e][i]) for i, k in enumerate(DIAG)}, status=int(status[e]))
+
+
+class Scan:
+    """Streaming scan (scatt_scan_*): energies wait in a queue and run in
+    `slots` device slots split into `groups` phase groups.  The groups start
+    staggered by a fraction of the radial sweep, so once the conveyor is full
+    a group finishes every 1/groups of a sweep and its slots take the next
+    queued energies; every slot stays busy while the queue lasts.
+    groups = 1 is the lock-step batch of ScanSolver.solve."""
+
+    def __init__(self, solver: ScanSolver, slots=0, groups=1, l_cont_max=None, opts=None, alloc=None):
+        _bind()
+        self.solver = solver
+        self._h = C.c_void_p()
+        self.l_cont_max = solver.l_cont_max if l_cont_max is None else l_cont_max
+        o = opts if opts is not None else default_opts()
+        check(lib().scatt_scan_open(solver._ctx, C.byref(o), int(slots), int(groups), int(self.l_cont_max),
+                                    C.byref(self._h)))
+        sl, gr = C.c_int(0), C.c_int(0)
+        check(lib().scatt_scan_shape(self._h, C.byref(sl), C.byref(gr)))
+        self.slots, self.groups = sl.value, gr.value
+        self.arr, self.status, self._out = output_arrays(self.slots, solver.Np, solver.n_occ, alloc)
+        self._idx = np.zeros(self.slots, dtype=np.int64)
+        self._E, self._lc = [], []
+        self.last_out_bytes = 0
+
+    def submit(self, energies, l_cont=None):
+        """Queue energies; returns their submission indices."""
+        E = np.ascontiguousarray(energies, dtype=np.float64).reshape(-1)
+        lc = None
+        if l_cont is not None:
+            lc = np.ascontiguousarray(np.broadcast_to(np.asarray(l_cont, dtype=np.int32), (E.size,)))
+        check(lib().scatt_scan_submit(self._h, E.size, as_dptr(E),
+                                      lc.ctypes.data_as(iptr) if lc is not None else None))
+        first = len(self._E)
+        self._E += [float(x) for x in E]
+        self._lc += [int(x) for x in lc] if lc is not None else [None] * E.size
+        return list(range(first, first + E.size))
+
+    def step(self, raise_on_error=True, results=True):
+        """Advance until the next group finishes; [(submission index, EnergyResult)]
+        (an empty list once nothing is queued or in flight).  results=False
+        returns the indices only and leaves the outputs in self.arr."""
+        n = C.c_int(0)
+        code = lib().scatt_scan_step(self._h, C.byref(self._out), self.slots, C.byref(n),
+                                     self._idx.ctypes.data_as(C.POINTER(C.c_longlong)))
+        if code != 0 and raise_on_error:
+            check(code)
+        self.last_out_bytes = output_bytes(self.arr, self.status, n.value)
+        idx = [int(self._idx[i]) for i in range(n.value)]
+        if not results:
+            return idx
+        return [(j, result_of(self.arr, self.status, i, self._E[j], self._lc[j], self.solver.Np))
+                for i, j in enumerate(idx)]
+
+    def pending(self):
+        q, f = C.c_int(0), C.c_int(0)
+        check(lib().scatt_scan_pending(self._h, C.byref(q), C.byref(f)))
+        return q.value, f.value
+
+    def close(self):
+        if self._h:
+            lib().scatt_scan_close(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

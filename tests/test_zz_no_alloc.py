@@ -33,6 +33,27 @@ def test_noalloc_matches_allocating_inverse_two_calls():
             assert np.max(np.abs(got[b] @ A[b] - np.eye(A.shape[1]))) < 1e-10
 
 
+@pytest.mark.parametrize("n,count,scheme", [(1046, 2, 0), (200, 3, 3)])
+def test_noalloc_row_contiguous_scheme_two_calls(n, count, scheme):
+    """Orders above 512 (or scheme 3 forced) run the row-contiguous inverse
+    without look-ahead, over several 64-column windows; order 1046 with two
+    matrices needs about 55 MB of the 64 MiB array."""
+    rng = np.random.default_rng(n)
+    M = rng.standard_normal((count, n, n))
+    A = M + np.transpose(M, (0, 2, 1)) + 2.0 * np.sqrt(n) * np.eye(n)
+    _lib.set_inverse_blocking(scheme)
+    try:
+        ref, st_ref = _lib.inverse_batched(A, symmetrize=True)
+        for _ in range(2):
+            got, st = _lib.inverse_batched(A, symmetrize=True, noalloc=True)
+            assert np.all(st == 0) and np.all(st_ref == 0)
+            for b in range(count):
+                assert _rel(got[b], ref[b]) < 1e-12
+                assert np.max(np.abs(got[b] @ A[b] - np.eye(n))) < 1e-9
+    finally:
+        _lib.set_inverse_blocking(0)
+
+
 def test_noalloc_reports_singular_like_allocating():
     A = np.ones((2, 6, 6))
     code = _lib.lib().scatt_inverse_batched_noalloc
