@@ -201,7 +201,7 @@ def main():
     ap.add_argument("--slots", type=int, default=0)
     ap.add_argument("--groups", type=int, default=0)
     ap.add_argument("--graphs", type=int, default=-1, help="replay chunks from CUDA graphs (default: per config)")
-    ap.add_argument("--autotune", type=int, default=0,
+    ap.add_argument("--autotune", type=int, default=1,
                     help="time the inverse's blockings for the workload's orders before the run")
     ap.add_argument("--cpu-budget", type=float, default=20.0,
                     help="seconds of oracle work per CPU sample (the reference arm takes one per step)")
@@ -266,9 +266,10 @@ def main():
 
     tuned = []
     if a.autotune:
-        Nt = sol.Np + sol.Nf
-        for n in sorted({Nt, sol.Np}):
-            tuned.append(_lib.autotune_inverse(n, slots, device=local))
+        # the scan's batches: R^-1 of order N_t over the slots, and the Schur
+        # inverses of order Np over the slots' 8 radial steps of a chunk
+        for n, count in sorted({(sol.Np + sol.Nf, slots), (sol.Np, slots * 8)}):
+            tuned.append(_lib.autotune_inverse(n, count, device=local))
     peak = cuda_dgemm_peak(torch) if rank == 0 else None
     alloc, _keep = pinned_alloc(torch)
     opts = S.default_opts(allow_closed_channels=1, timing=1, use_graphs=graphs)

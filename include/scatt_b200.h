@@ -104,6 +104,19 @@ int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call);
  * applies from the next inverse on, also in solves running on other threads. */
 int scatt_set_inverse_blocking(int scheme);
 
+/* Autotuner of the two-level inverses: times scheme 2 and scheme 3 (with and
+ * without look-ahead) with every panel shape that holds order n, on a batch
+ * of `count` seeded matrices of order n (reps timed calls each), and keeps
+ * the fastest for (current device, n, count).  Under the automatic scheme
+ * (scatt_set_inverse_blocking(0)) every later inverse of exactly that order
+ * and batch on that device -- the solver's Schur and R^-1 batches included
+ * -- uses the kept choice.  Outputs (each may be NULL): the scheme (2 or 3),
+ * the panel shape (0..4: 1x8, 2x8, 3x8, 3x12, 5x8 rows per thread x warps),
+ * look-ahead (0/1) and the chosen configuration's milliseconds per call.
+ * Orders 1..1280.  No counterpart in the reference. */
+int scatt_autotune_inverse(int n, int count, int reps, int* scheme, int* panel, int* look_ahead,
+                           double* best_ms);
+
 /* ------------------------------------------- per-step compatibility seam
  * The reference's per-radial-step device interface (GpuForwardStepper,
  * GpuSinvStepper, GpuBackStepper in src/scatt/GpuPropagate.hpp:83-279),

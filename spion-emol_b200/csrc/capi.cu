@@ -52,6 +52,75 @@ __global__ void fill_test_matrices(double* A, int n, int count, unsigned seed) {
 
 using namespace scatt;
 
+namespace {
+
+// Seeded test matrices (uniform entries in [-0.5, 0.5) plus 2 on the
+// diagonal) and their inverse entries (panel windows sized for the
+// look-ahead), for timing the inverse's kernels alone.
+struct InverseBench {
+    int n = 0, count = 0;
+    DevBuf<double> dA, dW, dO, dS, dP;
+    DevBuf<int> dsig, drid, dst, dsg;
+    DevBuf<GjEntry> dent;
+
+    int setup(int n_, int count_) {
+        n = n_;
+        count = count_;
+        const size_t nn = (size_t)n * n;
+        SCATT_TRY(dP.alloc((size_t)4 * n * 64 * count));
+        SCATT_TRY(dsg.alloc((size_t)4 * n * count));
+        SCATT_TRY(dA.alloc(nn * count));
+        SCATT_TRY(dS.alloc(nn * count));
+        SCATT_TRY(dW.alloc(nn * count));
+        SCATT_TRY(dO.alloc(nn * count));
+        SCATT_TRY(dsig.alloc((size_t)n * count));
+        SCATT_TRY(drid.alloc((size_t)n * count));
+        SCATT_TRY(dst.alloc(2 * (size_t)count));
+        fill_test_matrices<<<1024, 256>>>(dS.p, n, count, 12345u);
+        SCATT_CUDA_TRY(cudaGetLastError());
+        std::vector<GjEntry> ent(count);
+        for (int b = 0; b < count; ++b)
+            ent[b] = GjEntry{dA.p + nn * b, dW.p + nn * b, dO.p + nn * b, dsig.p + (size_t)n * b,
+                             drid.p + (size_t)n * b, dst.p + 2 * b, n, n, n,
+                             dP.p + (size_t)4 * n * 64 * b, dsg.p + (size_t)4 * n * b};
+        return dent.upload(ent);
+    }
+
+    // mean milliseconds of run() over reps calls after one untimed call; the
+    // input is restored before each call, outside the timed span
+    template <class F>
+    int time(int reps, double* ms_out, F run) {
+        const size_t bytes = (size_t)n * n * count * sizeof(double);
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        SCATT_CUDA_TRY(cudaEventCreate(&e0));
+        if (cudaEventCreate(&e1) != cudaSuccess) {
+            cudaEventDestroy(e0);
+            return cuda_status(cudaErrorMemoryAllocation, "cudaEventCreate");
+        }
+        double total = 0.0;
+        int st = SCATT_OK;
+        for (int r = 0; r < reps + 1 && st == SCATT_OK; ++r) {
+            cudaError_t ce = cudaMemcpyAsync(dA.p, dS.p, bytes, cudaMemcpyDeviceToDevice, 0);
+            if (ce == cudaSuccess) ce = cudaEventRecord(e0, 0);
+            if (ce != cudaSuccess) { st = cuda_status(ce, "inverse timing"); break; }
+            st = run();
+            if (st != SCATT_OK) break;
+            ce = cudaEventRecord(e1, 0);
+            if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+            if (ce != cudaSuccess) { st = cuda_status(ce, "inverse timing"); break; }
+            if (r > 0) total += ms;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (st == SCATT_OK) *ms_out = total / reps;
+        return st;
+    }
+};
+
+}  // namespace
+
 extern "C" {
 
 const char* scatt_version(void) { return "spion-emol_b200 0.1 (sm_100a, FP64 DMMA)"; }
@@ -169,43 +238,45 @@ int scatt_set_inverse_blocking(int scheme) {
 int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call) {
     if (n <= 0 || count <= 0 || reps <= 0 || !ms_per_call) return SCATT_ERR_ARG;
     SCATT_TRY(require_device());
-    const size_t nn = (size_t)n * n;
-    DevBuf<double> dA, dW, dO, dS, dP;
-    DevBuf<int> dsig, drid, dst, dsg;
-    SCATT_TRY(dP.alloc((size_t)4 * n * 64 * count));
-    SCATT_TRY(dsg.alloc((size_t)4 * n * count));
-    SCATT_TRY(dA.alloc(nn * count));
-    SCATT_TRY(dS.alloc(nn * count));
-    SCATT_TRY(dW.alloc(nn * count));
-    SCATT_TRY(dO.alloc(nn * count));
-    SCATT_TRY(dsig.alloc((size_t)n * count));
-    SCATT_TRY(drid.alloc((size_t)n * count));
-    SCATT_TRY(dst.alloc(2 * (size_t)count));
-    fill_test_matrices<<<1024, 256>>>(dS.p, n, count, 12345u);
-    std::vector<GjEntry> ent(count);
-    for (int b = 0; b < count; ++b)
-        ent[b] = GjEntry{dA.p + nn * b, dW.p + nn * b, dO.p + nn * b, dsig.p + (size_t)n * b,
-                         drid.p + (size_t)n * b, dst.p + 2 * b, n, n, n,
-                         dP.p + (size_t)4 * n * 64 * b, dsg.p + (size_t)4 * n * b};
-    DevBuf<GjEntry> dent;
-    SCATT_TRY(dent.upload(ent));
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    float total = 0.f;
-    for (int r = 0; r < reps + 1; ++r) {
-        SCATT_CUDA_TRY(cudaMemcpyAsync(dA.p, dS.p, nn * count * sizeof(double), cudaMemcpyDeviceToDevice));
-        cudaEventRecord(e0);
-        SCATT_TRY(gj_inverse_selected(dent.p, count, n, true, 0, true));
-        cudaEventRecord(e1);
-        SCATT_CUDA_TRY(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (r > 0) total += ms;
+    InverseBench bench;
+    SCATT_TRY(bench.setup(n, count));
+    return bench.time(reps, ms_per_call, [&]() { return gj_inverse_selected(bench.dent.p, count, n, true, 0, true); });
+}
+
+int scatt_autotune_inverse(int n, int count, int reps, int* scheme, int* panel, int* look_ahead, double* best_ms) {
+    if (n <= 0 || n > 1280 || count <= 0 || reps <= 0) {
+        set_last_error("scatt_autotune_inverse: order must be in [1, 1280], batch and reps positive");
+        return SCATT_ERR_ARG;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    *ms_per_call = total / reps;
+    SCATT_TRY(require_device());
+    int dev = 0;
+    SCATT_CUDA_TRY(cudaGetDevice(&dev));
+    InverseBench bench;
+    SCATT_TRY(bench.setup(n, count));
+    InverseTune best;
+    double best_t = 1e300;
+    for (int sch = 2; sch <= 3; ++sch)
+        for (int p = 0; p < GJ_PANEL_SHAPES; ++p) {
+            if (n > gj_panel_capacity(p)) continue;
+            for (int la = 0; la <= (sch == 3 ? 1 : 0); ++la) {
+                double ms = 0.0;
+                SCATT_TRY(bench.time(reps, &ms, [&]() {
+                    return sch == 3 ? gj_inverse_batched3(bench.dent.p, count, n, true, 0, la != 0, p)
+                                    : gj_inverse_batched2(bench.dent.p, count, n, true, 0, p);
+                }));
+                if (ms < best_t) {
+                    best_t = ms;
+                    best.scheme = sch;
+                    best.pcfg = p;
+                    best.look_ahead = la;
+                }
+            }
+        }
+    inverse_tune_store(dev, n, count, best);
+    if (scheme) *scheme = best.scheme;
+    if (panel) *panel = best.pcfg;
+    if (look_ahead) *look_ahead = best.look_ahead;
+    if (best_ms) *best_ms = best_t;
     return SCATT_OK;
 }
 

@@ -105,8 +105,9 @@ int gj_inverse_batched(const GjEntry* entries_dev, int count, int nmax,
 
 // Two-level blocked variant (64-column windows, rank-64 trailing updates) for
 // n <= 1280; every entry must carry P (2 x ld x 64 doubles) and sigt (2 n ints).
+// pcfg >= 0 forces the panel shape (see gj_panel_capacity).
 int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax,
-                        bool symmetrize, cudaStream_t stream);
+                        bool symmetrize, cudaStream_t stream, int pcfg = -1);
 
 // Two-level variant on the row-contiguous view: the column-major buffer of A
 // is treated as the row-major B = A^T (inv(A) = inv(B)^T), so pivot rows and
@@ -117,7 +118,26 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax,
 // then every entry needs P of 4 x ld x 64 doubles and sigt of 4 n ints
 // (without it, 2 x ld x 64 and 2 n as for gj_inverse_batched2).
 int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax,
-                        bool symmetrize, cudaStream_t stream, bool look_ahead);
+                        bool symmetrize, cudaStream_t stream, bool look_ahead, int pcfg = -1);
+
+// Panel shapes of the two-level inverses, as rows per thread x warps: 1x8,
+// 2x8, 3x8, 3x12, 5x8.  Shape p factors panels of up to gj_panel_capacity(p)
+// rows; the default is the smallest shape that holds the order.
+constexpr int GJ_PANEL_SHAPES = 5;
+inline int gj_panel_capacity(int pcfg) {
+    constexpr int cap[GJ_PANEL_SHAPES] = {256, 512, 768, 1152, 1280};
+    return cap[pcfg];
+}
+
+// A measured choice of scheme (2 or 3), panel shape and look-ahead for one
+// (device, order, batch).  The autotuner (scatt_autotune_inverse) stores
+// them; the automatic scheme uses a stored choice for an exact match of the
+// current device, order and batch, and its fixed rule otherwise.
+struct InverseTune {
+    int scheme = 0, pcfg = -1, look_ahead = 1;
+};
+bool inverse_tune_lookup(int n, int count, InverseTune* out);
+void inverse_tune_store(int device, int n, int count, const InverseTune& t);
 
 // Scheme of every dense inverse (entry points and solver): 0 = automatic
 // (row-contiguous two-level above order 512, where its contiguous pivot-row
@@ -135,9 +155,17 @@ inline int gj_inverse_selected(const GjEntry* entries_dev, int count, int nmax,
         case 1: return gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream);
         case 2: return gj_inverse_batched2(entries_dev, count, nmax, symmetrize, stream);
         case 3: return gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream, look_ahead);
-        default:
+        default: {
+            InverseTune t;
+            if (inverse_tune_lookup(nmax, count, &t)) {
+                if (t.scheme == 3)
+                    return gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream,
+                                               look_ahead && t.look_ahead, t.pcfg);
+                return gj_inverse_batched2(entries_dev, count, nmax, symmetrize, stream, t.pcfg);
+            }
             return nmax > 512 ? gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream, look_ahead)
                               : gj_inverse_batched2(entries_dev, count, nmax, symmetrize, stream);
+        }
     }
 }
 

@@ -30,7 +30,10 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <mutex>
+#include <string>
+#include <tuple>
 
 namespace scatt {
 
@@ -1348,12 +1351,28 @@ int look_ahead_resources(LookAhead** out) {
 }
 
 // panel shape (rows per thread x warps): 1x8 (n <= 256), 2x8 (<= 512),
-// 3x8 (<= 768), 3x12 (<= 1152), 5x8 (<= 1280)
-void panel_shape(int nmax, int& pcfg, int& pt) {
-    pcfg = nmax <= 256 ? 0 : nmax <= 512 ? 1 : nmax <= 768 ? 2 : nmax <= 1152 ? 3 : 4;
+// 3x8 (<= 768), 3x12 (<= 1152), 5x8 (<= 1280); `force` (>= 0) picks one
+// that holds nmax.  pt = the threads of the launch: ceil(nmax / rows) rounded
+// up to whole warps, at most the shape's warps since nmax <= its capacity.
+int panel_shape(int nmax, int& pcfg, int& pt, int force = -1) {
+    if (force >= 0) {
+        if (force >= GJ_PANEL_SHAPES || nmax > gj_panel_capacity(force)) {
+            set_last_error("inverse: panel shape " + std::to_string(force) + " does not hold order " +
+                           std::to_string(nmax));
+            return SCATT_ERR_ARG;
+        }
+        pcfg = force;
+    } else {
+        pcfg = nmax <= 256 ? 0 : nmax <= 512 ? 1 : nmax <= 768 ? 2 : nmax <= 1152 ? 3 : 4;
+    }
     const int prows = pcfg == 0 ? 1 : pcfg == 1 ? 2 : pcfg <= 3 ? 3 : 5;
     pt = 32 * (((nmax + prows - 1) / prows + 31) / 32);
+    return SCATT_OK;
 }
+
+// autotuned choices, keyed by (device, order, batch)
+std::mutex g_tune_mutex;
+std::map<std::tuple<int, int, int>, InverseTune> g_tune;
 
 // Kernel attributes are per device: one flag bit per device and scheme.
 std::mutex g_attr_mutex;
@@ -1429,8 +1448,24 @@ int gj_inverse_batched(const GjEntry* entries_dev, int count, int nmax,
     return SCATT_OK;
 }
 
+bool inverse_tune_lookup(int n, int count, InverseTune* out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    if (g_tune.empty()) return false;
+    const auto it = g_tune.find(std::make_tuple(dev, n, count));
+    if (it == g_tune.end()) return false;
+    *out = it->second;
+    return true;
+}
+
+void inverse_tune_store(int device, int n, int count, const InverseTune& t) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune[std::make_tuple(device, n, count)] = t;
+}
+
 int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax, bool symmetrize,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, int force_pcfg) {
     if (count <= 0 || nmax <= 0) return SCATT_OK;
     if (nmax > 1280) return gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream);
     SCATT_TRY(once_per_device(1, [&]() -> int {
@@ -1441,7 +1476,7 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax, bool sy
     const int outer = (nmax + OB - 1) / OB;
     const int tiles = (nmax + 63) / 64;
     int pcfg, pt;
-    panel_shape(nmax, pcfg, pt);
+    SCATT_TRY(panel_shape(nmax, pcfg, pt, force_pcfg));
     const size_t lab_smem = 2 * (size_t)nmax * sizeof(int);
     int launches = 0;
     for (int K = 0; K < outer; ++K) {
@@ -1461,7 +1496,7 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax, bool sy
 }
 
 int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax, bool symmetrize,
-                        cudaStream_t stream, bool look_ahead) {
+                        cudaStream_t stream, bool look_ahead, int force_pcfg) {
     if (count <= 0 || nmax <= 0) return SCATT_OK;
     if (nmax > 1280) return gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream);
     SCATT_TRY(once_per_device(2, [&]() -> int {
@@ -1475,7 +1510,7 @@ int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax, bool sy
     const int tiles = (nmax + 63) / 64;
     const int mtiles = (nmax + T3M - 1) / T3M;
     int pcfg, pt;
-    panel_shape(nmax, pcfg, pt);
+    SCATT_TRY(panel_shape(nmax, pcfg, pt, force_pcfg));
     const size_t lab_smem = 2 * (size_t)nmax * sizeof(int);
     int launches = 0;
     auto chain = [&](int K, cudaStream_t st, int la) -> int {

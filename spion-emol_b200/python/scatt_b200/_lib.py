@@ -126,6 +126,21 @@ def bench_inverse(n: int, count: int, reps: int = 5) -> float:
     return ms.value
 
 
+def autotune_inverse(n: int, count: int, reps: int = 3, device: int | None = None) -> dict:
+    """Time the two-level inverse's configurations for order n and batch
+    `count` on the current (or given) device and keep the fastest for every
+    later inverse of that order and batch (scatt_autotune_inverse)."""
+    if device is not None:
+        import torch
+        torch.cuda.set_device(device)
+    sc, pc, la = C.c_int(0), C.c_int(0), C.c_int(0)
+    ms = C.c_double(0.0)
+    check(lib().scatt_autotune_inverse(int(n), int(count), int(reps), C.byref(sc), C.byref(pc), C.byref(la),
+                                       C.byref(ms)))
+    return {"n": int(n), "count": int(count), "scheme": sc.value, "panel": pc.value,
+            "look_ahead": la.value, "ms": ms.value}
+
+
 def set_inverse_blocking(scheme: int):
     """0: automatic (default); 1: single-level; 2: two-level column-major;
     3: two-level row-contiguous."""

@@ -76,3 +76,20 @@ def test_inverse_every_scheme(scheme, n):
     for b in range(2):
         ref = np.linalg.inv(A[b])
         assert np.max(np.abs(inv[b] - ref)) / np.max(np.abs(ref)) < 1e-12
+
+
+@pytest.mark.parametrize("n,count", [(300, 4), (700, 3)])
+def test_autotuned_inverse_is_kept_and_exact(n, count):
+    """The autotuner keeps a valid configuration for (order, batch); inverses
+    of exactly that order and batch then run it and still equal numpy's."""
+    t = _lib.autotune_inverse(n, count, reps=1)
+    assert t["scheme"] in (2, 3) and 0 <= t["panel"] <= 4 and t["look_ahead"] in (0, 1) and t["ms"] > 0
+    assert n <= (256, 512, 768, 1152, 1280)[t["panel"]]
+    rng = np.random.default_rng(n + count)
+    M = rng.standard_normal((count, n, n))
+    A = M + np.transpose(M, (0, 2, 1)) + 2.0 * np.sqrt(n) * np.eye(n)
+    got, st = _lib.inverse_batched(A, symmetrize=True)
+    assert np.all(st == 0)
+    for b in range(count):
+        ref = np.linalg.inv(A[b])
+        assert np.max(np.abs(got[b] - ref)) / np.max(np.abs(ref)) < 1e-12
