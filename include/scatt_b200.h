@@ -32,6 +32,7 @@ extern "C" {
 #define SCATT_ERR_STATE          8   /* call order (e.g. solve before upload)       */
 #define SCATT_ERR_OOM            9   /* device allocation failed                    */
 #define SCATT_ERR_FIT_WINDOW    10   /* AsymptoticAmplitudes.cpp:85-91 abort        */
+#define SCATT_ERR_IO            11   /* file missing, unreadable or not the expected HDF5 */
 
 /* ------------------------------------------------------------------ misc */
 const char* scatt_version(void);
@@ -296,6 +297,116 @@ int scatt_scan_close(scatt_scan* scan);
  * seconds, out[6] floating-point operations of the sampled inversions
  * (2 n^3 per matrix of order n). */
 int scatt_last_stats(scatt_ctx* ctx, double* out7);
+
+/* ------------------------------------------------------ file formats
+ * Host-only entry points (no device work, no GPU needed) for the files
+ * around the path, on an HDF5 subset written from the public file-format
+ * specification (the container has no libhdf5): superblock 0, symbol-table
+ * groups, version-1 object headers, contiguous or chunked + deflate
+ * datasets, scalar attributes.  Readers also take superblock 1, continuation
+ * blocks, compact layout, shuffle and fletcher32; anything else returns
+ * SCATT_ERR_IO with the reason, never a misread. */
+
+/* Generic writer: the file appears at `path` on scatt_h5w_close(h, 1)
+ * (written as path.tmp.pid<PID>, then renamed); keep = 0 discards it.
+ * kind: 0 f64, 1 i64, 2 i32; rank 0 = scalar; data row-major; gzip 1..9
+ * stores the dataset chunked along its first dimension and deflated. */
+typedef struct scatt_h5w scatt_h5w;
+int scatt_h5w_open(const char* path, scatt_h5w** out);
+int scatt_h5w_group(scatt_h5w* h, const char* path);
+int scatt_h5w_dataset(scatt_h5w* h, const char* path, int kind, int rank, const long long* dims,
+                      const void* data, int gzip);
+int scatt_h5w_attr_f64(scatt_h5w* h, const char* obj, const char* name, double v);
+int scatt_h5w_attr_i64(scatt_h5w* h, const char* obj, const char* name, long long v);
+int scatt_h5w_attr_str(scatt_h5w* h, const char* obj, const char* name, const char* v);
+int scatt_h5w_close(scatt_h5w* h, int keep);
+
+/* Generic reader.  kind: 0 absent, 1 group, 2 dataset.  shape: rank,
+ * dims (<= 8) and element kind (0 float, 1 integer, 3 string).  read: the
+ * block [start, start + count) (both NULL: everything) converted to f64
+ * (as_int = 0) or int64, row-major.  list: member names, one per line.
+ * attr: kind 0 absent, 1 float, 2 integer-valued, 3 string. */
+typedef struct scatt_h5r scatt_h5r;
+int scatt_h5r_open(const char* path, scatt_h5r** out);
+int scatt_h5r_kind(scatt_h5r* h, const char* path, int* kind);
+int scatt_h5r_shape(scatt_h5r* h, const char* path, int* rank, long long* dims8, int* elem_kind);
+int scatt_h5r_read(scatt_h5r* h, const char* path, int as_int, int rank, const long long* start,
+                   const long long* count, void* out);
+int scatt_h5r_list(scatt_h5r* h, const char* group, char* buf, long long cap, long long* needed);
+int scatt_h5r_attr(scatt_h5r* h, const char* obj, const char* name, int* kind, double* f, long long* i,
+                   char* s, long long cap);
+int scatt_h5r_close(scatt_h5r* h);
+
+/* Dipole scan output in the layout of the reference's DipoleWriter
+ * (src/scatt/DipoleIO.hpp:115-148, DipoleIO.cpp:141-336): <scan_dir>/
+ * manifest.h5 (/grid, /kgrid attributes; /occ, /atoms datasets;
+ * /conventions, /run string attributes), one ik<NNNN>.h5 per energy (/meta
+ * attributes ik, k = ik dk, E = k^2 / 2, omega = E - E_HOMO,
+ * fit_residual_rel, K_symmetry_err; /A, /B (n_ch x n_ch), /b_overlap
+ * (n_ch x n_occ), /dipole/{length,velocity}/{x,y,z}/{D_ortho_re,
+ * D_ortho_im, D_raw_re, D_raw_im, d_raw, d_correction} + attribute
+ * partial_sigma) and __SUCCESS__ from finalize.  Files are written under a
+ * PID-tagged temporary name and renamed into place; a rename that loses to
+ * another process's identical file counts as success. */
+typedef struct {
+    double r_min, dr;
+    long long N_grid;
+    int    l_max_continuum;
+    double dk;
+    int    ik_min, ik_max;           /* ik_max exclusive */
+    double E_HOMO;                   /* initial-state energy (Koopmans) */
+    int    n_occ;
+    const double* occ_energies;      /* n_occ */
+    const double* occ_spin_factors;  /* n_occ */
+    int    n_atoms;
+    const int* Z;                    /* n_atoms */
+    const double* xyz_bohr;          /* n_atoms x 3 */
+    const char* molecule_name;       /* NULL: "" */
+    const char* git_hash;
+    const char* iso_date_utc;
+    const char* psi_dir_prefix;
+} scatt_dipole_meta;
+
+/* One energy's payload; matrices row-major in their natural orientation,
+ * slices in the order length x, y, z, velocity x, y, z. */
+typedef struct {
+    int ik, n_ch, n_occ;
+    const double *A, *B;             /* n_ch x n_ch */
+    const double* b_overlap;         /* n_ch x n_occ */
+    const double *D_re, *D_im;       /* 6 x n_ch, orthogonalised */
+    const double *Draw_re, *Draw_im; /* 6 x n_ch */
+    const double* d_raw;             /* 6 x n_ch */
+    const double* d_corr;            /* 6 x n_occ */
+    const double* partial_sigma;     /* 6 */
+    double fit_residual_rel, K_symmetry_err;
+} scatt_dipole_energy;
+
+/* Creates scan_dir and its manifest (kept as it is when present: a resumed scan). */
+int scatt_dipole_open(const char* scan_dir, const scatt_dipole_meta* meta);
+int scatt_dipole_has_energy(const char* scan_dir, int ik, int* has);
+int scatt_dipole_write_energy(const char* scan_dir, const scatt_dipole_meta* meta, const scatt_dipole_energy* e);
+int scatt_dipole_finalize(const char* scan_dir);
+
+/* Preprocessing input in the reference's schema (src/io/HDF5Reader.hpp:
+ * 42-86, 446-570): a path ending in .orbitals.h5 or .potentials.h5 whose
+ * sibling exists opens the split layout (orbitals + initial state from one
+ * file, potential + polarizability from the other), anything else one
+ * combined file.  info: out_i = {Nr, Lmax_sce, n_alpha, n_occ_alpha, n_sce,
+ * Nlm_orb_store, Nr_orb_store, has_initial_state}, out_d = {rmin, dr,
+ * initial-state energy, alpha_iso (0 when absent)}.  desc fills a scan
+ * description for continuum cutoff l_cont_max with the rows the reference
+ * reads (V_H: (2 l + 1)^2 multipoles; orbitals: (l + min(l, 10) + 1)^2
+ * channels, main.cpp:365, 700-721), pointing into memory the handle owns
+ * until close or the next desc; an /initial_state SOMO becomes orbital
+ * n_sce and the dipole initial state (main.cpp:787-808), else the HOMO.
+ * *E_init (may be NULL) receives that state's energy. */
+typedef struct scatt_preproc scatt_preproc;
+int scatt_preproc_open(const char* path, scatt_preproc** out);
+int scatt_preproc_info(scatt_preproc* p, int* out_i8, double* out_d4);
+int scatt_preproc_orbital_energies(scatt_preproc* p, double* out, int n);
+int scatt_preproc_atoms(scatt_preproc* p, double* out4, int n);
+int scatt_preproc_desc(scatt_preproc* p, int l_cont_max, scatt_scan_desc* desc, double* E_init);
+int scatt_preproc_close(scatt_preproc* p);
 
 #ifdef __cplusplus
 }

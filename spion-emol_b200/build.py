@@ -55,7 +55,7 @@ def compile_one(src, force, hm, verbose):
     if src.endswith(".cu"):
         cmd = [NVCC, *ARCH, *COMMON, "-Xptxas", "-v" if verbose else "-O3", "-c", src, "-o", obj]
     else:
-        cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-I", INCLUDE, "-I", CSRC,
+        cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-Wall", "-I", INCLUDE, "-I", CSRC,
                "-I", "/usr/local/cuda/include", "-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -80,7 +80,7 @@ def build(force: bool = False, jobs: int = 8, verbose: bool = False) -> str:
         raise RuntimeError("nvcc failed:\n" + "\n".join(errs))
     newest = max(os.path.getmtime(o) for o in objs)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lz"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

@@ -20,6 +20,7 @@ STATUS = {
     0: "SCATT_OK", 1: "SCATT_ERR_ARG", 2: "SCATT_ERR_CUDA", 3: "SCATT_ERR_SIZE",
     4: "SCATT_ERR_SINGULAR", 5: "SCATT_ERR_NONFINITE", 6: "SCATT_ERR_CLOSED_CHANNEL",
     7: "SCATT_ERR_NO_DEVICE", 8: "SCATT_ERR_STATE", 9: "SCATT_ERR_OOM", 10: "SCATT_ERR_FIT_WINDOW",
+    11: "SCATT_ERR_IO",
 }
 
 

@@ -135,6 +135,29 @@ class ScanSolver:
         d.chi_cutoff = 1e-15
         self._upload(d)
 
+    @classmethod
+    def from_preproc(cls, path, l_cont_max: int, device: int = 0, n_transition: int = 0) -> "ScanSolver":
+        """A solver on a preprocessing file in the reference's schema (split
+        or combined layout; see h5io.Preproc).  self.E_init is the dipole
+        initial state's energy, self.preproc the opened file's header."""
+        from .h5io import Preproc
+        _bind()
+        self = cls.__new__(cls)
+        self._ctx = C.c_void_p()
+        check(lib().scatt_ctx_create(device, C.byref(self._ctx)))
+        self.inp = None
+        self.l_cont_max = int(l_cont_max)
+        self._keep = []
+        with Preproc(path) as pp:
+            d, self.E_init = pp.desc(l_cont_max)
+            d.n_transition = n_transition
+            self._upload(d)                  # copies to the device before the file's buffers go
+            self.preproc = {k: getattr(pp, k) for k in ("Nr", "dr", "Lmax_sce", "n_alpha", "n_occ", "n_sce",
+                                                        "Nlm_orb_store", "Nr_orb_store", "has_initial_state")}
+            self.orb_energies = pp.orb_energies.copy()
+            self.atoms = pp.atoms.copy()
+        return self
+
     def _upload(self, d):
         check(lib().scatt_upload_static(self._ctx, C.byref(d)))
         info = np.zeros(5, dtype=np.int32)
