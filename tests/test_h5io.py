@@ -339,3 +339,30 @@ def test_preproc_initial_state_becomes_last_orbital(tmp_path):
         assert d.Nlm_store == max(min(cut, inp.psi_lm.shape[1]), min(cut, 30))
         np.testing.assert_array_equal(psi[-1, :min(cut, 30)], init[:min(cut, 30)])
         assert not psi[-1, min(cut, 30):].any()
+
+
+def test_cpp_interface(tmp_path):
+    """host/scatt_io.hpp compiled against the library: DipoleWriter ->
+    DipoleReader bit for bit, HDF5Reader on a file written here."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    pkg = os.path.join(root, "spion-emol_b200")
+    exe = tmp_path / "host_io_check"
+    cmd = ["g++", "-O1", "-std=c++17", "-Wall", "-Werror", "-I", os.path.join(root, "include"),
+           "-I", os.path.join(pkg, "host"), os.path.join(root, "tests", "host_io_check.cpp"), "-o", str(exe),
+           "-L", pkg, "-lscatt_b200", f"-Wl,-rpath,{pkg}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    inp = synth.h2o_like(Nr=301, dr=0.05, l_cont=3, lmax_orb=6, n_orb=3)
+    pre = h5io.write_preproc(tmp_path / "m", inp, split=True)
+    r = subprocess.run([str(exe), str(tmp_path / "scan"), pre], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    lines = [l.split() for l in r.stdout.splitlines()]
+    assert lines[0] == ["dipole", "ok"]
+    pre_line, desc = lines[1], lines[2]
+    assert pre_line[1] == "301" and pre_line[4] == str(inp.n_occ) and pre_line[5] == "3"
+    assert float(pre_line[10]) == 0.05 and float(pre_line[11]) == inp.orb_energies[-1]
+    cut = min((3 + 3 + 1) ** 2, inp.psi_lm.shape[1])
+    assert desc[1:5] == ["3", str(cut), str(inp.psi_lm.shape[2]), "-1"]
+    assert float(desc[8]) == inp.psi_lm[0, 0, 1]
+    assert float(desc[9]) == inp.orb_energies[inp.n_occ - 1]
