@@ -298,6 +298,54 @@ int scatt_scan_close(scatt_scan* scan);
  * (2 n^3 per matrix of order n). */
 int scatt_last_stats(scatt_ctx* ctx, double* out7);
 
+/* ------------------------------------------------------ adjoint
+ * Gradients of the dipoles (and of sigma, tau built on them) with respect
+ * to V(n) and the polarisation potential.  The reference has no adjoint.
+ * scatt_adjoint_forward solves n_energy energies as one lock-step batch
+ * (results into `outputs` as scatt_solve_batch, rows in submission order),
+ * keeping Rinv(a-1) and G(a-1)^T at every segment start a (segment: a
+ * positive multiple of 8 steps).  The small stages after the sweep (K
+ * extraction, psi_N, the fit window, the dipole algebra) are differentiated
+ * by the caller on views of the window store (scatt_adjoint_view_of; the
+ * Python binding runs them in torch), which writes dJ/dRinv(n),
+ * dJ/dSinv(n) (n_s <= n < N) and dJ/dG(N-1)^T into the view's cotangent
+ * buffers.  scatt_adjoint_reverse then recomputes each segment from its
+ * checkpoint and walks it backward: vtr (host, n_energy x Nr, may be NULL)
+ * receives tr dJ/dV(n) per energy, vfull (device [Nr][Np_max][Np_max],
+ * may be NULL) accumulates dJ/dV(n) summed over the energies.  The terms
+ * of V(N) itself (the outer boundary) stay with the caller's small stages.
+ * One reverse pass per forward.  Matrices are column-major. */
+typedef struct scatt_adjoint scatt_adjoint;
+typedef struct {
+    int N, n_s, n_window, n_tr, n_pts, n_start, ne_fit;
+    int Np, Nt, Nf, Krows, Np_max, l_cont;
+    double E;
+    double* Rwin;          /* (N - n_s + 1) x Nt x Nt: Rinv(n_s + i) */
+    double* Swin;          /* (N - n_s + 1) x Np x Np: Sinv(n_s + i) */
+    double* G_last;        /* Krows x Nt: G(N-1)^T */
+    double* RBwin;         /* n_window x Nt x Nt: dJ/dRinv(n_s + i), zero after the forward */
+    double* SBwin;         /* n_window x Np x Np: dJ/dSinv(n_s + i) */
+    double* GB_last;       /* Krows x Nt: dJ/dG(N-1)^T */
+    const double* V_N;     /* Np_max x Np_max: V(N) */
+    const double* B_N;     /* Np_max x Nf */
+    const double* Bs_N;    /* Np_max x Nf: B(N) D^-1(N) */
+    const double* C_N;     /* Krows x Np_max dipole rows at N, NULL when N is past them */
+    const double* Bs_win;  /* n_window x Np_max x Nf: Bs(n_s + i) (zero outside the exchange
+                              region), NULL when no window step is inside it */
+} scatt_adjoint_view;
+
+/* Polarisation potential V_pol(alpha, r_c) of the uploaded scan (form as in
+ * scatt_scan_desc) and an optional additive perturbation of V: a DEVICE
+ * array [Nr][Np_max][Np_max] (column-major per n, upper triangle read,
+ * NULL: none) that stays the caller's and must outlive its use. */
+int scatt_set_polarization(scatt_ctx* ctx, double alpha, double r_c, int pol_form);
+int scatt_set_potential_delta(scatt_ctx* ctx, const double* dV_device);
+int scatt_adjoint_forward(scatt_ctx* ctx, const scatt_solve_opts* opts, int n_energy, const double* energies,
+                          const int* l_cont, int segment, const scatt_outputs* outputs, scatt_adjoint** out);
+int scatt_adjoint_view_of(scatt_adjoint* adj, int i, scatt_adjoint_view* view);
+int scatt_adjoint_reverse(scatt_adjoint* adj, double* vtr, double* vfull_device);
+int scatt_adjoint_close(scatt_adjoint* adj);
+
 /* ------------------------------------------------------ file formats
  * Host-only entry points (no device work, no GPU needed) for the files
  * around the path, on an HDF5 subset written from the public file-format

@@ -2306,6 +2306,659 @@ int solve_batch(Context& ctx, const scatt_solve_opts& o, int n_energy, const dou
     return first;
 }
 
+// ================================================================ adjoint
+// Reverse pass of the forward recurrence and the dipole sweep for a batch of
+// energies solved as one phase group, with R-ratios checkpointed every
+// `segment` steps and each segment recomputed before it is walked backward.
+// The reference has no adjoint; the arithmetic is the one of the oracle's
+// DipoleAdjoint (oracle/adjoint_recurrence.py):
+//   Rbar(n)  = chain + H(n) Gbar(n)^T [+ dJ/dRinv(n) of the small stages]
+//   Hbar(n)  = Rinv(n) Gbar(n),  Gbar(n-1) = Hbar(n)
+//   chain    = X sym(Rbar) X  (the next step's Rbar start), X = Rinv(n)
+//   Wbar(n)  = -12 chain + E_psi L(n) Hbar(n)^T
+//   Sinvbar  = Wbar_pp + U Bs^T - Bs Wbar_fp,  U = Bs Wbar_ff - Wbar_pf  [+ small stages]
+//   Sbar     = -Y sym(Sinvbar) Y,  Y = Sinv(n)
+//   through the stability shifts (n < stab_n): Mbar -= tr(Mbar) P with P the
+//   projector on the eigenvectors of lambda_min (averaged over a degenerate
+//   cluster); dJ/dV(n) = -h^2/6 Abar, plus the analytic start's diagonal terms.
+// The small stages (K extraction, psi_N, the fit window, dipoles) are
+// differentiated by the caller (the Python binding runs them in torch on
+// views of the window store) and enter as dJ/dRinv, dJ/dSinv over the
+// window and dJ/dG(N-1).
+namespace {
+
+struct AdjSlot {
+    double *ckR, *ckG;             // per segment a: Rinv(a-1) (Nt x Nt), G(a-1)^T (K x Nt)
+    double *RB, *T1, *T2, *WB;     // Nt x Nt
+    double *GB0, *GB1;             // K x Nt: Gbar^T ping-pong (parity of n)
+    double *U;                     // Np x Nf
+    double *SBi, *SBs, *SB, *SB2;  // Np x Np
+    double *RBw, *SBw;             // window cotangents: (N - n_s) x Nt^2, (N - n_s) x Np^2
+    double *ab;                    // 2 Np: analytic-start terms of diag dJ/dV(n), dJ/dV(n+1)
+    double *vtr;                   // Nr: tr dJ/dV(n)
+    const double *PA, *PS;         // stab_n x Np x Np shift projectors
+    int Np, Nt;
+};
+
+enum { G_HG, G_HB, G_X1, G_X2, G_CH, G_U, G_S1, G_S2, G_Y1, G_Y2, G_NUM };
+
+struct AdjArgs {
+    AdjSlot* s;
+    EnergyDev* ed;
+    GemmEntry* gm;                 // G_NUM x count
+    const double* Ctab;
+    const double* Bs;              // Bs(n), Np_max x Nf
+    const double* Vn;              // V(n), Np_max x Np_max
+    const double* Vn1;             // V(n + 1)
+    const int* l_of_mu;
+    double* vfull;                 // optional [Nr][Np_max][Np_max] sum over slots
+    int count, K, Nf, Np_max, n_start, n_tr, n_pts, n_s, N, stab_n, seg_lo;
+    double dr, h2_6;
+};
+
+__global__ void k_prep_rev(AdjArgs a, int n) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.count) return;
+    const AdjSlot& S = a.s[e];
+    const EnergyDev& d = a.ed[e];
+    const GemmEntry none{nullptr, nullptr, nullptr, 0, 0, 0, 1, 1, 1, 0.0, 1.0};
+    GemmEntry* g = a.gm;
+    const int c = a.count;
+    if (!d.live) {
+        for (int k = 0; k < G_NUM; ++k) g[k * c + e] = none;
+        return;
+    }
+    const int Np = S.Np, Nt = S.Nt, K = a.K, Nf = a.Nf;
+    const size_t i = (size_t)(n - a.seg_lo);
+    double* Rn = d.segR + i * Nt * Nt;
+    double* Yn = d.segS + i * Np * Np;
+    double* Ht = d.segH + i * K * Nt;
+    double* GBt = (n & 1) ? S.GB1 : S.GB0;
+    double* HBt = (n & 1) ? S.GB0 : S.GB1;
+    const bool exch = n < a.n_tr && Nf > 0;
+    const bool chain = n >= a.n_start;
+    g[G_HG * c + e] = GemmEntry{Ht, GBt, S.RB, Nt, Nt, K, K, K, Nt, 1.0, 1.0};
+    g[G_HB * c + e] = GemmEntry{GBt, Rn, HBt, K, Nt, Nt, K, Nt, K, 1.0, 0.0};
+    g[G_X1 * c + e] = chain ? GemmEntry{Rn, S.T1, S.T2, Nt, Nt, Nt, Nt, Nt, Nt, 1.0, 0.0} : none;
+    g[G_X2 * c + e] = chain ? GemmEntry{S.T2, Rn, S.RB, Nt, Nt, Nt, Nt, Nt, Nt, 1.0, 0.0, 1} : none;
+    g[G_CH * c + e] = (n < a.n_pts) ? GemmEntry{a.Ctab + (size_t)n * K * a.Np_max, HBt, S.WB, Np, Nt, K, K, K, Nt,
+                                                1.0, 1.0}
+                                    : none;
+    g[G_U * c + e] = exch ? GemmEntry{a.Bs, S.WB + Np + (size_t)Np * Nt, S.U, Np, Nf, Nf, a.Np_max, Nt, Np, 1.0, 1.0}
+                          : none;
+    g[G_S1 * c + e] = exch ? GemmEntry{S.U, a.Bs, S.SBi, Np, Np, Nf, Np, a.Np_max, Np, 1.0, 1.0} : none;
+    g[G_S2 * c + e] = exch ? GemmEntry{a.Bs, S.WB + Np, S.SBi, Np, Np, Nf, a.Np_max, Nt, Np, -1.0, 1.0} : none;
+    g[G_Y1 * c + e] = GemmEntry{Yn, S.SBs, S.SB, Np, Np, Np, Np, Np, Np, 1.0, 0.0};
+    g[G_Y2 * c + e] = GemmEntry{S.SB, Yn, S.SB2, Np, Np, Np, Np, Np, Np, -1.0, 0.0, 1};
+}
+
+// RB += dJ/dRinv(n) of the small stages (window steps); grid (x, slots)
+__global__ void k_rev_window(AdjArgs a, int n) {
+    const AdjSlot& S = a.s[blockIdx.y];
+    if (!a.ed[blockIdx.y].live) return;
+    const size_t nt2 = (size_t)S.Nt * S.Nt;
+    const double* w = S.RBw + (size_t)(n - a.n_s) * nt2;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < nt2; idx += (size_t)gridDim.x * blockDim.x)
+        S.RB[idx] += w[idx];
+}
+
+// which = 0: T1 = sym(RB);  1: SBs = sym(SBi)
+__global__ void k_rev_sym(AdjArgs a, int which) {
+    const AdjSlot& S = a.s[blockIdx.y];
+    if (!a.ed[blockIdx.y].live) return;
+    const int n = which ? S.Np : S.Nt;
+    const double* in = which ? S.SBi : S.RB;
+    double* out = which ? S.SBs : S.T1;
+    const size_t tot = (size_t)n * n;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < tot; idx += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = idx % n, c = idx / n;
+        out[idx] = 0.5 * (in[idx] + in[c + r * n]);
+    }
+}
+
+// after the chain: WB = -12 RB (RB holds X sym(Rbar) X);  in the analytic
+// start (chain = 0): RB = 0, WB = 0
+__global__ void k_rev_wb(AdjArgs a, int chain) {
+    const AdjSlot& S = a.s[blockIdx.y];
+    if (!a.ed[blockIdx.y].live) return;
+    const size_t tot = (size_t)S.Nt * S.Nt;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < tot; idx += (size_t)gridDim.x * blockDim.x) {
+        if (chain) {
+            S.WB[idx] = -12.0 * S.RB[idx];
+        } else {
+            S.WB[idx] = 0.0;
+            S.RB[idx] = 0.0;
+        }
+    }
+}
+
+// d R_mumu / d V(n)_mumu and d R_mumu / d V(n+1)_mumu of the analytic start
+// (ForwardRPropagator.cpp:78-134) times Rbar_mumu; grid (channels, slots)
+__global__ void k_rev_analytic(AdjArgs a, int n) {
+    const int e = blockIdx.y;
+    const AdjSlot& S = a.s[e];
+    const EnergyDev& d = a.ed[e];
+    const int mu = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!d.live || mu >= S.Np) return;
+    double gn = 0.0, gn1 = 0.0;
+    if (n >= 1) {
+        const int l = a.l_of_mu[mu];
+        const double h = a.dr;
+        const double rn = a.dr + n * h, rn1 = a.dr + (n + 1) * h;
+        const double Mn = 1.0 + a.h2_6 * (d.E - a.Vn[mu + (size_t)mu * a.Np_max]);
+        const double Mn1 = 1.0 + a.h2_6 * (d.E - a.Vn1[mu + (size_t)mu * a.Np_max]);
+        const double yn = riccati_j(l, d.k * rn), yn1 = riccati_j(l, d.k * rn1);
+        const double den = Mn1 * yn1;
+        if (fabs(den) > 1e-300) {
+            const double rb = S.RB[mu + (size_t)mu * S.Nt];
+            gn = rb * (-a.h2_6 * yn / den);
+            gn1 = rb * (a.h2_6 * Mn * yn / (Mn1 * den));
+        }
+    }
+    S.ab[mu] = gn;
+    S.ab[S.Np + mu] = gn1;
+}
+
+// SBi = Wbar_pp [+ window dJ/dSinv(n)];  exchange steps: U = -Wbar_pf
+__global__ void k_rev_sbi(AdjArgs a, int n, int exch, int win) {
+    const AdjSlot& S = a.s[blockIdx.y];
+    if (!a.ed[blockIdx.y].live) return;
+    const int Np = S.Np, Nt = S.Nt;
+    const size_t np2 = (size_t)Np * Np;
+    const double* w = win ? S.SBw + (size_t)(n - a.n_s) * np2 : nullptr;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < np2; idx += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = idx % Np, c = idx / Np;
+        double v = S.WB[r + c * Nt];
+        if (w) v += w[idx];
+        S.SBi[idx] = v;
+    }
+    if (exch) {
+        const size_t tot = (size_t)Np * a.Nf;
+        for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < tot;
+             idx += (size_t)gridDim.x * blockDim.x) {
+            const size_t r = idx % Np, c = idx / Np;
+            S.U[idx] = -S.WB[r + (Np + c) * Nt];
+        }
+    }
+}
+
+__device__ double block_sum(double v, double* red) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[i];
+        red[32] = s;
+    }
+    __syncthreads();
+    return red[32];
+}
+
+// Sbar (in SB2) through the stability shifts of step n (in place: SB2 <- Abar)
+// and tr dJ/dV(n) = -h^2/6 tr Abar (+ the analytic start's terms); one block per slot
+__global__ void k_rev_vbar(AdjArgs a, int n) {
+    const int e = blockIdx.x;
+    const AdjSlot& S = a.s[e];
+    const EnergyDev& d = a.ed[e];
+    if (!d.live) return;
+    const int Np = S.Np;
+    const size_t np2 = (size_t)Np * Np;
+    __shared__ double red[33];
+    double t = 0.0;
+    for (int i = threadIdx.x; i < Np; i += blockDim.x) t += S.SB2[i + (size_t)i * Np];
+    double trS = block_sum(t, red);
+    double cS = 0.0, cA = 0.0;
+    if (n < a.stab_n) {
+        const bool shS = d.stabd[2 * n + 1] != 0.0, shA = d.stabd[2 * n] != 0.0;
+        cS = shS ? trS : 0.0;                  // Sbar -= tr(Sbar) P_S
+        cA = shA ? trS - cS : 0.0;             // Abar -= tr(Abar) P_A, tr(Abar) = tr(Sbar) - cS
+        if (cS != 0.0 || cA != 0.0) {
+            const double* PS = S.PS + (size_t)n * np2;
+            const double* PA = S.PA + (size_t)n * np2;
+            for (size_t idx = threadIdx.x; idx < np2; idx += blockDim.x)
+                S.SB2[idx] -= cS * PS[idx] + cA * PA[idx];
+        }
+    }
+    if (threadIdx.x == 0) {
+        S.vtr[n] += -a.h2_6 * (trS - cS - cA);
+        if (n < a.n_start && n >= 1) {
+            double s0 = 0.0, s1 = 0.0;
+            for (int mu = 0; mu < Np; ++mu) { s0 += S.ab[mu]; s1 += S.ab[Np + mu]; }
+            S.vtr[n] += s0;
+            S.vtr[n + 1] += s1;
+        }
+    }
+}
+
+// vfull[n] += sum over slots of dJ/dV(n) (and the analytic start's diagonal
+// terms at n and n + 1); slots in order, so the sum is deterministic
+__global__ void k_rev_vfull(AdjArgs a, int n) {
+    const size_t np2 = (size_t)a.Np_max * a.Np_max;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < np2; idx += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(idx % a.Np_max), c = (int)(idx / a.Np_max);
+        double v = 0.0, v1 = 0.0;
+        for (int e = 0; e < a.count; ++e) {
+            const AdjSlot& S = a.s[e];
+            if (!a.ed[e].live || r >= S.Np || c >= S.Np) continue;
+            v += -a.h2_6 * S.SB2[r + (size_t)c * S.Np];
+            if (r == c && n >= 1 && n < a.n_start) {
+                v += S.ab[r];
+                v1 += S.ab[S.Np + r];
+            }
+        }
+        a.vfull[(size_t)n * np2 + idx] += v;
+        if (v1 != 0.0) a.vfull[(size_t)(n + 1) * np2 + idx] += v1;
+    }
+}
+
+// cyclic Jacobi eigen-decomposition of a symmetric n x n matrix (column-major,
+// destroyed): eigenvalues w (ascending) and eigenvectors in the columns of Z
+void jacobi_eig(std::vector<double>& A, int n, std::vector<double>& w, std::vector<double>& Z) {
+    Z.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) Z[i + (size_t)i * n] = 1.0;
+    auto at = [&](int i, int j) -> double& { return A[i + (size_t)j * n]; };
+    double scale = 0.0;
+    for (double x : A) scale = std::max(scale, std::fabs(x));
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        double off = 0.0;
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < j; ++i) off = std::max(off, std::fabs(at(i, j)));
+        if (off <= 1e-17 * std::max(scale, 1e-300)) break;
+        for (int p = 0; p < n - 1; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                const double apq = at(p, q);
+                if (std::fabs(apq) <= 1e-300) continue;
+                const double theta = (at(q, q) - at(p, p)) / (2.0 * apq);
+                const double tt = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                const double cs = 1.0 / std::sqrt(tt * tt + 1.0), sn = tt * cs;
+                for (int k = 0; k < n; ++k) {           // columns p, q
+                    const double akp = at(k, p), akq = at(k, q);
+                    at(k, p) = cs * akp - sn * akq;
+                    at(k, q) = sn * akp + cs * akq;
+                }
+                for (int k = 0; k < n; ++k) {           // rows p, q
+                    const double apk = at(p, k), aqk = at(q, k);
+                    at(p, k) = cs * apk - sn * aqk;
+                    at(q, k) = sn * apk + cs * aqk;
+                }
+                for (int k = 0; k < n; ++k) {
+                    const double zkp = Z[k + (size_t)p * n], zkq = Z[k + (size_t)q * n];
+                    Z[k + (size_t)p * n] = cs * zkp - sn * zkq;
+                    Z[k + (size_t)q * n] = sn * zkp + cs * zkq;
+                }
+            }
+    }
+    w.resize(n);
+    for (int i = 0; i < n; ++i) w[i] = at(i, i);
+}
+
+// projector on the eigenvectors of the smallest eigenvalue of M (n x n,
+// column-major), averaged over the eigenvalues within a relative 1e-9 of it
+std::vector<double> min_eig_projector(std::vector<double> M, int n) {
+    std::vector<double> w, Z;
+    jacobi_eig(M, n, w, Z);
+    const int i0 = (int)(std::min_element(w.begin(), w.end()) - w.begin());
+    const double tol = 1e-9 * std::max(1.0, std::fabs(w[i0]));
+    std::vector<int> cl;
+    for (int i = 0; i < n; ++i)
+        if (w[i] - w[i0] <= tol) cl.push_back(i);
+    std::vector<double> P((size_t)n * n, 0.0);
+    for (int k : cl)
+        for (int c = 0; c < n; ++c)
+            for (int r = 0; r < n; ++r) P[r + (size_t)c * n] += Z[r + (size_t)k * n] * Z[c + (size_t)k * n];
+    for (double& x : P) x /= (double)cl.size();
+    return P;
+}
+
+}  // namespace
+
+// One adjoint batch: the forward scan (one phase group) with its checkpoints
+// and window cotangents, ready for the reverse pass.
+struct Adjoint {
+    Scan sc;
+    int segment = 256, nseg = 0, nwin = 0;
+    std::vector<AdjSlot> slot;           // host copies (device pointers)
+    DevBuf<AdjSlot> d_slot;
+    DevBuf<double> arena;                // checkpoints, segment stores, work, cotangents
+    DevBuf<double> stabd;                // 2 stab_n per slot
+    std::vector<DevBuf<double>> proj;    // shift projectors PA, PS per distinct Np (pairs)
+    std::vector<int> proj_Np;
+    DevBuf<GemmEntry> gm;
+    VBAt vb[2];                          // V/B at n (parity) for the reverse
+    VBAt vbN;                            // V(N), B(N), Bs(N) for the small stages
+    DevBuf<double> bswin;                // Bs(m) of the window steps inside the exchange region
+    int n_energy = 0;
+    std::vector<int> slot_of;            // submission order -> slot
+    bool reversed = false;
+};
+
+namespace {
+
+// device location of Rinv(n) outside any segment (rinv_at with in_seg false)
+double* rinv_home(const BatchDev& b, const EnergyDev& d, int n) {
+    const size_t nt2 = (size_t)d.Nt * d.Nt;
+    return n >= b.n_s ? d.tailR + (size_t)(n - b.n_s) * nt2 : ((n & 1) ? d.Rinv1 : d.Rinv0);
+}
+
+int adj_projectors(Adjoint& A, int Np, const double** out_PA, const double** out_PS) {
+    Scan& sc = A.sc;
+    const BatchDev& b = sc.b;
+    cudaStream_t s = sc.ctx->stream;
+    for (size_t i = 0; i < A.proj_Np.size(); ++i)
+        if (A.proj_Np[i] == Np) {
+            *out_PA = A.proj[2 * i].p;
+            *out_PS = A.proj[2 * i + 1].p;
+            return SCATT_OK;
+        }
+    const size_t np2 = (size_t)Np * Np;
+    const int ns = b.stab_n;
+    std::vector<double> PA(std::max<size_t>(1, ns * np2), 0.0), PS(std::max<size_t>(1, ns * np2), 0.0);
+    VBAt vb;
+    SCATT_TRY(vb.alloc(b));
+    const int Npm = b.Np_max, Nf = b.Nf;
+    std::vector<double> V((size_t)Npm * Npm), B((size_t)Npm * std::max(1, Nf)), Bs((size_t)Npm * std::max(1, Nf));
+    for (int n = 0; n < ns; ++n) {
+        vb.build(b, n, s);
+        SCATT_CUDA_TRY(cudaMemcpyAsync(V.data(), vb.V.p, V.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        SCATT_CUDA_TRY(cudaMemcpyAsync(B.data(), vb.B.p, B.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        SCATT_CUDA_TRY(cudaMemcpyAsync(Bs.data(), vb.Bs.p, Bs.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        SCATT_CUDA_TRY(cudaStreamSynchronize(s));
+        // the shifts compare c + lambda_min(-h^2/6 V) and c + dA + lambda_min(-h^2/6 V - Bs B^T):
+        // the identity terms move no eigenvector
+        std::vector<double> M(np2);
+        for (int c = 0; c < Np; ++c)
+            for (int r = 0; r < Np; ++r) M[r + (size_t)c * Np] = -b.h2_6 * V[r + (size_t)c * Npm];
+        const auto pa = min_eig_projector(M, Np);
+        std::copy(pa.begin(), pa.end(), PA.begin() + n * np2);
+        if (n < b.n_tr && Nf > 0) {
+            for (int c = 0; c < Np; ++c)
+                for (int r = 0; r < Np; ++r) {
+                    double acc = 0.0;
+                    for (int f = 0; f < Nf; ++f) acc += Bs[r + (size_t)f * Npm] * B[c + (size_t)f * Npm];
+                    M[r + (size_t)c * Np] = -b.h2_6 * V[r + (size_t)c * Npm] - acc;
+                }
+            // the device forms Bs B^T symmetric (lower tiles mirrored)
+            for (int c = 0; c < Np; ++c)
+                for (int r = 0; r < c; ++r) M[r + (size_t)c * Np] = M[c + (size_t)r * Np];
+            const auto ps = min_eig_projector(M, Np);
+            std::copy(ps.begin(), ps.end(), PS.begin() + n * np2);
+        }
+    }
+    A.proj_Np.push_back(Np);
+    A.proj.emplace_back();
+    SCATT_TRY(upload_vec(A.proj.back(), PA, s));
+    A.proj.emplace_back();
+    SCATT_TRY(upload_vec(A.proj.back(), PS, s));
+    SCATT_CUDA_TRY(cudaStreamSynchronize(s));
+    *out_PA = A.proj[A.proj.size() - 2].p;
+    *out_PS = A.proj.back().p;
+    return SCATT_OK;
+}
+
+AdjArgs adj_args(Adjoint& A) {
+    const BatchDev& b = A.sc.b;
+    const ScanTables& t = *A.sc.ctx->tab;
+    AdjArgs a{};
+    a.s = A.d_slot.p;
+    a.ed = A.sc.d_ed.p;
+    a.gm = A.gm.p;
+    a.Ctab = t.Ctab.p;
+    a.l_of_mu = t.d_l_of_mu.p;
+    a.count = A.sc.slots;
+    a.K = b.Krows;
+    a.Nf = b.Nf;
+    a.Np_max = b.Np_max;
+    a.n_start = b.n_start;
+    a.n_tr = b.n_tr;
+    a.n_pts = b.n_pts;
+    a.n_s = b.n_s;
+    a.N = b.N;
+    a.stab_n = b.stab_n;
+    a.dr = b.dr;
+    a.h2_6 = b.h2_6;
+    return a;
+}
+
+}  // namespace
+
+// Forward scan of n energies (one group, every slot live) keeping the
+// checkpoints; post stages as scatt_solve_batch (results into `out`, rows in
+// submission order).
+int adj_forward(Context& ctx, const scatt_solve_opts& o_in, int n, const double* E, const int* lc, int segment,
+                const scatt_outputs* out, Adjoint& A) {
+    ScanTables& t = *ctx.tab;
+    cudaStream_t s = ctx.stream;
+    if (n < 1 || segment < SCHUR_CHUNK || segment % SCHUR_CHUNK) {
+        set_last_error("scatt_adjoint_forward: need n_energy >= 1 and a segment that is a positive multiple of " +
+                       std::to_string(SCHUR_CHUNK));
+        return SCATT_ERR_ARG;
+    }
+    int l_cap = 0;
+    for (int e = 0; e < n; ++e) l_cap = std::max(l_cap, lc ? lc[e] : t.l_max);
+    scatt_solve_opts o = o_in;
+    o.use_graphs = 0;
+    Scan& sc = A.sc;
+    SCATT_TRY(scan_open(ctx, o, n, 1, l_cap, sc));
+    const BatchDev& b = sc.b;
+    const int K = b.Krows, Nf = b.Nf, N = b.N;
+    A.segment = segment;
+    A.nseg = (N + segment - 1) / segment;            // segments [a, min(a + segment, N)), a < N
+    A.nwin = N - b.n_s;                              // window steps n_s .. N - 1
+    A.n_energy = n;
+    for (int e = 0; e < n; ++e) sc.queue.push_back(Job{E[e], lc ? lc[e] : t.l_max, e});
+    sc.submitted = n;
+    SCATT_TRY(load_group(sc, 0));
+    A.slot_of.assign(n, -1);
+    for (int e = 0; e < n; ++e) A.slot_of[sc.job_of[e]] = e;
+    // ---- arena: per slot checkpoints, segment stores, work and cotangents
+    auto al = [](size_t c) { return (c + 31) & ~size_t(31); };
+    std::vector<size_t> per(n);
+    size_t total = 0;
+    for (int e = 0; e < n; ++e) {
+        const size_t Np = sc.ed[e].Np, Nt = sc.ed[e].Nt, np2 = Np * Np, nt2 = Nt * Nt, seg = segment;
+        per[e] = A.nseg * (al(nt2) + al(K * Nt)) + al(seg * nt2) + al(seg * np2) + al(seg * K * Nt) + 4 * al(nt2) +
+                 2 * al(K * Nt) + al(Np * std::max(1, Nf)) + 4 * al(np2) + al((size_t)A.nwin * nt2) +
+                 al((size_t)A.nwin * np2) + al(2 * Np) + al(t.Nr + 1);
+        total += per[e];
+    }
+    SCATT_TRY(A.arena.alloc(total));
+    SCATT_CUDA_TRY(cudaMemsetAsync(A.arena.p, 0, total * sizeof(double), s));
+    SCATT_TRY(A.stabd.alloc((size_t)n * 2 * std::max(1, b.stab_n)));
+    SCATT_CUDA_TRY(cudaMemsetAsync(A.stabd.p, 0, A.stabd.n * sizeof(double), s));
+    A.slot.assign(n, AdjSlot{});
+    double* p = A.arena.p;
+    auto take = [&p, &al](size_t c) { double* r = p; p += al(c); return r; };
+    for (int e = 0; e < n; ++e) {
+        EnergyDev& d = sc.ed[e];
+        AdjSlot& S = A.slot[e];
+        const size_t Np = d.Np, Nt = d.Nt, np2 = Np * Np, nt2 = Nt * Nt, seg = segment;
+        S.Np = d.Np;
+        S.Nt = d.Nt;
+        S.ckR = take(A.nseg * al(nt2));
+        S.ckG = take(A.nseg * al(K * Nt));
+        d.segR = take(seg * nt2);
+        d.segS = take(seg * np2);
+        d.segH = take(seg * K * Nt);
+        S.RB = take(nt2); S.T1 = take(nt2); S.T2 = take(nt2); S.WB = take(nt2);
+        S.GB0 = take(K * Nt); S.GB1 = take(K * Nt);
+        S.U = take(Np * std::max(1, Nf));
+        S.SBi = take(np2); S.SBs = take(np2); S.SB = take(np2); S.SB2 = take(np2);
+        S.RBw = take((size_t)A.nwin * nt2);
+        S.SBw = take((size_t)A.nwin * np2);
+        S.ab = take(2 * Np);
+        S.vtr = take(t.Nr + 1);
+        d.seg_lo = d.seg_hi = 0;
+        d.stabd = A.stabd.p + (size_t)e * 2 * std::max(1, b.stab_n);
+        SCATT_TRY(adj_projectors(A, d.Np, &S.PA, &S.PS));
+    }
+    SCATT_CUDA_TRY(cudaMemcpyAsync(sc.d_ed.p, sc.ed.data(), n * sizeof(EnergyDev), cudaMemcpyHostToDevice, s));
+    SCATT_TRY(upload_vec(A.d_slot, A.slot, s));
+    SCATT_TRY(A.gm.alloc((size_t)G_NUM * n));
+    // ---- the sweep, with a checkpoint at every segment start a: Rinv(a-1), G(a-1)^T
+    while (sc.grp[0].n0 >= 0) {
+        const int next = sc.grp[0].n0 + sc.grp[0].C;
+        SCATT_TRY(run_chunk(sc, nullptr));
+        if (next % segment == 0 && next < N) {
+            const int si = next / segment;
+            for (int e = 0; e < n; ++e) {
+                const EnergyDev& d = sc.ed[e];
+                const size_t nt2 = (size_t)d.Nt * d.Nt;
+                SCATT_CUDA_TRY(cudaMemcpyAsync(A.slot[e].ckR + si * al(nt2), rinv_home(b, d, next - 1),
+                                               nt2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+                SCATT_CUDA_TRY(cudaMemcpyAsync(A.slot[e].ckG + si * al((size_t)K * d.Nt), (next & 1) ? d.G1 : d.G0,
+                                               (size_t)K * d.Nt * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            }
+        }
+    }
+    // ---- post stages (slots keep their energies for the reverse pass)
+    std::vector<int> sel(n);
+    std::vector<long> rows(n);
+    for (int e = 0; e < n; ++e) { sel[e] = e; rows[e] = sc.job_of[e]; }
+    int first = SCATT_OK;
+    std::string msg;
+    SCATT_TRY(post_slots(sc, sel, rows, out, &first, &msg));
+    sc.grp[0].n0 = -1;
+    // ---- what the small stages read besides the window store: V(N), B(N), Bs(N); Bs of window steps
+    SCATT_TRY(A.vbN.alloc(b));
+    A.vbN.build(b, N, s);
+    int nwx = 0;
+    for (int m = b.n_s; m < N; ++m) nwx += (m < b.n_tr && Nf > 0) ? 1 : 0;
+    SCATT_TRY(A.vb[0].alloc(b));
+    SCATT_TRY(A.vb[1].alloc(b));
+    if (nwx > 0) {
+        const size_t sl = (size_t)b.Np_max * Nf;
+        SCATT_TRY(A.bswin.alloc((size_t)A.nwin * sl));
+        SCATT_CUDA_TRY(cudaMemsetAsync(A.bswin.p, 0, A.bswin.n * sizeof(double), s));
+        for (int m = b.n_s; m < N; ++m)
+            if (m < b.n_tr) {
+                A.vb[0].build(b, m, s);
+                SCATT_CUDA_TRY(cudaMemcpyAsync(A.bswin.p + (size_t)(m - b.n_s) * sl, A.vb[0].Bs.p, sl * sizeof(double),
+                                               cudaMemcpyDeviceToDevice, s));
+            }
+    }
+    SCATT_CUDA_TRY(cudaStreamSynchronize(s));
+    if (first != SCATT_OK) set_last_error(msg);
+    return first;
+}
+
+// The reverse pass: per segment, last to first, recompute it from its
+// checkpoint, then walk its steps backward.  vtr_host: n_energy x (Nr)
+// tr dJ/dV(n) in submission order; vfull (device, may be null):
+// [Nr][Np_max][Np_max] += dJ/dV(n) summed over the energies.
+int adj_reverse(Adjoint& A, double* vtr_host, double* vfull) {
+    Scan& sc = A.sc;
+    BatchDev& b = sc.b;
+    cudaStream_t s = sc.ctx->stream;
+    const int n = sc.slots, N = b.N, K = b.Krows, seg = A.segment;
+    auto al = [](size_t c) { return (c + 31) & ~size_t(31); };
+    if (A.reversed) {
+        set_last_error("scatt_adjoint_reverse: the pass has run; run the forward again");
+        return SCATT_ERR_STATE;
+    }
+    A.reversed = true;
+    AdjArgs args = adj_args(A);
+    args.vfull = vfull;
+    // RB(N-1) starts at zero; Gbar(N-1)^T is the caller's dJ/dG(N-1)^T (buffer of parity N-1)
+    for (int e = 0; e < n; ++e)
+        SCATT_CUDA_TRY(cudaMemsetAsync(A.slot[e].RB, 0, (size_t)A.slot[e].Nt * A.slot[e].Nt * sizeof(double), s));
+    A.vb[N & 1].build(b, N, s);                       // V(n + 1) for the first step n = N - 1
+    const int Ntc = sc.Nt_cap, Npc = sc.Np_cap, Nf = b.Nf;
+    auto gemm = [&](int which, int M, int Nn, int opA, int opB) {
+        return gemm_batched(A.gm.p + (size_t)which * n, n, M, Nn, opA, opB, s);
+    };
+    const dim3 eg(64, n);
+    for (int si = A.nseg - 1; si >= 0; --si) {
+        const int a = si * seg, bnd = std::min(a + seg, N);
+        // ---- recompute [a, bnd) from the checkpoint into the segment stores
+        for (int e = 0; e < n; ++e) {
+            EnergyDev& d = sc.ed[e];
+            const size_t nt2 = (size_t)d.Nt * d.Nt, kn = (size_t)K * d.Nt;
+            if (a >= 1) {
+                SCATT_CUDA_TRY(cudaMemcpyAsync(rinv_home(b, d, a - 1), A.slot[e].ckR + si * al(nt2),
+                                               nt2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+                SCATT_CUDA_TRY(cudaMemcpyAsync(d.segH, A.slot[e].ckG + si * al(kn), kn * sizeof(double),
+                                               cudaMemcpyDeviceToDevice, s));
+            } else {
+                SCATT_CUDA_TRY(cudaMemsetAsync(d.segH, 0, kn * sizeof(double), s));
+            }
+            d.seg_lo = a;
+            d.seg_hi = bnd;
+        }
+        SCATT_CUDA_TRY(cudaMemcpyAsync(sc.d_ed.p, sc.ed.data(), n * sizeof(EnergyDev), cudaMemcpyHostToDevice, s));
+        b.n_stop = bnd;
+        k_set_group<<<1, 1, 0, s>>>(b, 0, a);
+        SCATT_COUNT_LAUNCH(1);
+        sc.grp[0].n0 = a;
+        sc.grp[0].C = std::min(SCHUR_CHUNK, bnd - a);
+        while (sc.grp[0].n0 >= 0) SCATT_TRY(run_chunk(sc, nullptr));
+        sc.grp[0].n0 = -1;
+        // ---- the steps of the segment, backward
+        args.seg_lo = a;
+        for (int m = bnd - 1; m >= a; --m) {
+            VBAt& vc = A.vb[m & 1];
+            vc.build(b, m, s);
+            args.Bs = vc.Bs.p;
+            args.Vn = vc.V.p;
+            args.Vn1 = A.vb[(m + 1) & 1].V.p;
+            const bool exch = m < b.n_tr && Nf > 0;
+            const bool win = m >= b.n_s && m <= N - 1;
+            k_prep_rev<<<cdiv(n, 64), 64, 0, s>>>(args, m);
+            SCATT_COUNT_LAUNCH(1);
+            if (win) { k_rev_window<<<eg, TPB, 0, s>>>(args, m); SCATT_COUNT_LAUNCH(1); }
+            SCATT_TRY(gemm(G_HG, Ntc, Ntc, 1, 0));
+            SCATT_TRY(gemm(G_HB, K, Ntc, 0, 0));
+            if (m >= b.n_start) {
+                k_rev_sym<<<eg, TPB, 0, s>>>(args, 0);
+                SCATT_COUNT_LAUNCH(1);
+                SCATT_TRY(gemm(G_X1, Ntc, Ntc, 0, 0));
+                SCATT_TRY(gemm(G_X2, Ntc, Ntc, 0, 0));
+                k_rev_wb<<<eg, TPB, 0, s>>>(args, 1);
+                SCATT_COUNT_LAUNCH(1);
+            } else {
+                k_rev_analytic<<<dim3(cdiv(Npc, 128), n), 128, 0, s>>>(args, m);
+                SCATT_COUNT_LAUNCH(1);
+                k_rev_wb<<<eg, TPB, 0, s>>>(args, 0);
+                SCATT_COUNT_LAUNCH(1);
+            }
+            if (m < b.n_pts) SCATT_TRY(gemm(G_CH, Npc, Ntc, 1, 0));
+            k_rev_sbi<<<eg, TPB, 0, s>>>(args, m, exch ? 1 : 0, win ? 1 : 0);
+            SCATT_COUNT_LAUNCH(1);
+            if (exch) {
+                SCATT_TRY(gemm(G_U, Npc, Nf, 0, 0));
+                SCATT_TRY(gemm(G_S1, Npc, Npc, 0, 1));
+                SCATT_TRY(gemm(G_S2, Npc, Npc, 0, 0));
+            }
+            k_rev_sym<<<eg, TPB, 0, s>>>(args, 1);
+            SCATT_COUNT_LAUNCH(1);
+            SCATT_TRY(gemm(G_Y1, Npc, Npc, 0, 0));
+            SCATT_TRY(gemm(G_Y2, Npc, Npc, 0, 0));
+            k_rev_vbar<<<n, TPB, 0, s>>>(args, m);
+            SCATT_COUNT_LAUNCH(1);
+            if (vfull) {
+                k_rev_vfull<<<cdiv((long)b.Np_max * b.Np_max, TPB), TPB, 0, s>>>(args, m);
+                SCATT_COUNT_LAUNCH(1);
+            }
+            SCATT_CUDA_TRY(cudaGetLastError());
+        }
+    }
+    // segment mode off again
+    for (int e = 0; e < n; ++e) sc.ed[e].seg_lo = sc.ed[e].seg_hi = 0;
+    SCATT_CUDA_TRY(cudaMemcpyAsync(sc.d_ed.p, sc.ed.data(), n * sizeof(EnergyDev), cudaMemcpyHostToDevice, s));
+    b.n_stop = b.Nr;
+    if (vtr_host) {
+        for (int i = 0; i < A.n_energy; ++i) {
+            const int e = A.slot_of[i];
+            SCATT_CUDA_TRY(cudaMemcpyAsync(vtr_host + (size_t)i * b.Nr, A.slot[e].vtr, b.Nr * sizeof(double),
+                                           cudaMemcpyDeviceToHost, s));
+        }
+    }
+    SCATT_CUDA_TRY(cudaStreamSynchronize(s));
+    return SCATT_OK;
+}
+
 }  // namespace scatt
 
 // ================================================================ C ABI
@@ -2499,6 +3152,104 @@ int scatt_scan_close(scatt_scan* sc) {
     cudaSetDevice(sc->ctx->c.device);
     cudaStreamSynchronize(sc->ctx->c.stream);
     delete sc;
+    return SCATT_OK;
+}
+
+// ---------------------------------------------------------------- adjoint
+struct scatt_adjoint {
+    scatt_ctx* ctx = nullptr;
+    Adjoint a;
+};
+
+int scatt_set_polarization(scatt_ctx* ctx, double alpha, double r_c, int pol_form) {
+    if (!ctx || !ctx->c.tab || !ctx->c.tab->ready) return SCATT_ERR_STATE;
+    if (!(r_c > 0.0) || (pol_form != 0 && pol_form != 1) || !std::isfinite(alpha)) return SCATT_ERR_ARG;
+    ScanTables& t = *ctx->c.tab;
+    t.alpha_pol = alpha;
+    t.r_c = r_c;
+    t.pol_form = pol_form;
+    t.stab.clear();            // the stability spectra follow V
+    return SCATT_OK;
+}
+
+int scatt_set_potential_delta(scatt_ctx* ctx, const double* dV) {
+    if (!ctx || !ctx->c.tab || !ctx->c.tab->ready) return SCATT_ERR_STATE;
+    ctx->c.tab->dV = dV;
+    ctx->c.tab->stab.clear();
+    return SCATT_OK;
+}
+
+int scatt_adjoint_forward(scatt_ctx* ctx, const scatt_solve_opts* opts, int n_energy, const double* energies,
+                          const int* l_cont, int segment, const scatt_outputs* outputs, scatt_adjoint** out) {
+    if (!ctx || !energies || !out || n_energy < 1) return SCATT_ERR_ARG;
+    if (!ctx->c.tab || !ctx->c.tab->ready) {
+        set_last_error("scatt_adjoint_forward: upload the static inputs first");
+        return SCATT_ERR_STATE;
+    }
+    SCATT_TRY(require_device());
+    SCATT_CUDA_TRY(cudaSetDevice(ctx->c.device));
+    SCATT_TRY(check_energies(*ctx->c.tab, n_energy, energies, l_cont, "scatt_adjoint_forward"));
+    scatt_solve_opts o;
+    if (opts) o = *opts;
+    else scatt_default_opts(&o);
+    auto* h = new scatt_adjoint();
+    h->ctx = ctx;
+    const int st = adj_forward(ctx->c, o, n_energy, energies, l_cont, segment, outputs, h->a);
+    if (st != SCATT_OK && h->a.slot.empty()) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return st;
+}
+
+int scatt_adjoint_view_of(scatt_adjoint* h, int i, scatt_adjoint_view* v) {
+    if (!h || !v || i < 0 || i >= h->a.n_energy) return SCATT_ERR_ARG;
+    const Adjoint& A = h->a;
+    const BatchDev& b = A.sc.b;
+    const ScanTables& t = *A.sc.ctx->tab;
+    const int e = A.slot_of[i];
+    const EnergyDev& d = A.sc.ed[e];
+    const AdjSlot& S = A.slot[e];
+    std::memset(v, 0, sizeof(*v));
+    v->N = b.N;
+    v->n_s = b.n_s;
+    v->n_window = A.nwin;
+    v->n_tr = b.n_tr;
+    v->n_pts = b.n_pts;
+    v->n_start = b.n_start;
+    v->ne_fit = A.sc.ne_fit;
+    v->Np = d.Np;
+    v->Nt = d.Nt;
+    v->Nf = b.Nf;
+    v->Krows = b.Krows;
+    v->Np_max = b.Np_max;
+    v->l_cont = d.l_cont;
+    v->E = d.E;
+    v->Rwin = d.tailR;
+    v->Swin = d.tailS;
+    v->G_last = (b.N & 1) ? d.G1 : d.G0;
+    v->RBwin = S.RBw;
+    v->SBwin = S.SBw;
+    v->GB_last = ((b.N - 1) & 1) ? S.GB1 : S.GB0;
+    v->V_N = A.vbN.V.p;
+    v->B_N = A.vbN.B.p;
+    v->Bs_N = A.vbN.Bs.p;
+    v->C_N = (b.N < b.n_pts) ? t.Ctab.p + (size_t)b.N * b.Krows * b.Np_max : nullptr;
+    v->Bs_win = A.bswin.p;
+    return SCATT_OK;
+}
+
+int scatt_adjoint_reverse(scatt_adjoint* h, double* vtr, double* vfull_device) {
+    if (!h) return SCATT_ERR_ARG;
+    SCATT_CUDA_TRY(cudaSetDevice(h->ctx->c.device));
+    return adj_reverse(h->a, vtr, vfull_device);
+}
+
+int scatt_adjoint_close(scatt_adjoint* h) {
+    if (!h) return SCATT_OK;
+    cudaSetDevice(h->ctx->c.device);
+    delete h;
     return SCATT_OK;
 }
 

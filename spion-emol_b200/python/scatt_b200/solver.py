@@ -114,6 +114,8 @@ class ScanSolver:
         self._ctx = C.c_void_p()
         check(lib().scatt_ctx_create(device, C.byref(self._ctx)))
         self.inp = inp
+        self.dr = float(inp.dr)
+        self.device = int(device)
         self.l_cont_max = inp.l_cont if l_cont_max is None else l_cont_max
         self._keep = []
         psi = np.ascontiguousarray(inp.psi_lm, dtype=np.float64)
@@ -146,10 +148,12 @@ class ScanSolver:
         self._ctx = C.c_void_p()
         check(lib().scatt_ctx_create(device, C.byref(self._ctx)))
         self.inp = None
+        self.device = int(device)
         self.l_cont_max = int(l_cont_max)
         self._keep = []
         with Preproc(path) as pp:
             d, self.E_init = pp.desc(l_cont_max)
+            self.dr = float(pp.dr)
             d.n_transition = n_transition
             self._upload(d)                  # copies to the device before the file's buffers go
             self.preproc = {k: getattr(pp, k) for k in ("Nr", "dr", "Lmax_sce", "n_alpha", "n_occ", "n_sce",
