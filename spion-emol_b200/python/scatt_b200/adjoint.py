@@ -342,6 +342,10 @@ class Dipoles(torch.autograd.Function):
             out = torch.stack([torch.view_as_real(D) for D in Ds])
         ctx.adj, ctx.out, ctx.pol_form = adj, out, int(pol_form)
         ctx.solver = solver
+        # the reverse pass recomputes V(n) from the values of this forward
+        # (V_pol parameters and dV are copied into the batch; dV's memory is
+        # read again and must stay as it is until backward)
+        ctx.dV = dV
         ctx.save_for_backward(alpha, r_c)
         ctx.has_dV = dV is not None
         return out.detach().clone()
