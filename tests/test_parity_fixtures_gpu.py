@@ -1,0 +1,81 @@
+"""GPU results against oracle fixtures at the benchmark shapes.
+
+tests/golden/make_parity_fixtures.py solves each case with the oracle in
+both of its LAPACK builds (partial-pivot LU, and dsytrf/dsytri); their
+spread per observable is the rounding floor of the case.  Each GPU
+observable must agree with the oracle to max(1e-10, 10 x that floor)
+relative to the observable's largest entry.  Matrices above 100 rows are
+compared through products with the fixture's four random vectors and their
+diagonals.  A case or energy missing from the fixture file is skipped.
+"""
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+
+from scatt_b200 import solver as S
+from scatt_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_spec = importlib.util.spec_from_file_location("make_parity_fixtures",
+                                               os.path.join(HERE, "golden", "make_parity_fixtures.py"))
+F = importlib.util.module_from_spec(_spec)
+_spec.loader.exec_module(F)
+
+# observables compared, with the GPU result's counterpart of each fixture key
+MATS = ("K_kme", "A", "B", "K_aa")
+
+
+def _gpu_record(r, V):
+    out = {}
+    for name, M in (("K_kme", r.K_kme), ("A", r.A), ("B", r.B), ("K_aa", r.K_aa)):
+        for k, v in F.reduce_matrix(M, V).items():
+            out[f"{name}.{k}"] = v
+    out["b_overlap"] = r.b_overlap
+    for key in ("D", "D_raw", "d_raw", "d_corr", "partial_sigma"):
+        out[key] = getattr(r, key)
+    out["eig_kme"] = np.sort(r.eig_kme)                 # eigenphases atan(eig K)
+    out["shifts"] = np.array([r.diag["shifts_A"], r.diag["shifts_S"]])
+    out["n_closed_l"] = np.array(r.diag["n_closed_l"])
+    return out
+
+
+def _rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(float(np.max(np.abs(b))), 1e-300))
+
+
+@pytest.mark.parametrize("case", list(F.CASES))
+def test_gpu_matches_oracle_fixture(case):
+    path = os.path.join(HERE, "golden", f"parity_{case}.npz")
+    if not os.path.exists(path):
+        pytest.skip(f"no fixture for {case}")
+    fx = dict(np.load(path))
+    cfg = F.CASES[case]
+    # energies solved in both builds (the floor needs the pair)
+    ks = [k for ik, k in enumerate(cfg["ks"]) if f"e{ik}/eigen/D" in fx and f"e{ik}/mkl/D" in fx]
+    if not ks:
+        pytest.skip(f"fixture for {case} holds no energy yet")
+    inp = getattr(synth, cfg["builder"])(**cfg["kw"])
+    sol = S.ScanSolver(inp)
+    assert sol.n_transition == int(fx["n_tr"]) and sol.Np + sol.Nf == int(fx["Nt"])
+    res = sol.solve([0.5 * k * k for k in ks], opts=S.default_opts(allow_closed_channels=1))
+    V = fx["proj_vectors"]
+    worst = {}
+    for r, k in zip(res, ks):
+        ik = cfg["ks"].index(k)
+        got = _gpu_record(r, V)
+        for key, g in got.items():
+            ref = fx[f"e{ik}/eigen/{key}"]
+            if key in ("shifts", "n_closed_l"):
+                assert np.array_equal(np.asarray(g), ref), (case, k, key)
+                continue
+            floor = _rel(fx[f"e{ik}/mkl/{key}"], ref)
+            tol = max(1e-10, 10.0 * floor)
+            err = _rel(g, ref)
+            worst[key] = max(worst.get(key, 0.0), err)
+            assert err <= tol, (case, k, key, err, tol)
+    print(case, {k: f"{v:.2e}" for k, v in sorted(worst.items())})
