@@ -58,6 +58,36 @@ CONFIGS = {
 INVERSE_TRAFFIC: dict = {}
 
 
+# Device seconds of one chunk (8 radial steps) with every slot busy, measured
+# on one B200 in FP64 for the default slot counts; the wall-time prediction
+# below scales them by the slot count.
+CHUNK_S = {"h2o_like": (32, 0.0556), "h2_like": (20, 0.0052)}
+
+
+def plan(config: str, slots: int, groups: int, steps: int, warmup: int) -> dict:
+    """Chunks of 8 radial steps the bench runs.  The first step ends when
+    group 0 has swept the whole grid (the later groups start 1/groups of a
+    sweep apart); every later step is one group finishing, 1/groups of a
+    sweep.  Warm-up steps come first."""
+    Nr = CONFIGS[config]["kw"]["Nr"]
+    cps = -(-Nr // 8)                        # a sweep covers n = 0 .. N = Nr - 1
+    per_step = -(-cps // groups)
+    n_steps = warmup + steps
+    total = (cps + (n_steps - 1) * per_step) if n_steps > 0 else 0
+    return {"chunks_per_sweep": cps, "chunks_first_step": cps, "chunks_per_step": per_step,
+            "chunks_total": total, "chunks_timed": steps * per_step if warmup > 0 else total}
+
+
+def predict_seconds(config: str, slots: int, groups: int, steps: int, warmup: int, setup_s: float = 120.0,
+                    cpu_s: float = 30.0) -> float:
+    """Wall time of `bench.py --config C --steps K --warmup W`: the chunks at
+    the measured cost per chunk (a slot-count multiple of it), post stages
+    included in that cost, plus setup (upload, cuBLAS peak, autotune) and
+    the CPU baseline."""
+    s0, c0 = CHUNK_S[config]
+    return setup_s + cpu_s + plan(config, slots, groups, steps, warmup)["chunks_total"] * c0 * slots / s0
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -1,0 +1,32 @@
+"""The bench's shape: what the driver's `--steps 20 --warmup 5` runs, and
+that it ends well inside the driver's 1800 s limit at the measured cost of a
+chunk of radial steps (bench.CHUNK_S)."""
+import importlib.util
+import os
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+_spec = importlib.util.spec_from_file_location("bench", os.path.join(ROOT, "bench.py"))
+bench = importlib.util.module_from_spec(_spec)
+_spec.loader.exec_module(bench)
+
+
+def test_step_is_one_group_of_a_staggered_sweep():
+    p = bench.plan("h2o_like", 32, 8, steps=20, warmup=5)
+    assert p["chunks_per_sweep"] == 1501                  # 12001 points, 8 per chunk
+    assert p["chunks_per_step"] == 188
+    assert p["chunks_total"] == 1501 + 24 * 188
+    assert p["chunks_timed"] == 20 * 188
+
+
+def test_driver_run_fits_with_margin():
+    for cfg in ("h2o_like", "h2_like"):
+        c = bench.CONFIGS[cfg]
+        t = bench.predict_seconds(cfg, c["slots"], c["groups"], steps=20, warmup=5)
+        assert t <= 1500.0, (cfg, t)
+    # the lock-step batch the earlier bench ran (one group) would not fit
+    assert bench.predict_seconds("h2o_like", 32, 1, steps=20, warmup=5) > 1800.0
+
+
+def test_default_run_is_short():
+    c = bench.CONFIGS["h2o_like"]
+    assert bench.predict_seconds("h2o_like", c["slots"], c["groups"], steps=8, warmup=3) <= 600.0
