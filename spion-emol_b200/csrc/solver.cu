@@ -347,7 +347,8 @@ __global__ void k_stab(BatchDev b, int which) {
         double delta = 0.0;
         if (me < b.W_min) {
             delta = b.W_min - me + b.margin;
-            if (which == 0) d.shiftsA += 1; else d.shiftsS += 1;
+            // the chunk's steps run in parallel blocks of this slot: count atomically
+            atomicAdd(which == 0 ? &d.shiftsA : &d.shiftsS, 1);
         }
         if (which == 0) d.deltaAc[slot] = delta;
         if (d.stabd) d.stabd[2 * n + which] = delta;

@@ -94,13 +94,17 @@ def test_scan_mixed_l_cont():
 
 
 def test_scan_rejects_bad_requests():
-    inp = synth.h2_like(Nr=401, dr=0.05, l_cont=3)
+    # l_cont 11 uploaded: the exchange cutoff min(l, 10) = 10 is shared, so a
+    # scan may be opened at l_cont_max 10 and 11 but not below 10
+    inp = synth.h2o_like(Nr=301, dr=0.05, l_cont=11, lmax_orb=8, n_orb=2)
     sol = S.ScanSolver(inp)
     with pytest.raises(Exception):
         sol.scan(slots=2, groups=65)
-    scan = sol.scan(slots=2, groups=1, l_cont_max=2)
     with pytest.raises(Exception):
-        scan.submit([0.5], l_cont=[3])          # above the scan's l_cont_max
+        sol.scan(slots=2, groups=1, l_cont_max=9)
+    scan = sol.scan(slots=2, groups=1, l_cont_max=10)
+    with pytest.raises(Exception):
+        scan.submit([0.5], l_cont=[11])         # above the scan's l_cont_max
     with pytest.raises(Exception):
         scan.submit([-0.1])
     assert scan.step() == []                    # nothing queued
