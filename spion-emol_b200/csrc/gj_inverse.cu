@@ -1320,25 +1320,23 @@ int launch_panel(int pcfg, int count, int pt, size_t smem, cudaStream_t stream, 
     return SCATT_OK;
 }
 
-// Side stream (highest priority) and two events per device for the
-// look-ahead of the row-contiguous inverse; created once per device.  The
-// enqueueing of one inverse holds the mutex, so its event record / wait pairs
-// cannot interleave with another thread's.
+// Side stream (highest priority) and two events per (device, main stream)
+// for the look-ahead of the row-contiguous inverse, created on first use.
+// Inverses enqueued on different streams (the phase groups of a scan) get
+// different side streams, so their look-ahead chains do not queue behind
+// one another.  The enqueueing of one inverse holds the mutex, so its event
+// record / wait pairs cannot interleave with another thread's.
 struct LookAhead {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_main = nullptr, ev_side = nullptr;
 };
 std::mutex g_la_mutex;
-LookAhead g_la[64];
+std::map<std::pair<int, cudaStream_t>, LookAhead> g_la;
 
-int look_ahead_resources(LookAhead** out) {
+int look_ahead_resources(cudaStream_t main, LookAhead** out) {
     int dev = 0;
     SCATT_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) {
-        set_last_error("look-ahead inverse: device ordinal out of range");
-        return SCATT_ERR_ARG;
-    }
-    LookAhead& r = g_la[dev];
+    LookAhead& r = g_la[std::make_pair(dev, main)];
     if (!r.side) {
         int lo = 0, hi = 0;
         SCATT_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
@@ -1530,7 +1528,7 @@ int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax, bool sy
     } else {
         std::lock_guard<std::mutex> lock(g_la_mutex);
         LookAhead* la = nullptr;
-        SCATT_TRY(look_ahead_resources(&la));
+        SCATT_TRY(look_ahead_resources(stream, &la));
         SCATT_TRY(chain(0, stream, 1));
         for (int K = 0; K < outer; ++K) {
             if (K + 1 < outer) {
