@@ -59,9 +59,10 @@ INVERSE_TRAFFIC: dict = {}
 
 
 # Device seconds of one chunk (8 radial steps) with every slot busy, measured
-# on one B200 in FP64 for the default slot counts; the wall-time prediction
-# below scales them by the slot count.
-CHUNK_S = {"h2o_like": (32, 0.0556), "h2_like": (20, 0.0052)}
+# on one B200 in FP64 (H2O-like: 32 slots in 8 groups, 10.77 s per step of
+# 188 chunks; H2-like: 20 slots in 4 groups without graphs, 0.40 s per step of
+# 126 chunks); the wall-time prediction below scales them by the slot count.
+CHUNK_S = {"h2o_like": (32, 0.0573), "h2_like": (20, 0.0032)}
 
 
 def plan(config: str, slots: int, groups: int, steps: int, warmup: int) -> dict:
