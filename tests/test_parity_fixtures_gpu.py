@@ -3,8 +3,9 @@
 tests/golden/make_parity_fixtures.py solves each case with the oracle in
 both of its LAPACK builds (partial-pivot LU, and dsytrf/dsytri); their
 spread per observable is the rounding floor of the case.  Each GPU
-observable must agree with the oracle to max(1e-10, 10 x that floor)
-relative to the observable's largest entry; K (both extractions), A, B
+observable must agree with the nearer of the two builds (either is a
+reference path) to max(1e-10, 10 x that floor) relative to the
+observable's largest entry; K (both extractions), A, B
 and the overlaps derive from one boundary value psi_N = J + Y K and share
 the largest of their floors, as in test_parity_gpu.  Matrices above 100 rows are
 compared through products with the fixture's four random vectors and their
@@ -81,7 +82,7 @@ def test_gpu_matches_oracle_fixture(case):
             if key in coupled_keys:
                 floor = max(floor, coupled)
             tol = max(1e-10, 10.0 * floor)
-            err = _rel(g, ref)
+            err = min(_rel(g, ref), _rel(g, fx[f"e{ik}/mkl/{key}"]))
             worst[key] = max(worst.get(key, 0.0), err)
             assert err <= tol, (case, k, key, err, tol)
     print(case, {k: f"{v:.2e}" for k, v in sorted(worst.items())})
