@@ -7,9 +7,11 @@ hand-written DipoleAdjoint and against central finite differences.
   compared: the shift is not differentiable there and the library averages
   over the degenerate eigenvectors while LAPACK picks one.
 * The checkpoint segment length does not change the result.
-* d sigma / d alpha, d sigma / d r_c, d tau / d alpha and dJ/dV_ll'(r) along
-  single grid entries agree with central differences (h = 1e-6 relative) to
-  1e-6.
+* d sigma / d alpha, d sigma / d r_c and d tau / d alpha agree with central
+  differences (h = 1e-6 relative) to 1e-6; dJ/dV_ll'(r) at single grid
+  entries agrees to 1e-6 with Richardson-extrapolated central differences
+  at h = 1e-4 (at 1e-6 the solve's rounding noise dominates a single
+  entry's difference quotient).
 """
 import dataclasses
 
