@@ -297,10 +297,9 @@ def main():
 
     tuned = []
     if a.autotune:
-        # the scan's batches (one per phase group, each on its own stream): R^-1
-        # of order N_t over a group's slots, and the Schur inverses of order Np
-        # over its slots' 8 radial steps of a chunk
-        for n, count in sorted({(sol.Np + sol.Nf, gsize), (sol.Np, gsize * 8)}):
+        # the scan's batches: R^-1 of order N_t over the slots, and the Schur
+        # inverses of order Np over the slots' 8 radial steps of a chunk
+        for n, count in sorted({(sol.Np + sol.Nf, slots), (sol.Np, slots * 8)}):
             tuned.append(_lib.autotune_inverse(n, count, device=local))
     peak = cuda_dgemm_peak(torch) if rank == 0 else None
     alloc, _keep = pinned_alloc(torch)

@@ -30,8 +30,6 @@
 #include <cstring>
 #include <deque>
 #include <map>
-#include <memory>
-#include <tuple>
 #include <string>
 #include <vector>
 
@@ -1289,95 +1287,73 @@ struct Job {
     long index;       // submission index
 };
 
-}  // namespace
-
-// Post-stage resources of one phase group (its stream, buffers for its slots).
-struct GroupPost {
-    cudaStream_t s = nullptr;
-    Launcher L{nullptr};
-    std::vector<PostBufs> P;            // one per slot of the group
-    VBAt vb;                            // V/B at one step for the post stages
-    DevBuf<double> parena;
-    DevBuf<int> pia;
+// CUDA events created once per scan and destroyed with it, so no early
+// return leaks one.
+struct EventPool {
+    std::vector<cudaEvent_t> ev;
+    size_t used = 0;
+    ~EventPool() {
+        for (auto e : ev) cudaEventDestroy(e);
+    }
+    int get(cudaEvent_t* out) {
+        if (used == ev.size()) {
+            cudaEvent_t e;
+            SCATT_CUDA_TRY(cudaEventCreate(&e));
+            ev.push_back(e);
+        }
+        *out = ev[used++];
+        return SCATT_OK;
+    }
+    void reset() { used = 0; }
 };
 
+}  // namespace
+
 // A scan: `slots` energies in flight in `ngroups` phase groups; energies
-// wait in a queue and enter a group whenever the group is free.  Each group
-// is its own lock-step batch on its own stream (G > 1), so a group in the
-// cheap outer region does not wait for one inside the exchange region, and
-// the latency-bound inverse chains of different groups overlap on the GPU.
+// wait in a queue and enter a group whenever the group is free.
 struct Scan {
     Context* ctx = nullptr;
     scatt_solve_opts o{};
-    BatchDev b{};                       // scan-wide constants (count = slots)
+    BatchDev b{};
     int slots = 0, G = 1, gs = 1;
     int l_cap = 0, Np_cap = 0, Nt_cap = 0;
     int chunks_per_sweep = 0;
     std::vector<EnergyDev> ed;          // host copy of the slot state (pointers fixed at open)
     std::vector<GroupDev> grp;          // host mirror of the group state
     std::vector<long> job_of;           // submission index held by each slot (-1 empty)
-    std::vector<long> start_chunk;      // chunks of group 0 after which each idle group may start
+    std::vector<long> start_chunk;      // first chunk at which each idle group may start
     std::deque<Job> queue;
-    long chunk = 0;                     // chunks enqueued for group 0 (the stagger clock)
+    long chunk = 0;
     long submitted = 0;
     DevBuf<EnergyDev> d_ed;
     DevBuf<GroupDev> d_grp;
-    DevBuf<double> arena, garena;
-    DevBuf<int> iarena;
-    // per group: its batch view (count = its slots, ngroups = 1), stream, entry arrays, post resources
-    std::vector<BatchDev> gb;
-    std::vector<cudaStream_t> gstream;
-    bool own_streams = false;
-    std::vector<DevBuf<GemmEntry>> ggm;
-    std::vector<DevBuf<GjEntry>> ggj;
-    std::vector<std::unique_ptr<GroupPost>> gpost;
-    // flow control: events after each enqueued chunk (at most `ahead` per group)
-    std::vector<std::deque<cudaEvent_t>> inflight;
-    std::vector<cudaEvent_t> done_ev;   // recorded after a group's last chunk
-    std::vector<char> done_rec;
-    std::vector<cudaEvent_t> free_ev;
-    std::vector<cudaEvent_t> all_ev;
-    cudaEvent_t last_end = nullptr;     // device clock at the end of the previous step
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> rinv_pending;   // sampled R^-1 timings
-    std::vector<double> rinv_pending_flops;
-    int ahead = 8;
-    int nfit = 0, ne_fit = 0;           // the amplitude fit window
+    DevBuf<double> arena, garena, parena;
+    DevBuf<int> iarena, pia;
+    DevBuf<GemmEntry> gm;
+    DevBuf<GjEntry> gj;
+    VBAt vb;                            // V/B at one step for the post stages
+    std::vector<PostBufs> P;            // gs energies
     std::vector<DevBuf<double>> keep;   // stability spectra per l_cont
     std::vector<std::pair<int, std::pair<const double*, const double*>>> stab_ptr;
+    EventPool events;
+    Launcher L{nullptr};
+    int nfit = 0, ne_fit = 0;
     struct Graph {
         cudaGraphExec_t exec;
         unsigned long long launches;    // kernels per replay
     };
-    std::map<std::tuple<int, uint64_t, int>, Graph> graphs;   // (group, stage pattern, stop step) -> replay
+    std::map<std::pair<uint64_t, int>, Graph> graphs;   // (stage pattern, stop step) -> replay
     Scan() = default;
     Scan(const Scan&) = delete;
     Scan& operator=(const Scan&) = delete;
-    int event(cudaEvent_t* out) {
-        if (free_ev.empty()) {
-            cudaEvent_t e;
-            SCATT_CUDA_TRY(cudaEventCreate(&e));
-            all_ev.push_back(e);
-            free_ev.push_back(e);
-        }
-        *out = free_ev.back();
-        free_ev.pop_back();
-        return SCATT_OK;
-    }
-    void release(cudaEvent_t e) { free_ev.push_back(e); }
     ~Scan() {
         for (auto& g : graphs) cudaGraphExecDestroy(g.second.exec);
-        if (own_streams)
-            for (auto st : gstream) {
-                cudaStreamSynchronize(st);
-                cudaStreamDestroy(st);
-            }
-        for (auto e : all_ev) cudaEventDestroy(e);
     }
 };
 
 namespace {
 
-int gemm_slots(Scan& sc, int g, GemmEntry* ents, int count, int which, int opA, int opB) {
+int gemm_slots(Scan& sc, GemmEntry* ents, int count, int which, int opA, int opB) {
     const int Np = sc.Np_cap, Nt = sc.Nt_cap, Nf = sc.b.Nf, K = sc.b.Krows;
     int M = 0, N = 0;
     switch (which) {
@@ -1388,7 +1364,7 @@ int gemm_slots(Scan& sc, int g, GemmEntry* ents, int count, int which, int opA, 
         case 4: M = K; N = Nf; break;        // G2
         case 5: M = K; N = Nt; break;        // G3
     }
-    return gemm_batched(ents, count, M, N, opA, opB, sc.gstream[g]);
+    return gemm_batched(ents, count, M, N, opA, opB, sc.ctx->stream);
 }
 
 int stab_for(Scan& sc, int l_cont, const double** lmA, const double** lmS) {
@@ -1413,6 +1389,7 @@ int scan_open(Context& ctx, const scatt_solve_opts& o, int slots, int ngroups, i
     }
     sc.ctx = &ctx;
     sc.o = o;
+    sc.L.s = s;
     BatchDev& b = sc.b;
     SCATT_TRY(make_consts(t, o, b));
     sc.slots = slots;
@@ -1468,7 +1445,7 @@ int scan_open(Context& ctx, const scatt_solve_opts& o, int slots, int ngroups, i
         d.stR = q; q += 4;
         d.sgS = q; q += SCHUR_CHUNK * 4 * Np;
         d.sgR = q; q += 4 * Nt;
-        d.grp = 0;                 // index into its group's batch view (b.grp of that view)
+        d.grp = e / sc.gs;
         d.live = 0;
     }
     SCATT_TRY(upload_vec(sc.d_ed, sc.ed, s));
@@ -1495,48 +1472,26 @@ int scan_open(Context& ctx, const scatt_solve_opts& o, int slots, int ngroups, i
     // staggered starts: group g first starts g / G of a sweep after group 0
     sc.start_chunk.assign(ngroups, 0);
     for (int g = 0; g < ngroups; ++g) sc.start_chunk[g] = (long)g * sc.chunks_per_sweep / ngroups;
-    // ---- per group: stream, batch view, entry arrays, post buffers
-    sc.gb.assign(ngroups, b);
-    sc.gstream.assign(ngroups, s);
-    sc.own_streams = ngroups > 1;
-    if (sc.own_streams)
-        for (int g = 0; g < ngroups; ++g) {
-            SCATT_CUDA_TRY(cudaStreamCreateWithFlags(&sc.gstream[g], cudaStreamNonBlocking));
-        }
-    sc.ggm.resize(ngroups);
-    sc.ggj.resize(ngroups);
-    sc.inflight.assign(ngroups, {});
-    sc.done_ev.assign(ngroups, nullptr);
-    sc.done_rec.assign(ngroups, 0);
-    sc.gpost.clear();
-    const int Np = sc.Np_cap, Nt = sc.Nt_cap;
-    const size_t pd = post_doubles(b, Np, Nt, l_cap, sc.nfit, t.n_occ);
-    const size_t np2 = (size_t)Np * Np;
-    for (int g = 0; g < ngroups; ++g) {
-        const int e0 = g * sc.gs, cnt = std::max(0, std::min(slots, e0 + sc.gs) - e0);
-        BatchDev& B = sc.gb[g];
-        B.count = cnt;
-        B.ngroups = 1;
-        B.ed = sc.d_ed.p + e0;
-        B.grp = sc.d_grp.p + g;
-        SCATT_TRY(sc.ggm[g].alloc((5 + SCHUR_CHUNK) * (size_t)std::max(cnt, 1)));
-        SCATT_TRY(sc.ggj[g].alloc((1 + SCHUR_CHUNK) * (size_t)std::max(cnt, 1)));
-        GemmEntry* gm = sc.ggm[g].p;
-        B.gmT = gm; B.gmF = gm + cnt;
-        B.gmG1 = gm + 2 * cnt; B.gmG2 = gm + 3 * cnt; B.gmG3 = gm + 4 * cnt;
-        B.gmS = gm + 5 * cnt;                          // SCHUR_CHUNK x cnt
-        B.gjR = sc.ggj[g].p; B.gjS = sc.ggj[g].p + cnt;
-        auto gp = std::make_unique<GroupPost>();
-        gp->s = sc.gstream[g];
-        gp->L.s = sc.gstream[g];
-        SCATT_TRY(gp->vb.alloc(b));
-        SCATT_TRY(gp->parena.alloc(pd * std::max(cnt, 1)));
-        SCATT_TRY(gp->pia.alloc((4 * (size_t)Np + 8) * std::max(cnt, 1)));
-        gp->P.assign(cnt, PostBufs{});
-        for (int i = 0; i < cnt; ++i) {
-            double* p = gp->parena.p + pd * i;
-            int* q = gp->pia.p + (4 * (size_t)Np + 8) * i;
-            PostBufs& x = gp->P[i];
+    // ---- entry arrays
+    SCATT_TRY(sc.gm.alloc((5 + SCHUR_CHUNK) * (size_t)slots));
+    SCATT_TRY(sc.gj.alloc((1 + SCHUR_CHUNK) * (size_t)slots));
+    b.gmT = sc.gm.p; b.gmF = sc.gm.p + slots;
+    b.gmG1 = sc.gm.p + 2 * slots; b.gmG2 = sc.gm.p + 3 * slots; b.gmG3 = sc.gm.p + 4 * slots;
+    b.gmS = sc.gm.p + 5 * slots;                   // SCHUR_CHUNK x slots
+    b.gjR = sc.gj.p; b.gjS = sc.gj.p + slots;      // gjS: SCHUR_CHUNK x slots
+    // ---- post-stage buffers for one group
+    SCATT_TRY(sc.vb.alloc(b));
+    {
+        const int Np = sc.Np_cap, Nt = sc.Nt_cap;
+        const size_t pd = post_doubles(b, Np, Nt, l_cap, sc.nfit, t.n_occ);
+        SCATT_TRY(sc.parena.alloc(pd * sc.gs));
+        SCATT_TRY(sc.pia.alloc((4 * (size_t)Np + 8) * sc.gs));
+        sc.P.assign(sc.gs, PostBufs{});
+        const size_t np2 = (size_t)Np * Np;
+        for (int i = 0; i < sc.gs; ++i) {
+            double* p = sc.parena.p + pd * i;
+            int* q = sc.pia.p + (4 * (size_t)Np + 8) * i;
+            PostBufs& x = sc.P[i];
             x.tab = p; p += 6 * Np;
             x.Amat = p; p += np2; x.Bmat = p; p += np2; x.Bw = p; p += np2; x.Binv = p; p += np2;
             x.Kraw = p; p += np2; x.K = p; p += np2; x.psibc = p; p += np2; x.VP = p; p += np2;
@@ -1557,7 +1512,6 @@ int scan_open(Context& ctx, const scatt_solve_opts& o, int slots, int ngroups, i
             x.Kc = p; p += 2 * np2;
             x.sig = q; q += 2 * Np; x.rid = q; q += 2 * Np; x.st = q; q += 8;
         }
-        sc.gpost.push_back(std::move(gp));
     }
     SCATT_CUDA_TRY(cudaStreamSynchronize(s));
     return SCATT_OK;
@@ -1567,7 +1521,7 @@ int scan_open(Context& ctx, const scatt_solve_opts& o, int slots, int ngroups, i
 // at n = 0 (no-op when the queue is empty).
 int load_group(Scan& sc, int g) {
     if (sc.queue.empty()) return SCATT_OK;
-    cudaStream_t s = sc.gstream[g];
+    cudaStream_t s = sc.ctx->stream;
     const int e0 = g * sc.gs, e1 = std::min(sc.slots, e0 + sc.gs);
     const BatchDev& b = sc.b;
     for (int e = e0; e < e1; ++e) {
@@ -1597,61 +1551,61 @@ int load_group(Scan& sc, int g) {
     // a pageable copy: the host copy may change as soon as the call returns
     SCATT_CUDA_TRY(cudaMemcpyAsync(sc.d_ed.p + e0, sc.ed.data() + e0, (size_t)(e1 - e0) * sizeof(EnergyDev),
                                    cudaMemcpyHostToDevice, s));
-    k_set_group<<<1, 1, 0, s>>>(sc.gb[g], 0, 0);
+    k_set_group<<<1, 1, 0, s>>>(sc.b, g, 0);
     SCATT_COUNT_LAUNCH(1);
     sc.grp[g].n0 = 0;
-    sc.grp[g].C = std::min(SCHUR_CHUNK, sc.gb[g].n_stop);
-    sc.done_rec[g] = 0;
+    sc.grp[g].C = std::min(SCHUR_CHUNK, b.n_stop);
     return SCATT_OK;
 }
 
 struct ChunkTiming {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> rinv;   // sampled R^-1 inversions
-    std::vector<double> flops;                                // 2 n^3 over each one's matrices
+    double flops = 0.0;                                       // 2 n^3 over their matrices
 };
 
-// One chunk of SCHUR_CHUNK radial steps of group g, on the group's stream.
-// With opts.use_graphs the chunk's launches are replayed from a CUDA graph:
-// every kernel reads its radial step from the device-resident group state
-// and its entries from device-side preparation, so one captured graph
-// serves every chunk of the group that needs the same stages at each chunk
-// position.
-int run_chunk(Scan& sc, int g, ChunkTiming* tm) {
-    BatchDev& b = sc.gb[g];
-    cudaStream_t s = sc.gstream[g];
-    const int count = b.count, Nf = b.Nf, e0 = g * sc.gs;
-    GroupDev& gr = sc.grp[g];
-    if (gr.n0 < 0 || count == 0) return SCATT_OK;
-    // what the group needs at each chunk position (host mirror)
+// One chunk of SCHUR_CHUNK radial steps for every running group.  With
+// opts.use_graphs the chunk's launches are replayed from a CUDA graph: every
+// kernel reads its radial step from the device-resident group state and its
+// entries from device-side preparation, so one captured graph serves every
+// chunk whose running groups need the same stages at each chunk position.
+int run_chunk(Scan& sc, ChunkTiming* tm) {
+    BatchDev& b = sc.b;
+    cudaStream_t s = sc.ctx->stream;
+    const int count = sc.slots, G = sc.G, Nf = b.Nf;
+    // what the running groups need at each chunk position (host mirror)
     bool step[SCHUR_CHUNK] = {}, exch[SCHUR_CHUNK] = {}, start[SCHUR_CHUNK] = {}, rinv[SCHUR_CHUNK] = {};
     bool sweep[SCHUR_CHUNK] = {}, pts[SCHUR_CHUNK] = {};
     bool stab = false, stab_x = false, any_exch = false;
-    int live = 0;
-    for (int e = e0; e < e0 + count; ++e) live += sc.ed[e].live;
-    for (int j = 0; j < gr.C; ++j) {
-        const int n = gr.n0 + j;
-        step[j] = true;
-        const bool x = n < b.n_tr && Nf > 0;
-        exch[j] = x;
-        any_exch |= x;
-        start[j] = n < b.n_start;
-        rinv[j] = n >= b.n_start;
-        sweep[j] = n <= b.N - 1;
-        pts[j] = n < b.n_pts && n <= b.N - 1;
-        stab |= n < b.stab_n;
-        stab_x |= n < b.stab_n && x;
+    int live_rinv[SCHUR_CHUNK] = {};
+    std::vector<int> live_in(G, 0);
+    for (int e = 0; e < count; ++e) live_in[sc.ed[e].grp] += sc.ed[e].live;
+    for (int g = 0; g < G; ++g) {
+        const GroupDev& gr = sc.grp[g];
+        if (gr.n0 < 0) continue;
+        for (int j = 0; j < gr.C; ++j) {
+            const int n = gr.n0 + j;
+            step[j] = true;
+            const bool x = n < b.n_tr && Nf > 0;
+            exch[j] |= x;
+            any_exch |= x;
+            start[j] |= n < b.n_start;
+            if (n >= b.n_start) { rinv[j] = true; live_rinv[j] += live_in[g]; }
+            sweep[j] |= n <= b.N - 1;
+            pts[j] |= n < b.n_pts && n <= b.N - 1;
+            stab |= n < b.stab_n;
+            stab_x |= n < b.stab_n && x;
+        }
     }
     // one R^-1 call in two chunks is timed (one in 16 under graphs) while every slot takes part
-    const bool sample_chunk = tm && rinv[0] && live == count &&
-                              (gr.n0 / SCHUR_CHUNK) % (sc.o.use_graphs ? 16 : 2) == 0;
-    const int Np_cap = sc.Np_cap, Nt_cap = sc.Nt_cap;
+    const bool sample_chunk = tm && rinv[0] && live_rinv[0] == count &&
+                              (sc.chunk % (sc.o.use_graphs ? 16 : 2) == 0);
     auto issue = [&]() -> int {
         // ---- Schur complements of the chunk's steps: A(n), S(n) = A - Bs B^T, one batched inverse
-        k_build_V<<<dim3(cdiv(b.n_pairs, TPB), 1, SCHUR_CHUNK), TPB, 0, s>>>(b);
+        k_build_V<<<dim3(cdiv(b.n_pairs, TPB), G, SCHUR_CHUNK), TPB, 0, s>>>(b);
         SCATT_COUNT_LAUNCH(1);
         {
             const int rows = std::max(b.Np_max * b.n_sigma, b.Nf);
-            k_build_B<<<dim3(cdiv(rows, 128), 1, SCHUR_CHUNK), 128, 0, s>>>(b);
+            k_build_B<<<dim3(cdiv(rows, 128), G, SCHUR_CHUNK), 128, 0, s>>>(b);
             SCATT_COUNT_LAUNCH(1);
         }
         k_init_S<<<dim3(64, count, SCHUR_CHUNK), TPB, 0, s>>>(b);
@@ -1659,21 +1613,21 @@ int run_chunk(Scan& sc, int g, ChunkTiming* tm) {
         if (stab) { k_stab<<<dim3(count, SCHUR_CHUNK), TPB, 0, s>>>(b, 0); SCATT_COUNT_LAUNCH(1); }
         k_prepare_schur<<<cdiv(count * SCHUR_CHUNK, 128), 128, 0, s>>>(b);
         SCATT_COUNT_LAUNCH(1);
-        if (any_exch) SCATT_TRY(gemm_slots(sc, g, b.gmS, count * SCHUR_CHUNK, 0, 0, 1));
+        if (any_exch) SCATT_TRY(gemm_slots(sc, b.gmS, count * SCHUR_CHUNK, 0, 0, 1));
         if (stab_x) { k_stab<<<dim3(count, SCHUR_CHUNK), TPB, 0, s>>>(b, 1); SCATT_COUNT_LAUNCH(1); }
-        SCATT_TRY(gj_inverse_selected(b.gjS, count * SCHUR_CHUNK, Np_cap, true, s, true));
+        SCATT_TRY(gj_inverse_selected(b.gjS, count * SCHUR_CHUNK, sc.Np_cap, true, s, true));
         // ---- the R-ratio recurrence over the chunk's steps
         const dim3 eg(64, count);
         for (int j = 0; j < SCHUR_CHUNK; ++j) {
             if (!step[j]) continue;
             k_prepare<<<cdiv(count, 128), 128, 0, s>>>(b, j);
             SCATT_COUNT_LAUNCH(1);
-            if (start[j]) { k_vdiag<<<dim3(cdiv(b.Np_max, 128), 1), 128, 0, s>>>(b, j); SCATT_COUNT_LAUNCH(1); }
+            if (start[j]) { k_vdiag<<<dim3(cdiv(b.Np_max, 128), G), 128, 0, s>>>(b, j); SCATT_COUNT_LAUNCH(1); }
             k_collect<<<cdiv(count, 128), 128, 0, s>>>(b, j, 0);
             SCATT_COUNT_LAUNCH(1);
             if (exch[j]) {
-                SCATT_TRY(gemm_slots(sc, g, b.gmT, count, 1, 0, 0));
-                SCATT_TRY(gemm_slots(sc, g, b.gmF, count, 2, 1, 0));
+                SCATT_TRY(gemm_slots(sc, b.gmT, count, 1, 0, 0));
+                SCATT_TRY(gemm_slots(sc, b.gmF, count, 2, 1, 0));
             }
             if (start[j]) {
                 k_analytic_R<<<eg, TPB, 0, s>>>(b, j);
@@ -1687,30 +1641,28 @@ int run_chunk(Scan& sc, int g, ChunkTiming* tm) {
                 const bool sample = sample_chunk && j == 0;
                 cudaEvent_t a0 = nullptr, a1 = nullptr;
                 if (sample) {
-                    SCATT_TRY(sc.event(&a0));
-                    SCATT_TRY(sc.event(&a1));
+                    SCATT_TRY(sc.events.get(&a0));
+                    SCATT_TRY(sc.events.get(&a1));
                     SCATT_CUDA_TRY(cudaEventRecord(a0, s));
                 }
-                // order N_t at every step: past n_transition the coupling carried by
-                // Rinv(n-1) keeps R from being block-diagonal
-                SCATT_TRY(gj_inverse_selected(b.gjR, count, Nt_cap, true, s, true));
+                SCATT_TRY(gj_inverse_selected(b.gjR, count, sc.Nt_cap, true, s, true));
                 if (sample) {
                     SCATT_CUDA_TRY(cudaEventRecord(a1, s));
                     tm->rinv.push_back({a0, a1});
-                    double f = 0.0;
-                    for (int e = e0; e < e0 + count; ++e) {
+                    // order N_t at every step: past n_transition the coupling
+                    // carried by Rinv(n-1) keeps R from being block-diagonal
+                    for (int e = 0; e < count; ++e) {
                         const double n = sc.ed[e].Nt;
-                        f += 2.0 * n * n * n;
+                        tm->flops += 2.0 * n * n * n;
                     }
-                    tm->flops.push_back(f);
                 }
                 k_collect<<<cdiv(count, 128), 128, 0, s>>>(b, j, 1);
                 SCATT_COUNT_LAUNCH(1);
             }
             if (sweep[j]) {
-                if (pts[j]) SCATT_TRY(gemm_slots(sc, g, b.gmG1, count, 3, 0, 0));
-                if (pts[j] && exch[j]) SCATT_TRY(gemm_slots(sc, g, b.gmG2, count, 4, 0, 0));
-                SCATT_TRY(gemm_slots(sc, g, b.gmG3, count, 5, 0, 0));
+                if (pts[j]) SCATT_TRY(gemm_slots(sc, b.gmG1, count, 3, 0, 0));
+                if (pts[j] && exch[j]) SCATT_TRY(gemm_slots(sc, b.gmG2, count, 4, 0, 0));
+                SCATT_TRY(gemm_slots(sc, b.gmG3, count, 5, 0, 0));
             }
         }
         k_advance<<<1, MAX_GROUPS, 0, s>>>(b);
@@ -1723,22 +1675,22 @@ int run_chunk(Scan& sc, int g, ChunkTiming* tm) {
                               (rinv[j] ? 8u : 0u) | (sweep[j] ? 16u : 0u) | (pts[j] ? 32u : 0u);
         key |= bits << (3 + 6 * j);
     }
-    if (sc.o.use_graphs && !sample_chunk && gr.n0 > 0) {
-        const auto gk = std::make_tuple(g, key, b.n_stop);
+    if (sc.o.use_graphs && !sample_chunk && sc.chunk > 0) {
+        const auto gk = std::make_pair(key, b.n_stop);
         auto it = sc.graphs.find(gk);
         if (it == sc.graphs.end()) {
             SCATT_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
             const unsigned long long l0 = launch_counter();
             const int st = issue();
-            cudaGraph_t gph = nullptr;
-            const cudaError_t ce = cudaStreamEndCapture(s, &gph);
+            cudaGraph_t g = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(s, &g);
             const unsigned long long nl = launch_counter() - l0;
             launch_counter().fetch_sub(nl);          // captured, not launched
-            if (st != SCATT_OK) { if (gph) cudaGraphDestroy(gph); return st; }
-            if (ce != cudaSuccess) { if (gph) cudaGraphDestroy(gph); return cuda_status(ce, "cudaStreamEndCapture"); }
+            if (st != SCATT_OK) { if (g) cudaGraphDestroy(g); return st; }
+            if (ce != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_status(ce, "cudaStreamEndCapture"); }
             cudaGraphExec_t ex = nullptr;
-            const cudaError_t ie = cudaGraphInstantiate(&ex, gph, 0);
-            cudaGraphDestroy(gph);
+            const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+            cudaGraphDestroy(g);
             if (ie != cudaSuccess) return cuda_status(ie, "cudaGraphInstantiate");
             it = sc.graphs.emplace(gk, Scan::Graph{ex, nl}).first;
         }
@@ -1747,10 +1699,13 @@ int run_chunk(Scan& sc, int g, ChunkTiming* tm) {
     } else {
         SCATT_TRY(issue());
     }
-    const int n0 = gr.n0 + gr.C;
-    if (n0 >= b.n_stop) { gr.n0 = -2; gr.C = 0; }      // finished: post stages pending
-    else { gr.n0 = n0; gr.C = std::min(SCHUR_CHUNK, b.n_stop - n0); }
-    if (g == 0) ++sc.chunk;
+    for (auto& gr : sc.grp) {
+        if (gr.n0 < 0) continue;
+        const int n0 = gr.n0 + gr.C;
+        if (n0 >= b.n_stop) { gr.n0 = -2; gr.C = 0; }      // finished: post stages pending
+        else { gr.n0 = n0; gr.C = std::min(SCHUR_CHUNK, b.n_stop - n0); }
+    }
+    ++sc.chunk;
     return SCATT_OK;
 }
 
@@ -1759,19 +1714,19 @@ int run_chunk(Scan& sc, int g, ChunkTiming* tm) {
 // asymptotic window, the amplitude fit and the dipoles.  Outputs go to rows
 // `rows` of `out`.  A failed energy (singular pivot, closed channel) leaves
 // its status in out->status and the first one in *first_status / *first_msg.
-int post_slots(Scan& sc, GroupPost& gp, const std::vector<int>& sel, const std::vector<long>& rows,
-               const scatt_outputs* out, int* first_status, std::string* first_msg) {
+int post_slots(Scan& sc, const std::vector<int>& sel, const std::vector<long>& rows, const scatt_outputs* out,
+               int* first_status, std::string* first_msg) {
     ScanTables& t = *sc.ctx->tab;
     const scatt_solve_opts& o = sc.o;
-    cudaStream_t s = gp.s;
+    cudaStream_t s = sc.ctx->stream;
     BatchDev& b = sc.b;
     const int cnt = (int)sel.size();
     if (cnt == 0) return SCATT_OK;
     const int N = b.N, K = b.Krows, Nf = b.Nf;
     const int ne_fit = sc.ne_fit, nfit = sc.nfit;
     auto ED = [&](int i) -> const EnergyDev& { return sc.ed[sel[i]]; };
-    std::vector<PostBufs>& P = gp.P;
-    Launcher& L = gp.L;
+    std::vector<PostBufs>& P = sc.P;
+    Launcher& L = sc.L;
     int maxNp = 0;
     for (int e = 0; e < cnt; ++e) maxNp = std::max(maxNp, ED(e).Np);
     // the slots' device counters: stability shifts and the first failing step
@@ -1875,15 +1830,15 @@ int post_slots(Scan& sc, GroupPost& gp, const std::vector<int>& sel, const std::
     }
 
     // ---- outer boundary Z_N (BackPropagator.cpp:127-197) and the dipole contraction
-    gp.vb.build(b, N, s);
+    sc.vb.build(b, N, s);
     {
         std::vector<GemmEntry> mv, mf, mb;
         for (int e = 0; e < cnt; ++e) {
             const EnergyDev& d = ED(e);
             const int Np = d.Np;
-            mv.push_back(GemmEntry{gp.vb.V.p, P[e].psibc, P[e].VP, Np, Np, Np, b.Np_max, Np, Np, b.h2_6, 0.0});
+            mv.push_back(GemmEntry{sc.vb.V.p, P[e].psibc, P[e].VP, Np, Np, Np, b.Np_max, Np, Np, b.h2_6, 0.0});
             if (N < b.n_tr && Nf > 0) {
-                mf.push_back(GemmEntry{gp.vb.B.p, P[e].psibc, P[e].fN, Nf, Np, Np, b.Np_max, Np, Nf, 1.0, 0.0});
+                mf.push_back(GemmEntry{sc.vb.B.p, P[e].psibc, P[e].fN, Nf, Np, Np, b.Np_max, Np, Nf, 1.0, 0.0});
             }
         }
         SCATT_TRY(L.gemm(mv, 0, 0));
@@ -1894,7 +1849,7 @@ int post_slots(Scan& sc, GroupPost& gp, const std::vector<int>& sel, const std::
             // B_N f_N = B_N (-(D^-1 B^T psi)) = -(Bs_N)(B_N^T psi) with Bs = B D^-1.
             for (int e = 0; e < cnt; ++e) {
                 const int Np = ED(e).Np;
-                mb.push_back(GemmEntry{gp.vb.Bs.p, P[e].fN, P[e].Bf, Np, Np, Nf, b.Np_max, Nf, Np, -1.0, 0.0});
+                mb.push_back(GemmEntry{sc.vb.Bs.p, P[e].fN, P[e].Bf, Np, Np, Nf, b.Np_max, Nf, Np, -1.0, 0.0});
             }
             SCATT_TRY(L.gemm(mb, 0, 0));
         }
@@ -1935,7 +1890,7 @@ int post_slots(Scan& sc, GroupPost& gp, const std::vector<int>& sel, const std::
         for (int e = 0; e < cnt; ++e) { zc[e] = P[e].Z0; zn[e] = P[e].Z1; }
         for (int n = N - 1; n >= b.n_s; --n) {
             const bool exch = n < b.n_tr && Nf > 0;
-            if (exch) gp.vb.build(b, n, s);
+            if (exch) sc.vb.build(b, n, s);
             std::vector<GemmEntry> mz, mr, mp;
             std::vector<CopyEntry> cr;
             for (int e = 0; e < cnt; ++e) {
@@ -1946,7 +1901,7 @@ int post_slots(Scan& sc, GroupPost& gp, const std::vector<int>& sel, const std::
                 const double* sinv = d.tailS + slot * Np * Np;
                 if (exch) {
                     cr.push_back(CopyEntry{zn[e], P[e].rhs, Np, Np, Nt, Np, 1.0});
-                    mr.push_back(GemmEntry{gp.vb.Bs.p, zn[e] + Np, P[e].rhs, Np, Np, Nf, b.Np_max, Nt, Np, -1.0, 1.0});
+                    mr.push_back(GemmEntry{sc.vb.Bs.p, zn[e] + Np, P[e].rhs, Np, Np, Nf, b.Np_max, Nt, Np, -1.0, 1.0});
                     mp.push_back(GemmEntry{sinv, P[e].rhs, d.psiT + slot * Np * Np, Np, Np, Np, Np, Np, Np, 1.0, 0.0});
                 } else {
                     mp.push_back(GemmEntry{sinv, zn[e], d.psiT + slot * Np * Np, Np, Np, Np, Np, Nt, Np, 1.0, 0.0});
@@ -2202,41 +2157,38 @@ int post_slots(Scan& sc, GroupPost& gp, const std::vector<int>& sel, const std::
 }
 
 // Runs chunks until at least one group has finished its sweep, then its
-// post stages.  Each group advances on its own stream; the host keeps up to
-// sc.ahead chunks of every running group enqueued and polls the events that
-// follow them, so no group waits for another.  out_row(slot, i) gives the
-// output row of the i-th finished energy (held by `slot`).  *n_done receives
-// the number of finished energies (0: nothing was in flight and the queue is
-// empty); done_jobs lists their submission indices.  Device time of a step
-// runs from the end of the previous step (or from the first launch) to the
-// end of this step's post stages, on the GPU clock.
+// post stages.  out_row(slot, i) gives the output row of the i-th finished
+// energy (held by `slot`).  *n_done receives the number of finished energies
+// (0: nothing was in flight and the queue is empty); done_jobs lists their
+// submission indices.
 template <class RowOf>
 int scan_advance(Scan& sc, const scatt_outputs* out, RowOf out_row, int* n_done, std::vector<long>* done_jobs,
                  int* first_status, std::string* first_msg) {
+    cudaStream_t s = sc.ctx->stream;
     *n_done = 0;
     SolveStats& stats = sc.ctx->stats;
     const unsigned long long launches0 = launch_counter();
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp = nullptr;
     ChunkTiming tm;
-    ChunkTiming* tmp = sc.o.timing ? &tm : nullptr;
-    if (sc.o.timing && !sc.last_end) {
-        SCATT_TRY(sc.event(&sc.last_end));
-        SCATT_CUDA_TRY(cudaEventRecord(sc.last_end, sc.gstream[0]));
+    sc.events.reset();
+    if (sc.o.timing) {
+        SCATT_TRY(sc.events.get(&ev0));
+        SCATT_TRY(sc.events.get(&ev1));
+        SCATT_TRY(sc.events.get(&evp));
+        SCATT_CUDA_TRY(cudaEventRecord(ev0, s));
     }
-    auto running = [&](int g) { return sc.grp[g].n0 >= 0; };
-    int ready = -1;                       // a finished group whose chunks have all completed
+    std::vector<int> finished;
     for (;;) {
         // idle groups whose turn has come take queued energies
         for (int g = 0; g < sc.G; ++g)
-            if (sc.grp[g].n0 == -1 && sc.chunk >= sc.start_chunk[g] && !sc.queue.empty()) {
+            if (sc.grp[g].n0 == -1 && sc.chunk >= sc.start_chunk[g] && !sc.queue.empty())
                 SCATT_TRY(load_group(sc, g));
-            }
-        bool any_running = false, waiting = false, any_done = false;
+        bool running = false, waiting = false;
         for (int g = 0; g < sc.G; ++g) {
-            any_running |= running(g);
+            running |= sc.grp[g].n0 >= 0;
             waiting |= sc.grp[g].n0 == -1 && sc.chunk < sc.start_chunk[g];
-            any_done |= sc.grp[g].n0 == -2;
         }
-        if (!any_running && !any_done) {
+        if (!running) {
             if (sc.queue.empty() || !waiting) break;
             // nothing runs until the next staggered start: start it now
             long next = -1;
@@ -2245,45 +2197,13 @@ int scan_advance(Scan& sc, const scatt_outputs* out, RowOf out_row, int* n_done,
             sc.chunk = std::max(sc.chunk, next);
             continue;
         }
-        // enqueue: every running group with room gets its next chunk
-        bool enqueued = false;
-        for (int g = 0; g < sc.G; ++g) {
-            auto& q = sc.inflight[g];
-            while (!q.empty() && cudaEventQuery(q.front()) == cudaSuccess) {
-                sc.release(q.front());
-                q.pop_front();
-            }
-            if (!running(g) || (int)q.size() >= sc.ahead) continue;
-            SCATT_TRY(run_chunk(sc, g, tmp));
-            cudaEvent_t ev;
-            SCATT_TRY(sc.event(&ev));
-            SCATT_CUDA_TRY(cudaEventRecord(ev, sc.gstream[g]));
-            q.push_back(ev);
-            enqueued = true;
-            if (sc.grp[g].n0 == -2 && !sc.done_rec[g]) {
-                if (!sc.done_ev[g]) SCATT_TRY(sc.event(&sc.done_ev[g]));
-                SCATT_CUDA_TRY(cudaEventRecord(sc.done_ev[g], sc.gstream[g]));
-                sc.done_rec[g] = 1;
-            }
-        }
-        // a finished group whose chunks have completed
-        for (int g = 0; g < sc.G && ready < 0; ++g)
-            if (sc.grp[g].n0 == -2 && sc.done_rec[g] && cudaEventQuery(sc.done_ev[g]) == cudaSuccess) ready = g;
-        if (ready >= 0) break;
-        if (!enqueued) {
-            // every running group is `ahead` chunks ahead and no finished one is
-            // done: wait for the oldest outstanding chunk of some group
-            int gw = -1;
-            for (int g = 0; g < sc.G; ++g)
-                if (!sc.inflight[g].empty()) { gw = g; break; }
-            for (int g = 0; g < sc.G; ++g)
-                if (sc.grp[g].n0 == -2 && sc.done_rec[g]) { SCATT_CUDA_TRY(cudaEventSynchronize(sc.done_ev[g])); gw = -2; break; }
-            if (gw >= 0) SCATT_CUDA_TRY(cudaEventSynchronize(sc.inflight[gw].front()));
-        }
+        SCATT_TRY(run_chunk(sc, sc.o.timing ? &tm : nullptr));
+        for (int g = 0; g < sc.G; ++g)
+            if (sc.grp[g].n0 == -2) finished.push_back(g);
+        if (!finished.empty()) break;
     }
-    if (ready >= 0) {
-        const int g = ready;
-        GroupPost& gp = *sc.gpost[g];
+    if (sc.o.timing) SCATT_CUDA_TRY(cudaEventRecord(evp, s));
+    for (int g : finished) {
         std::vector<int> sel;
         std::vector<long> rows;
         for (int e = g * sc.gs; e < std::min(sc.slots, (g + 1) * sc.gs); ++e)
@@ -2291,7 +2211,7 @@ int scan_advance(Scan& sc, const scatt_outputs* out, RowOf out_row, int* n_done,
                 sel.push_back(e);
                 rows.push_back(out_row(e, *n_done + (int)sel.size() - 1));
             }
-        SCATT_TRY(post_slots(sc, gp, sel, rows, out, first_status, first_msg));
+        SCATT_TRY(post_slots(sc, sel, rows, out, first_status, first_msg));
         for (int e : sel) {
             if (done_jobs) done_jobs->push_back(sc.job_of[e]);
             sc.ed[e].live = 0;
@@ -2299,45 +2219,26 @@ int scan_advance(Scan& sc, const scatt_outputs* out, RowOf out_row, int* n_done,
         }
         *n_done += (int)sel.size();
         sc.grp[g].n0 = -1;                    // k_advance already stopped it on the device
-        sc.done_rec[g] = 0;
         sc.start_chunk[g] = sc.chunk;         // refill at once: the group keeps its phase
-        if (sc.o.timing) {
-            cudaEvent_t end;
-            SCATT_TRY(sc.event(&end));
-            SCATT_CUDA_TRY(cudaEventRecord(end, gp.s));
-            SCATT_CUDA_TRY(cudaEventSynchronize(end));
-            float ms = 0.f;
-            SCATT_CUDA_TRY(cudaEventElapsedTime(&ms, sc.last_end, end));
-            stats.device_s += ms * 1e-3;
-            sc.release(sc.last_end);
-            sc.last_end = end;
-        }
     }
     if (sc.o.timing) {
-        // sampled R^-1 timings: those complete by now (the rest on a later step)
-        for (size_t k = 0; k < tm.rinv.size(); ++k) {
-            sc.rinv_pending.push_back(tm.rinv[k]);
-            sc.rinv_pending_flops.push_back(tm.flops[k]);
-        }
-        std::vector<std::pair<cudaEvent_t, cudaEvent_t>> keep;
-        std::vector<double> keepf;
-        for (size_t k = 0; k < sc.rinv_pending.size(); ++k) {
-            auto pr = sc.rinv_pending[k];
-            if (cudaEventQuery(pr.second) != cudaSuccess) {
-                keep.push_back(pr);
-                keepf.push_back(sc.rinv_pending_flops[k]);
-                continue;
-            }
+        SCATT_CUDA_TRY(cudaEventRecord(ev1, s));
+        SCATT_CUDA_TRY(cudaEventSynchronize(ev1));
+        float ms_all = 0.f, ms_sweep = 0.f;
+        SCATT_CUDA_TRY(cudaEventElapsedTime(&ms_all, ev0, ev1));
+        SCATT_CUDA_TRY(cudaEventElapsedTime(&ms_sweep, ev0, evp));
+        double rs = 0.0;
+        for (auto& pr : tm.rinv) {
             float ms = 0.f;
             SCATT_CUDA_TRY(cudaEventElapsedTime(&ms, pr.first, pr.second));
-            stats.rinv_s += ms * 1e-3;
-            stats.rinv_calls += 1.0;
-            stats.rinv_flops += sc.rinv_pending_flops[k];
-            sc.release(pr.first);
-            sc.release(pr.second);
+            rs += ms * 1e-3;
         }
-        sc.rinv_pending.swap(keep);
-        sc.rinv_pending_flops.swap(keepf);
+        stats.device_s += ms_all * 1e-3;
+        stats.sweep_s += ms_sweep * 1e-3;
+        stats.post_s += (ms_all - ms_sweep) * 1e-3;
+        stats.rinv_s += rs;
+        stats.rinv_calls += (double)tm.rinv.size();
+        stats.rinv_flops += tm.flops;
     }
     stats.launches += launch_counter() - launches0;
     return SCATT_OK;
@@ -2901,7 +2802,7 @@ int adj_forward(Context& ctx, const scatt_solve_opts& o_in, int n, const double*
     // ---- the sweep, with a checkpoint at every segment start a: Rinv(a-1), G(a-1)^T
     while (sc.grp[0].n0 >= 0) {
         const int next = sc.grp[0].n0 + sc.grp[0].C;
-        SCATT_TRY(run_chunk(sc, 0, nullptr));
+        SCATT_TRY(run_chunk(sc, nullptr));
         if (next % segment == 0 && next < N) {
             const int si = next / segment;
             for (int e = 0; e < n; ++e) {
@@ -2920,7 +2821,7 @@ int adj_forward(Context& ctx, const scatt_solve_opts& o_in, int n, const double*
     for (int e = 0; e < n; ++e) { sel[e] = e; rows[e] = sc.job_of[e]; }
     int first = SCATT_OK;
     std::string msg;
-    SCATT_TRY(post_slots(sc, *sc.gpost[0], sel, rows, out, &first, &msg));
+    SCATT_TRY(post_slots(sc, sel, rows, out, &first, &msg));
     sc.grp[0].n0 = -1;
     // ---- what the small stages read besides the window store: V(N), B(N), Bs(N); Bs of window steps
     SCATT_TRY(A.vbN.alloc(b));
@@ -2990,12 +2891,11 @@ int adj_reverse(Adjoint& A, double* vtr_host, double* vfull) {
         }
         SCATT_CUDA_TRY(cudaMemcpyAsync(sc.d_ed.p, sc.ed.data(), n * sizeof(EnergyDev), cudaMemcpyHostToDevice, s));
         b.n_stop = bnd;
-        sc.gb[0].n_stop = bnd;
-        k_set_group<<<1, 1, 0, s>>>(sc.gb[0], 0, a);
+        k_set_group<<<1, 1, 0, s>>>(b, 0, a);
         SCATT_COUNT_LAUNCH(1);
         sc.grp[0].n0 = a;
         sc.grp[0].C = std::min(SCHUR_CHUNK, bnd - a);
-        while (sc.grp[0].n0 >= 0) SCATT_TRY(run_chunk(sc, 0, nullptr));
+        while (sc.grp[0].n0 >= 0) SCATT_TRY(run_chunk(sc, nullptr));
         sc.grp[0].n0 = -1;
         // ---- the steps of the segment, backward
         args.seg_lo = a;
@@ -3050,7 +2950,6 @@ int adj_reverse(Adjoint& A, double* vtr_host, double* vfull) {
     for (int e = 0; e < n; ++e) sc.ed[e].seg_lo = sc.ed[e].seg_hi = 0;
     SCATT_CUDA_TRY(cudaMemcpyAsync(sc.d_ed.p, sc.ed.data(), n * sizeof(EnergyDev), cudaMemcpyHostToDevice, s));
     b.n_stop = b.Nr;
-    sc.gb[0].n_stop = b.Nr;
     if (vtr_host) {
         for (int i = 0; i < A.n_energy; ++i) {
             const int e = A.slot_of[i];

@@ -1,6 +1,6 @@
 """Oracle fixtures for GPU parity at the benchmark shapes.
 
-    python tests/golden/make_parity_fixtures.py CASE [--threads T]
+    python tests/golden/make_parity_fixtures.py CASE [--threads T] [--accum]
 
 CASE is one of:
   h2_c1        the H2-like workload at its full size (Nr 4001, dr 0.01,
@@ -16,6 +16,12 @@ LU and MKL dgetri / dsytrf + dsytri); their spread is the rounding floor the
 GPU tests scale their tolerance by.  Matrices with more than 100 rows are
 stored as products with four seeded random vectors plus their diagonals,
 which checks every entry with probability one at a fraction of the size.
+With --accum the six dipoles are also computed by the oracle's restatement
+of the GPU's own order of summation (oracle/adjoint_recurrence.DipoleAdjoint:
+the dipole rows accumulated forward with the R-ratios, Q = G(N-1)^T Z_N,
+instead of a back sweep), stored as e<i>/accum/D: the spread between the
+two summation orders is the floor of the dipoles where they are
+ill-conditioned.
 The file is tests/golden/parity_CASE.npz; it is rewritten after every solve,
 so a long case keeps what it has finished.  The full-size grids use the
 oracle's checkpointed solve (solve_energy_lean), whose results equal
@@ -76,6 +82,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=list(CASES))
     ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--accum", action="store_true")
     a = ap.parse_args()
     if a.threads:
         for v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
@@ -111,6 +118,18 @@ def main():
                 data[tag + key] = v
             np.savez_compressed(path, **data)
             print(f"{a.case} k={k} {build}: {time.time() - t0:.0f} s", flush=True)
+    if a.accum:
+        from oracle import adjoint_recurrence as AR
+        O.BUILD = "eigen"
+        for ik, k in enumerate(cfg["ks"]):
+            key = f"e{ik}/accum/D"
+            if key in data:
+                continue
+            t0 = time.time()
+            da = AR.DipoleAdjoint(st, 0.5 * k * k, lambda n: O.V_at(st, n))
+            data[key] = np.array(da.dipoles())
+            np.savez_compressed(path, **data)
+            print(f"{a.case} k={k} accum: {time.time() - t0:.0f} s", flush=True)
     O.BUILD = "eigen"
 
 

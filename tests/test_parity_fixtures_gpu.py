@@ -9,7 +9,11 @@ observable's largest entry; K (both extractions), A, B
 and the overlaps derive from one boundary value psi_N = J + Y K and share
 the largest of their floors, as in test_parity_gpu.  Matrices above 100 rows are
 compared through products with the fixture's four random vectors and their
-diagonals.  A case or energy missing from the fixture file is skipped.
+diagonals.  Where the fixture also holds the dipoles in the GPU's own
+order of summation (the forward accumulation Q = G(N-1)^T Z_N, key
+e<i>/accum/D), that is a third reference for D and its spread from the
+back-sweep result joins D's floor.  A case or energy missing from the
+fixture file is skipped; all deviations are reported before the assert.
 """
 import importlib.util
 import os
@@ -69,6 +73,7 @@ def test_gpu_matches_oracle_fixture(case):
     V = fx["proj_vectors"]
     worst = {}
     coupled_keys = [key for key in _gpu_record(res[0], V) if key.split(".")[0] in MATS or key == "b_overlap"]
+    fails = []
     for r, k in zip(res, ks):
         ik = cfg["ks"].index(k)
         got = _gpu_record(r, V)
@@ -78,11 +83,18 @@ def test_gpu_matches_oracle_fixture(case):
             if key in ("shifts", "n_closed_l"):
                 assert np.array_equal(np.asarray(g), ref), (case, k, key)
                 continue
-            floor = _rel(fx[f"e{ik}/mkl/{key}"], ref)
+            refs = [ref, fx[f"e{ik}/mkl/{key}"]]
+            floor = _rel(refs[1], ref)
             if key in coupled_keys:
                 floor = max(floor, coupled)
+            acc = fx.get(f"e{ik}/accum/{key}")
+            if acc is not None:
+                refs.append(acc)
+                floor = max(floor, _rel(acc, ref))
             tol = max(1e-10, 10.0 * floor)
-            err = min(_rel(g, ref), _rel(g, fx[f"e{ik}/mkl/{key}"]))
+            err = min(_rel(g, x) for x in refs)
             worst[key] = max(worst.get(key, 0.0), err)
-            assert err <= tol, (case, k, key, err, tol)
+            if not err <= tol:
+                fails.append(f"{case} k={k} {key}: err {err:.3e} floor {floor:.3e} tol {tol:.1e}")
     print(case, {k: f"{v:.2e}" for k, v in sorted(worst.items())})
+    assert not fails, "\n".join(fails)
