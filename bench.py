@@ -46,7 +46,7 @@ import numpy as np  # noqa: E402
 
 CONFIGS = {
     "h2o_like": dict(builder="h2o_like", kw=dict(Nr=12001, dr=0.005, l_cont=20, lmax_orb=40, n_orb=5),
-                     ks=lambda: np.linspace(0.05, 2.0, 200), slots=32, groups=8, graphs=0),
+                     ks=lambda: np.linspace(0.05, 2.0, 200), slots=128, groups=16, graphs=0),
     "h2_like": dict(builder="h2_like", kw=dict(Nr=4001, dr=0.01, l_cont=8),
                     ks=lambda: np.arange(1, 21) * 0.1, slots=20, groups=4, graphs=1),
 }
@@ -232,6 +232,8 @@ def main():
     ap.add_argument("--slots", type=int, default=0)
     ap.add_argument("--groups", type=int, default=0)
     ap.add_argument("--graphs", type=int, default=-1, help="replay chunks from CUDA graphs (default: per config)")
+    ap.add_argument("--keep-window", type=int, default=0,
+                    help="1: keep the fit window store (fit residual diagnostics); 0: accumulate the fit forward")
     ap.add_argument("--autotune", type=int, default=1,
                     help="time the inverse's blockings for the workload's orders before the run")
     ap.add_argument("--cpu-budget", type=float, default=20.0,
@@ -303,7 +305,7 @@ def main():
             tuned.append(_lib.autotune_inverse(n, count, device=local))
     peak = cuda_dgemm_peak(torch) if rank == 0 else None
     alloc, _keep = pinned_alloc(torch)
-    opts = S.default_opts(allow_closed_channels=1, timing=1, use_graphs=graphs)
+    opts = S.default_opts(allow_closed_channels=1, timing=1, use_graphs=graphs, keep_window=a.keep_window)
     scan = sol.scan(slots=slots, groups=groups, opts=opts, alloc=alloc)
     assert (scan.slots, scan.groups) == (slots, groups)
     scan.submit(next_energies(slots))
@@ -352,8 +354,10 @@ def main():
             "data": "synthetic (seeded H2O-like inputs of the benchmark shapes)"
                     if a.config == "h2o_like" else "synthetic (seeded H2-like inputs of the benchmark shapes)",
             "config": {**workload, "parallelism": f"energy-sharded x{ws}", "cuda_graphs": bool(graphs),
+                       "fit": "window store and back sweep (fit residual diagnostics)" if a.keep_window else
+                              "accumulated forward, [A; B] = G_A(N-1)^T Z_N (no window store; fit residual not computed)",
                        "autotuned_inverses": tuned,
-                       "l2": "inputs larger than L2 (per-slot state of the scan > 126 MB)"},
+                       "l2": "inputs larger than L2 (the scan's device state, several GB, exceeds the 126 MB L2)"},
             "e2e": {"value": n_total / host_s, "unit": "energies/s", "h2d_bytes_per_step": 8 * gsize,
                     "d2h_bytes_per_step": int(out_bytes / max(a.steps, 1))},
             "gpu_launches": int(launches),

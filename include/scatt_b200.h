@@ -198,6 +198,13 @@ typedef struct {
                                      of stages (same results, fewer launches)    */
     int    diagnostics;           /* 1: S-matrix unitarity and eigenphases            */
     int    timing;                /* 1: CUDA-event timing of the solve (scatt_last_stats) */
+    int    keep_window;           /* (1) keep Rinv and Sinv over the fit window and sweep psi back
+                                     over it (BackPropagator.cpp:603-703), which the fit residual
+                                     diagnostics need; 0: accumulate the fit forward, [A; B] =
+                                     G_A(N-1)^T Z_N like the dipole rows, which drops the window
+                                     store (about 1.8 GB of the 2.5 GB per energy at l_cont 20,
+                                     N_t 1046) so that many more energies share each batched
+                                     call; the fit residual diagnostics are then NaN */
 } scatt_solve_opts;
 
 /* Diagnostics per energy (index into scatt_outputs.diag). */

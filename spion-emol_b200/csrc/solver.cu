@@ -210,14 +210,14 @@ __device__ __forceinline__ bool in_seg(const EnergyDev& d, int n) { return n >= 
 __device__ __forceinline__ double* sinv_at(const BatchDev& b, const EnergyDev& d, int n, int j) {
     const size_t np2 = (size_t)d.Np * d.Np;
     if (in_seg(d, n)) return d.segS + (size_t)(n - d.seg_lo) * np2;
-    return n >= b.n_s ? d.tailS + (size_t)(n - b.n_s) * np2 : d.Sinv + (size_t)j * np2;
+    return (n >= b.n_s && d.tailS) ? d.tailS + (size_t)(n - b.n_s) * np2 : d.Sinv + (size_t)j * np2;
 }
 
 // Rinv(n): the segment store, the asymptotic window store, or the ping-pong pair.
 __device__ __forceinline__ double* rinv_at(const BatchDev& b, const EnergyDev& d, int n) {
     const size_t nt2 = (size_t)d.Nt * d.Nt;
     if (in_seg(d, n)) return d.segR + (size_t)(n - d.seg_lo) * nt2;
-    return n >= b.n_s ? d.tailR + (size_t)(n - b.n_s) * nt2 : ((n & 1) ? d.Rinv1 : d.Rinv0);
+    return (n >= b.n_s && d.tailR) ? d.tailR + (size_t)(n - b.n_s) * nt2 : ((n & 1) ? d.Rinv1 : d.Rinv0);
 }
 
 // G(n-1)^T, accumulated into H(n)^T during step n (K x N_t, ld K).
@@ -262,7 +262,7 @@ __global__ void k_prepare(BatchDev b, int j) {
     const int n = step_of(b, d, j);
     const GemmEntry none{nullptr, nullptr, nullptr, 0, 0, 0, 1, 1, 1, 0.0, 1.0};
     if (n < 0) {
-        b.gmT[e] = b.gmF[e] = b.gmG1[e] = b.gmG2[e] = b.gmG3[e] = none;
+        b.gmT[e] = b.gmF[e] = b.gmG1[e] = b.gmG2[e] = b.gmG3[e] = b.gmGA[e] = none;
         b.gjR[e] = GjEntry{d.Ra, d.Rw, d.Ra, d.sigR, d.ridR, d.stR, 0, 1, 1, d.PR, d.sgR};
         return;
     }
@@ -282,6 +282,11 @@ __global__ void k_prepare(BatchDev b, int j) {
     b.gmG2[e] = (sweep && Cn && exch) ? GemmEntry{Cn, d.T, gcur + (size_t)Np * K, K, Nf, Np, K, Np, K, -1.0, 1.0}
                                       : none;
     b.gmG3[e] = sweep ? GemmEntry{gcur, rinv, gnext, K, Nt, Nt, K, Nt, K, 1.0, 0.0} : none;
+    // the fit accumulation G_A(n)^T = H_A(n)^T Rinv(n) over n_s <= n <= N - 1
+    b.gmGA[e] = (d.GA0 && n >= b.n_s && sweep)
+                    ? GemmEntry{(n & 1) ? d.GA1 : d.GA0, rinv, (n & 1) ? d.GA0 : d.GA1, 2 * Np, Nt, Nt, 2 * Np, Nt,
+                                2 * Np, 1.0, 0.0}
+                    : none;
     b.gjR[e] = GjEntry{d.Ra, d.Rw, rinv, d.sigR, d.ridR, d.stR, n >= b.n_start ? Nt : 0, Nt, Nt, d.PR, d.sgR};
 }
 
@@ -455,6 +460,99 @@ __global__ void k_collect(BatchDev b, int j, int which) {
     if (st != 0 && d.err_code == 0) {
         d.err_code = (st == DEV_SINGULAR) ? SCATT_ERR_SINGULAR : SCATT_ERR_NONFINITE;
         d.err_step = n;
+    }
+}
+
+// ---- forward accumulation of the amplitude fit (no window store)
+// The fit (AsymptoticAmplitudes.cpp:64-359) is linear in psi over the window
+// [n_s, ne_fit]: per channel mu of angular momentum l,
+//   A[mu, :] = sum_i (M00 j_l(i) + M01 y_l(i)) psi_i[mu, :],  B likewise with M10, M11,
+// with M the inverse of the 2 x 2 normal matrix of (j_l, y_l) on the window.
+// psi_i = E_psi W^-1(i) Z(i) and Z(i) = Rinv(i) ... Rinv(N-1) Z_N, so [A; B] =
+// G_A(N-1)^T Z_N with G_A accumulated forward like the dipole rows.
+
+// normal matrices per l (as k_aa_normal, same order of summation); grid (l, slots of the range)
+__global__ void k_ab_normal(BatchDev b, int e0) {
+    EnergyDev& d = b.ed[e0 + blockIdx.y];
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!d.live || !d.Mab || l > d.l_cont) return;
+    double m00 = 0.0, m01 = 0.0, m11 = 0.0;
+    for (int i = 0; i < b.nfit; ++i) {
+        const double r = b.dr + (b.n_s + i) * b.dr;
+        const double jv = riccati_j(l, d.k * r), yv = riccati_y(l, d.k * r);
+        m00 += jv * jv;
+        m01 += jv * yv;
+        m11 += yv * yv;
+    }
+    const double det = m00 * m11 - m01 * m01;
+    const double mx = fmax(fabs(m00), fmax(fabs(m01), fabs(m11)));
+    const bool singular = !(fabs(det) > 1e-20 * mx * mx);
+    double* o = d.Mab + l * 8;
+    o[4] = singular ? 1.0 : 0.0;
+    o[5] = det;
+    o[6] = mx;
+    if (!singular) {
+        o[0] = m11 / det; o[1] = -m01 / det; o[2] = -m01 / det; o[3] = m00 / det;
+    } else {
+        o[0] = 1.0; o[1] = 0.0; o[2] = 0.0; o[3] = 1.0;
+    }
+}
+
+// fit weights wAB[i][a][mu]; grid (x, slots of the range)
+__global__ void k_ab_weights(BatchDev b, int e0) {
+    EnergyDev& d = b.ed[e0 + blockIdx.y];
+    if (!d.live || !d.wAB) return;
+    const int Np = d.Np;
+    const long total = (long)b.nfit * Np;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx / Np), mu = (int)(idx % Np);
+        const int l = b.l_of_mu[mu];
+        const double r = b.dr + (b.n_s + i) * b.dr;
+        const double jv = riccati_j(l, d.k * r), yv = riccati_y(l, d.k * r);
+        const double* m = d.Mab + l * 8;
+        const bool closed = m[4] != 0.0;
+        d.wAB[((size_t)i * 2 + 0) * Np + mu] = closed ? 0.0 : m[0] * jv + m[1] * yv;
+        d.wAB[((size_t)i * 2 + 1) * Np + mu] = closed ? 0.0 : m[2] * jv + m[3] * yv;
+    }
+}
+
+// H_A(n)^T = G_A(n-1)^T + D_AB(n) [Sinv, -T] on the fit window; grid (x, slots)
+__global__ void k_acc_ab(BatchDev b, int j) {
+    const EnergyDev& d = b.ed[blockIdx.y];
+    const int n = step_of(b, d, j);
+    if (n < b.n_s || n > b.ne_fit || !d.GA0) return;
+    const int Np = d.Np, Nt = d.Nt, two = 2 * Np;
+    const bool exch = n < b.n_tr && b.Nf > 0;
+    const double* sinv = sinv_at(b, d, n, j);
+    const double* w = d.wAB + (size_t)(n - b.n_s) * two;
+    double* ga = (n & 1) ? d.GA1 : d.GA0;
+    const long total = (long)two * Nt;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
+        const int r = (int)(idx % two), c = (int)(idx / two);
+        const int mu = r % Np;
+        double v;
+        if (c < Np) v = sinv[mu + (size_t)c * Np];
+        else v = exch ? -d.T[mu + (size_t)(c - Np) * Np] : 0.0;
+        ga[idx] += w[r] * v;
+    }
+}
+
+// rows of closed channels: A = I, B = 0 (AsymptoticAmplitudes.cpp:177-212); grid (x, energies)
+struct AbEntry {
+    double* A;
+    double* B;
+    const double* Mab;
+    int Np;
+};
+__global__ void k_ab_closed(const AbEntry* __restrict__ ents, const int* l_of_mu) {
+    const AbEntry a = ents[blockIdx.y];
+    const long total = (long)a.Np * a.Np;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
+        const int mu = (int)(idx % a.Np), col = (int)(idx / a.Np);
+        if (a.Mab[l_of_mu[mu] * 8 + 4] != 0.0) {
+            a.A[idx] = (col == mu) ? 1.0 : 0.0;
+            a.B[idx] = 0.0;
+        }
     }
 }
 
@@ -1129,6 +1227,8 @@ int make_consts(const ScanTables& t, const scatt_solve_opts& o, BatchDev& b) {
             return SCATT_ERR_FIT_WINDOW;
         }
         b.n_s = nsf;
+        b.ne_fit = nef;
+        b.nfit = nef - nsf + 1;
     }
     b.stab_n = std::min(o.stab_n_max, t.Nr);
     b.Np_max = t.Np_max;
@@ -1250,13 +1350,18 @@ int ensure_stab(Context& ctx, const scatt_solve_opts& o, int l_cont, const doubl
 // Device doubles of one slot sized for (Np, Nt): the chunk's Schur slots,
 // the W^-1 blocks, the R ping-pong buffers, the dipole rows, the asymptotic
 // window store and the inverse's panel windows (every piece 256-byte aligned).
-size_t slot_doubles(const BatchDev& b, int Np, int Nt) {
+// Without the window store (keep_window = 0) the fit is accumulated
+// forward instead: 2 x (2 Np x N_t) accumulators, the fit weights and the
+// per-l normal matrices replace (N - n_s + 1) x (N_t^2 + 2 Np^2).
+size_t slot_doubles(const BatchDev& b, int Np, int Nt, int l_cont, bool keep_window) {
     const int nslots = b.N - b.n_s + 1;
     auto al = [](size_t c) { return (c + 31) & ~size_t(31); };
     const size_t np2 = (size_t)Np * Np, nt2 = (size_t)Nt * Nt;
-    return 3 * al(SCHUR_CHUNK * np2) + al((size_t)Np * b.Nf) + al((size_t)b.Nf * b.Nf) + 4 * al(nt2) +
-           2 * al((size_t)b.Krows * Nt) + al((size_t)nslots * nt2) + 2 * al((size_t)nslots * np2) +
-           al((size_t)SCHUR_CHUNK * 4 * 64 * Np) + al((size_t)4 * 64 * Nt);
+    const size_t base = 3 * al(SCHUR_CHUNK * np2) + al((size_t)Np * b.Nf) + al((size_t)b.Nf * b.Nf) +
+                        4 * al(nt2) + 2 * al((size_t)b.Krows * Nt) + al((size_t)SCHUR_CHUNK * 4 * 64 * Np) +
+                        al((size_t)4 * 64 * Nt);
+    if (keep_window) return base + al((size_t)nslots * nt2) + 2 * al((size_t)nslots * np2);
+    return base + 2 * al((size_t)2 * Np * Nt) + al((size_t)b.nfit * 2 * Np) + al((size_t)8 * (l_cont + 1));
 }
 size_t slot_ints(int Np, int Nt) { return SCHUR_CHUNK * (6 * (size_t)Np + 4) + 6 * (size_t)Nt + 4; }
 // Device doubles of one group's chunk arrays (V, B, Bs, D^-1 of SCHUR_CHUNK steps, V(n+1) diagonal).
@@ -1363,6 +1468,7 @@ int gemm_slots(Scan& sc, GemmEntry* ents, int count, int which, int opA, int opB
         case 3: M = K; N = Np; break;        // G1
         case 4: M = K; N = Nf; break;        // G2
         case 5: M = K; N = Nt; break;        // G3
+        case 6: M = 2 * Np; N = Nt; break;   // GA (the fit accumulation)
     }
     return gemm_batched(ents, count, M, N, opA, opB, sc.ctx->stream);
 }
@@ -1405,7 +1511,8 @@ int scan_open(Context& ctx, const scatt_solve_opts& o, int slots, int ngroups, i
     b.ngroups = ngroups;
     const int K = b.Krows, Nf = b.Nf;
     // ---- slot arena
-    const size_t per = slot_doubles(b, sc.Np_cap, sc.Nt_cap);
+    const bool keep = o.keep_window != 0;
+    const size_t per = slot_doubles(b, sc.Np_cap, sc.Nt_cap, l_cap, keep);
     SCATT_TRY(sc.arena.alloc(per * slots));
     SCATT_TRY(sc.iarena.alloc(slot_ints(sc.Np_cap, sc.Nt_cap) * slots));
     SCATT_CUDA_TRY(cudaMemsetAsync(sc.iarena.p, 0, sc.iarena.n * sizeof(int), s));
@@ -1430,9 +1537,16 @@ int scan_open(Context& ctx, const scatt_solve_opts& o, int slots, int ngroups, i
         d.Rinv1 = take(nt2);
         d.G0 = take((size_t)K * sc.Nt_cap);
         d.G1 = take((size_t)K * sc.Nt_cap);
-        d.tailR = take((size_t)nslots * nt2);
-        d.tailS = take((size_t)nslots * np2);
-        d.psiT = take((size_t)nslots * np2);
+        if (keep) {
+            d.tailR = take((size_t)nslots * nt2);
+            d.tailS = take((size_t)nslots * np2);
+            d.psiT = take((size_t)nslots * np2);
+        } else {
+            d.GA0 = take((size_t)2 * sc.Np_cap * sc.Nt_cap);
+            d.GA1 = take((size_t)2 * sc.Np_cap * sc.Nt_cap);
+            d.wAB = take((size_t)b.nfit * 2 * sc.Np_cap);
+            d.Mab = take((size_t)8 * (l_cap + 1));
+        }
         d.PS = take((size_t)SCHUR_CHUNK * 4 * 64 * sc.Np_cap);
         d.PR = take((size_t)4 * 64 * sc.Nt_cap);
         int* q = sc.iarena.p + slot_ints(sc.Np_cap, sc.Nt_cap) * e;
@@ -1473,11 +1587,12 @@ int scan_open(Context& ctx, const scatt_solve_opts& o, int slots, int ngroups, i
     sc.start_chunk.assign(ngroups, 0);
     for (int g = 0; g < ngroups; ++g) sc.start_chunk[g] = (long)g * sc.chunks_per_sweep / ngroups;
     // ---- entry arrays
-    SCATT_TRY(sc.gm.alloc((5 + SCHUR_CHUNK) * (size_t)slots));
+    SCATT_TRY(sc.gm.alloc((6 + SCHUR_CHUNK) * (size_t)slots));
     SCATT_TRY(sc.gj.alloc((1 + SCHUR_CHUNK) * (size_t)slots));
     b.gmT = sc.gm.p; b.gmF = sc.gm.p + slots;
     b.gmG1 = sc.gm.p + 2 * slots; b.gmG2 = sc.gm.p + 3 * slots; b.gmG3 = sc.gm.p + 4 * slots;
-    b.gmS = sc.gm.p + 5 * slots;                   // SCHUR_CHUNK x slots
+    b.gmGA = sc.gm.p + 5 * slots;
+    b.gmS = sc.gm.p + 6 * slots;                   // SCHUR_CHUNK x slots
     b.gjR = sc.gj.p; b.gjS = sc.gj.p + slots;      // gjS: SCHUR_CHUNK x slots
     // ---- post-stage buffers for one group
     SCATT_TRY(sc.vb.alloc(b));
@@ -1551,6 +1666,20 @@ int load_group(Scan& sc, int g) {
     // a pageable copy: the host copy may change as soon as the call returns
     SCATT_CUDA_TRY(cudaMemcpyAsync(sc.d_ed.p + e0, sc.ed.data() + e0, (size_t)(e1 - e0) * sizeof(EnergyDev),
                                    cudaMemcpyHostToDevice, s));
+    if (sc.o.keep_window == 0) {
+        // the fit accumulation starts at zero; weights from this energy's k
+        for (int e = e0; e < e1; ++e) {
+            const EnergyDev& d = sc.ed[e];
+            if (!d.live) continue;
+            const size_t ga = (size_t)2 * d.Np * d.Nt * sizeof(double);
+            SCATT_CUDA_TRY(cudaMemsetAsync(d.GA0, 0, ga, s));
+            SCATT_CUDA_TRY(cudaMemsetAsync(d.GA1, 0, ga, s));
+        }
+        k_ab_normal<<<dim3(cdiv(sc.l_cap + 1, 32), e1 - e0), 32, 0, s>>>(sc.b, e0);
+        SCATT_COUNT_LAUNCH(1);
+        k_ab_weights<<<dim3(64, e1 - e0), TPB, 0, s>>>(sc.b, e0);
+        SCATT_COUNT_LAUNCH(1);
+    }
     k_set_group<<<1, 1, 0, s>>>(sc.b, g, 0);
     SCATT_COUNT_LAUNCH(1);
     sc.grp[g].n0 = 0;
@@ -1574,8 +1703,9 @@ int run_chunk(Scan& sc, ChunkTiming* tm) {
     const int count = sc.slots, G = sc.G, Nf = b.Nf;
     // what the running groups need at each chunk position (host mirror)
     bool step[SCHUR_CHUNK] = {}, exch[SCHUR_CHUNK] = {}, start[SCHUR_CHUNK] = {}, rinv[SCHUR_CHUNK] = {};
-    bool sweep[SCHUR_CHUNK] = {}, pts[SCHUR_CHUNK] = {};
+    bool sweep[SCHUR_CHUNK] = {}, pts[SCHUR_CHUNK] = {}, win[SCHUR_CHUNK] = {};
     bool stab = false, stab_x = false, any_exch = false;
+    const bool acc = sc.o.keep_window == 0;
     int live_rinv[SCHUR_CHUNK] = {};
     std::vector<int> live_in(G, 0);
     for (int e = 0; e < count; ++e) live_in[sc.ed[e].grp] += sc.ed[e].live;
@@ -1592,6 +1722,7 @@ int run_chunk(Scan& sc, ChunkTiming* tm) {
             if (n >= b.n_start) { rinv[j] = true; live_rinv[j] += live_in[g]; }
             sweep[j] |= n <= b.N - 1;
             pts[j] |= n < b.n_pts && n <= b.N - 1;
+            win[j] |= acc && n >= b.n_s && n <= b.N - 1;
             stab |= n < b.stab_n;
             stab_x |= n < b.stab_n && x;
         }
@@ -1664,6 +1795,11 @@ int run_chunk(Scan& sc, ChunkTiming* tm) {
                 if (pts[j] && exch[j]) SCATT_TRY(gemm_slots(sc, b.gmG2, count, 4, 0, 0));
                 SCATT_TRY(gemm_slots(sc, b.gmG3, count, 5, 0, 0));
             }
+            if (win[j]) {
+                k_acc_ab<<<eg, TPB, 0, s>>>(b, j);
+                SCATT_COUNT_LAUNCH(1);
+                SCATT_TRY(gemm_slots(sc, b.gmGA, count, 6, 0, 0));
+            }
         }
         k_advance<<<1, MAX_GROUPS, 0, s>>>(b);
         SCATT_COUNT_LAUNCH(1);
@@ -1672,8 +1808,9 @@ int run_chunk(Scan& sc, ChunkTiming* tm) {
     uint64_t key = (stab ? 1u : 0u) | (stab_x ? 2u : 0u) | (any_exch ? 4u : 0u);
     for (int j = 0; j < SCHUR_CHUNK; ++j) {
         const uint64_t bits = (step[j] ? 1u : 0u) | (exch[j] ? 2u : 0u) | (start[j] ? 4u : 0u) |
-                              (rinv[j] ? 8u : 0u) | (sweep[j] ? 16u : 0u) | (pts[j] ? 32u : 0u);
-        key |= bits << (3 + 6 * j);
+                              (rinv[j] ? 8u : 0u) | (sweep[j] ? 16u : 0u) | (pts[j] ? 32u : 0u) |
+                              (win[j] ? 64u : 0u);
+        key |= bits << (3 + 7 * j);
     }
     if (sc.o.use_graphs && !sample_chunk && sc.chunk > 0) {
         const auto gk = std::make_pair(key, b.n_stop);
@@ -1744,7 +1881,8 @@ int post_slots(Scan& sc, const std::vector<int>& sel, const std::vector<long>& r
         std::vector<GjEntry> gj;
         for (int e = 0; e < cnt; ++e) {
             const EnergyDev& d = ED(e);
-            const double* rin = d.tailR + (size_t)(N - 1 - b.n_s) * d.Nt * d.Nt;
+            const double* rin = d.tailR ? d.tailR + (size_t)(N - 1 - b.n_s) * d.Nt * d.Nt
+                                        : (((N - 1) & 1) ? d.Rinv1 : d.Rinv0);
             cp.push_back(CopyEntry{rin, d.Ra, d.Nt, d.Nt, d.Nt, d.Nt, 1.0});
             gj.push_back(GjEntry{d.Ra, d.Rw, d.Rinv0, d.sigR, d.ridR, d.stR, d.Nt, d.Nt, d.Nt});
         }
@@ -1878,8 +2016,10 @@ int post_slots(Scan& sc, const std::vector<int>& sel, const std::vector<long>& r
         SCATT_TRY(L.gemm(mc, 0, 0));
     }
 
-    // ---- backward sweep over the asymptotic window (BackPropagator.cpp:603-703)
-    {
+    // ---- backward sweep over the asymptotic window (BackPropagator.cpp:603-703),
+    // when the window is kept; otherwise the fit was accumulated forward
+    const bool keep = o.keep_window != 0;
+    if (keep) {
         std::vector<CopyEntry> c0;
         for (int e = 0; e < cnt; ++e) {
             const EnergyDev& d = ED(e);
@@ -1918,7 +2058,37 @@ int post_slots(Scan& sc, const std::vector<int>& sel, const std::vector<long>& r
     // ---- AsymptoticAmplitudes (AsymptoticAmplitudes.cpp:64-359)
     std::vector<double> aared(2 * cnt), aasym(2 * cnt);
     std::vector<int> nclosed(cnt, 0);
+    if (!keep) {
+        // [A; B] = G_A(N-1)^T Z_N, then the closed channels' rows
+        std::vector<GemmEntry> ma;
+        std::vector<AbEntry> ab;
+        for (int e = 0; e < cnt; ++e) {
+            const EnergyDev& d = ED(e);
+            const double* GA = (N & 1) ? d.GA1 : d.GA0;
+            const int Np = d.Np, Nt = d.Nt;
+            ma.push_back(GemmEntry{GA, P[e].Z0, P[e].Aaa, Np, Np, Nt, 2 * Np, Nt, Np, 1.0, 0.0});
+            ma.push_back(GemmEntry{GA + Np, P[e].Z0, P[e].Baa, Np, Np, Nt, 2 * Np, Nt, Np, 1.0, 0.0});
+            ab.push_back(AbEntry{P[e].Aaa, P[e].Baa, d.Mab, Np});
+        }
+        SCATT_TRY(L.gemm(ma, 0, 0));
+        DevBuf<AbEntry> dab;
+        SCATT_TRY(upload_vec(dab, ab, s));
+        k_ab_closed<<<dim3(64, cnt), TPB, 0, s>>>(dab.p, t.d_l_of_mu.p);
+        SCATT_COUNT_LAUNCH(1);
+        SCATT_CUDA_TRY(cudaGetLastError());
+        SCATT_CUDA_TRY(cudaStreamSynchronize(s));
+        for (int e = 0; e < cnt; ++e) {
+            aared[2 * e] = 1.0;                 // the fit residual needs psi at every window point: not kept
+            aared[2 * e + 1] = NAN;
+            std::vector<double> M(8 * (size_t)(ED(e).l_cont + 1));
+            SCATT_CUDA_TRY(cudaMemcpy(M.data(), ED(e).Mab, M.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            for (int l = 0; l <= ED(e).l_cont; ++l)
+                if (M[8 * l + 4] != 0.0) ++nclosed[e];
+            if (nclosed[e] > 0 && !o.allow_closed_channels && status[e] == SCATT_OK) status[e] = SCATT_ERR_CLOSED_CHANNEL;
+        }
+    }
     {
+      if (keep) {
         std::vector<AaEntry> ae;
         int maxl = 0;
         for (int e = 0; e < cnt; ++e) {
@@ -1955,6 +2125,7 @@ int post_slots(Scan& sc, const std::vector<int>& sel, const std::vector<long>& r
                 if (M[8 * l + 4] != 0.0) ++nclosed[e];
             if (nclosed[e] > 0 && !o.allow_closed_channels && status[e] == SCATT_OK) status[e] = SCATT_ERR_CLOSED_CHANNEL;
         }
+      }
         // K = B A^-1
         std::vector<CopyEntry> ca;
         std::vector<GjEntry> ga;
@@ -2270,7 +2441,8 @@ int slots_that_fit(Context& ctx, const scatt_solve_opts& o, int l_cap, int group
     SCATT_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
     const int Np = (l_cap + 1) * (l_cap + 1), Nt = Np + t.Nf;
     const int nfit = std::min(t.Nr - 1 - 3, b.N) - b.n_s + 1;
-    const size_t per = 8 * (slot_doubles(b, Np, Nt) + post_doubles(b, Np, Nt, l_cap, nfit, t.n_occ)) +
+    const size_t per = 8 * (slot_doubles(b, Np, Nt, l_cap, o.keep_window != 0) +
+                            post_doubles(b, Np, Nt, l_cap, nfit, t.n_occ)) +
                        4 * slot_ints(Np, Nt);
     const size_t fixed = 8 * group_doubles(b) * (size_t)groups + (64u << 20);
     const size_t avail = (size_t)(0.85 * freeb) > fixed ? (size_t)(0.85 * freeb) - fixed : 0;
@@ -2742,6 +2914,7 @@ int adj_forward(Context& ctx, const scatt_solve_opts& o_in, int n, const double*
     for (int e = 0; e < n; ++e) l_cap = std::max(l_cap, lc ? lc[e] : t.l_max);
     scatt_solve_opts o = o_in;
     o.use_graphs = 0;
+    o.keep_window = 1;                 // the small stages read the window store
     Scan& sc = A.sc;
     SCATT_TRY(scan_open(ctx, o, n, 1, l_cap, sc));
     const BatchDev& b = sc.b;
@@ -2989,6 +3162,7 @@ void scatt_default_opts(scatt_solve_opts* o) {
     o->use_graphs = 0;
     o->diagnostics = 1;
     o->timing = 0;
+    o->keep_window = 1;
 }
 
 int scatt_last_stats(scatt_ctx* ctx, double* out7) {

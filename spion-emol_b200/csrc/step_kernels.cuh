@@ -58,6 +58,12 @@ struct EnergyDev {
     int *sigR, *ridR, *stR;
     double *PS, *PR;       // two-level panel windows (4 x Np x 64 per Schur slot, 4 x Nt x 64)
     int *sgS, *sgR;        // composite row maps of the windows (4 x Np per Schur slot, 4 x Nt)
+    // forward accumulation of the amplitude fit (no window store: tailR == nullptr):
+    // GA0 / GA1 (2 Np x N_t, ld 2 Np) hold G_A(n-1)^T by parity, with
+    // G_A(n)^T = (G_A(n-1)^T + D_AB(n) E_psi W^-1(n)) Rinv(n) over the window, so that
+    // [A; B] = G_A(N-1)^T Z_N; wAB [i][2][Np] are the fit weights of window point
+    // n_s + i; Mab [l][8] the 2 x 2 normal-matrix inverse, closed flag, det, max
+    double *GA0, *GA1, *wAB, *Mab;
 };
 
 // Scan-level constants, static tables and the slot / group arrays.
@@ -66,6 +72,7 @@ struct BatchDev {
     int ngroups;
     int n_stop;             // chunks end before this step (N + 1 for a whole sweep)
     int Nr, N, n_tr, n_pts, n_start, n_s, stab_n;
+    int ne_fit, nfit;       // fit window [n_s, ne_fit] and its length
     int Np_max, Nf, n_sigma, n_occ, Krows, n_lambda, n_lambda_ex;
     double dr, h2_6, h2_12, W_min, margin;
     double alpha_pol, r_c;
@@ -84,7 +91,7 @@ struct BatchDev {
     const int* l_sigma;
     GroupDev* grp;          // ngroups entries
     // entry arrays written by k_prepare
-    GemmEntry *gmS, *gmT, *gmF, *gmG1, *gmG2, *gmG3;
+    GemmEntry *gmS, *gmT, *gmF, *gmG1, *gmG2, *gmG3, *gmGA;
     GjEntry *gjS, *gjR;
     EnergyDev* ed;
 };

@@ -42,7 +42,7 @@ class SolveOpts(C.Structure):
     _fields_ = [("W_min", C.c_double), ("stab_n_max", C.c_int), ("shift_margin", C.c_double),
                 ("n_asym", C.c_int), ("allow_closed_channels", C.c_int), ("orthogonalize", C.c_int),
                 ("max_batch", C.c_int), ("use_graphs", C.c_int), ("diagnostics", C.c_int),
-                ("timing", C.c_int)]
+                ("timing", C.c_int), ("keep_window", C.c_int)]
 
 
 class Outputs(C.Structure):
