@@ -58,11 +58,12 @@ CONFIGS = {
 INVERSE_TRAFFIC: dict = {}
 
 
-# Device seconds of one chunk (8 radial steps) with every slot busy, measured
-# on one B200 in FP64 (H2O-like: 32 slots in 8 groups, 10.77 s per step of
-# 188 chunks; H2-like: 20 slots in 4 groups without graphs, 0.40 s per step of
-# 126 chunks); the wall-time prediction below scales them by the slot count.
-CHUNK_S = {"h2o_like": (32, 0.0573), "h2_like": (20, 0.0032)}
+# Device seconds of one chunk (8 radial steps) with every slot busy, as
+# fixed + per-slot parts: the inverse's pivot chain is one CTA per matrix and
+# costs the same for any batch, the trailing updates and GEMMs grow with the
+# slots.  Measured on one B200 in FP64: H2O-like 57.3 ms per chunk at 32 slots
+# (8 x 3.6 ms of it the chain); H2-like 3.2 ms at 20 slots (launch-bound).
+CHUNK_S = {"h2o_like": (0.0288, 0.00089), "h2_like": (0.0016, 0.00008)}
 
 
 def plan(config: str, slots: int, groups: int, steps: int, warmup: int) -> dict:
@@ -82,11 +83,10 @@ def plan(config: str, slots: int, groups: int, steps: int, warmup: int) -> dict:
 def predict_seconds(config: str, slots: int, groups: int, steps: int, warmup: int, setup_s: float = 120.0,
                     cpu_s: float = 30.0) -> float:
     """Wall time of `bench.py --config C --steps K --warmup W`: the chunks at
-    the measured cost per chunk (a slot-count multiple of it), post stages
-    included in that cost, plus setup (upload, cuBLAS peak, autotune) and
-    the CPU baseline."""
-    s0, c0 = CHUNK_S[config]
-    return setup_s + cpu_s + plan(config, slots, groups, steps, warmup)["chunks_total"] * c0 * slots / s0
+    the measured cost per chunk (post stages included in it), plus setup
+    (upload, cuBLAS peak, autotune) and the CPU baseline."""
+    fixed, per_slot = CHUNK_S[config]
+    return setup_s + cpu_s + plan(config, slots, groups, steps, warmup)["chunks_total"] * (fixed + per_slot * slots)
 
 
 def dist_env():

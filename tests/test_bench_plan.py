@@ -23,7 +23,7 @@ def test_driver_run_fits_with_margin():
         c = bench.CONFIGS[cfg]
         t = bench.predict_seconds(cfg, c["slots"], c["groups"], steps=20, warmup=5)
         assert t <= 1500.0, (cfg, t)
-    # the lock-step batch the earlier bench ran (one group) would not fit
+    # a lock-step batch (one group) would not fit: every step a whole sweep
     assert bench.predict_seconds("h2o_like", 32, 1, steps=20, warmup=5) > 1800.0
 
 
