@@ -1666,7 +1666,7 @@ int load_group(Scan& sc, int g) {
     // a pageable copy: the host copy may change as soon as the call returns
     SCATT_CUDA_TRY(cudaMemcpyAsync(sc.d_ed.p + e0, sc.ed.data() + e0, (size_t)(e1 - e0) * sizeof(EnergyDev),
                                    cudaMemcpyHostToDevice, s));
-    if (sc.o.keep_window == 0) {
+    if (sc.o.keep_window == 0 && e1 > e0) {
         // the fit accumulation starts at zero; weights from this energy's k
         for (int e = e0; e < e1; ++e) {
             const EnergyDev& d = sc.ed[e];
