@@ -97,4 +97,10 @@ def test_gpu_matches_oracle_fixture(case):
             if not err <= tol:
                 fails.append(f"{case} k={k} {key}: err {err:.3e} floor {floor:.3e} tol {tol:.1e}")
     print(case, {k: f"{v:.2e}" for k, v in sorted(worst.items())})
+    report = os.environ.get("PARITY_REPORT")
+    if report:                          # per-observable maxima, for the results table
+        import json
+        old = json.load(open(report)) if os.path.exists(report) else {}
+        old[case] = {k: float(v) for k, v in worst.items()}
+        json.dump(old, open(report, "w"), indent=1, sort_keys=True)
     assert not fails, "\n".join(fails)
