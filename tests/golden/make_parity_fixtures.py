@@ -19,7 +19,7 @@ which checks every entry with probability one at a fraction of the size.
 With --accum the six dipoles are also computed by the oracle's restatement
 of the GPU's own order of summation (oracle/adjoint_recurrence.DipoleAdjoint:
 the dipole rows accumulated forward with the R-ratios, Q = G(N-1)^T Z_N,
-instead of a back sweep), stored as e<i>/accum/D: the spread between the
+instead of a back sweep), stored as e<i>/accum/{D, D_raw, d_raw}: the spread between the
 two summation orders is the floor of the dipoles where they are
 ill-conditioned.
 The file is tests/golden/parity_CASE.npz; it is rewritten after every solve,
@@ -122,12 +122,15 @@ def main():
         from oracle import adjoint_recurrence as AR
         O.BUILD = "eigen"
         for ik, k in enumerate(cfg["ks"]):
-            key = f"e{ik}/accum/D"
-            if key in data:
+            if f"e{ik}/accum/D_raw" in data:
                 continue
             t0 = time.time()
             da = AR.DipoleAdjoint(st, 0.5 * k * k, lambda n: O.V_at(st, n))
-            data[key] = np.array(da.dipoles())
+            data[f"e{ik}/accum/D"] = np.array(da.dipoles())
+            # D_raw = ((A - iB)^-1)^dagger d_raw, d_raw = the first six rows of Q
+            M = np.linalg.inv(da.A.astype(complex) - 1j * da.B).conj().T
+            data[f"e{ik}/accum/D_raw"] = (M @ da.Q[:6].T).T
+            data[f"e{ik}/accum/d_raw"] = np.array(da.Q[:6])
             np.savez_compressed(path, **data)
             print(f"{a.case} k={k} accum: {time.time() - t0:.0f} s", flush=True)
     O.BUILD = "eigen"
