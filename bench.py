@@ -49,6 +49,10 @@ CONFIGS = {
                      ks=lambda: np.linspace(0.05, 2.0, 200), slots=128, groups=16, graphs=0),
     "h2_like": dict(builder="h2_like", kw=dict(Nr=4001, dr=0.01, l_cont=8),
                     ks=lambda: np.arange(1, 21) * 0.1, slots=20, groups=4, graphs=1),
+    # the batched scan of mixed continuum cutoffs: 256 energies, l_cont 12 / 16 / 20 in turn
+    "h2o_mixed": dict(builder="h2o_like", kw=dict(Nr=12001, dr=0.005, l_cont=20, lmax_orb=40, n_orb=5),
+                      ks=lambda: np.linspace(0.05, 2.0, 256), slots=128, groups=16, graphs=0,
+                      l_conts=(12, 16, 20)),
 }
 
 
@@ -63,7 +67,7 @@ INVERSE_TRAFFIC: dict = {}
 # costs the same for any batch, the trailing updates and GEMMs grow with the
 # slots.  Measured on one B200 in FP64: H2O-like 57.3 ms per chunk at 32 slots
 # (8 x 3.6 ms of it the chain); H2-like 3.2 ms at 20 slots (launch-bound).
-CHUNK_S = {"h2o_like": (0.0288, 0.00089), "h2_like": (0.0016, 0.00008)}
+CHUNK_S = {"h2o_like": (0.0288, 0.00089), "h2_like": (0.0016, 0.00008), "h2o_mixed": (0.0288, 0.00089)}
 
 
 def plan(config: str, slots: int, groups: int, steps: int, warmup: int) -> dict:
@@ -249,7 +253,9 @@ def main():
     graphs = cfg["graphs"] if a.graphs < 0 else a.graphs
     workload = {"workload": a.config, **cfg["kw"], "energies": int(len(ks)), "slots": slots, "groups": groups,
                 "energies_per_step": slots // groups,
-                "seed": synth.SEED_BASE + (1 if a.config == "h2o_like" else 0)}
+                "seed": synth.SEED_BASE + (1 if cfg["builder"] == "h2o_like" else 0)}
+    if cfg.get("l_conts"):
+        workload["l_cont_per_energy"] = list(cfg["l_conts"])
 
     if a.impl == "reference":
         if rank != 0:
@@ -285,8 +291,12 @@ def main():
     setup_s = time.time() - t0
     # this rank's contiguous block of the k grid (cost-balanced; one l_cont here)
     from scatt_b200 import shard
-    blocks = shard.partition(shard.energy_cost(np.full(len(ks), cfg["kw"]["l_cont"]), sol.Nf), ws)
+    lcs = cfg.get("l_conts")
+    lc_all = (np.array([lcs[i % len(lcs)] for i in range(len(ks))], dtype=np.int32) if lcs
+              else np.full(len(ks), cfg["kw"]["l_cont"], dtype=np.int32))
+    blocks = shard.partition(shard.energy_cost(lc_all, sol.Nf), ws)
     Es_all = 0.5 * ks[blocks[rank]] ** 2
+    lc_mine = lc_all[blocks[rank]]
     if slots > len(Es_all):
         raise SystemExit(f"--slots {slots} exceeds this rank's {len(Es_all)} energies")
     gsize = slots // groups
@@ -295,7 +305,7 @@ def main():
     def next_energies(n):
         idx = [(cursor[0] + i) % len(Es_all) for i in range(n)]
         cursor[0] += n
-        return Es_all[idx]
+        return Es_all[idx], lc_mine[idx]
 
     tuned = []
     if a.autotune:
@@ -308,9 +318,9 @@ def main():
     opts = S.default_opts(allow_closed_channels=1, timing=1, use_graphs=graphs, keep_window=a.keep_window)
     scan = sol.scan(slots=slots, groups=groups, opts=opts, alloc=alloc)
     assert (scan.slots, scan.groups) == (slots, groups)
-    scan.submit(next_energies(slots))
+    scan.submit(*next_energies(slots))
     for w in range(a.warmup):
-        scan.submit(next_energies(gsize))
+        scan.submit(*next_energies(gsize))
         scan.step(results=False)
     torch.cuda.synchronize()
     if ws > 1:
@@ -322,7 +332,7 @@ def main():
     out_bytes = 0
     t_host = time.time()
     for k in range(a.steps):
-        scan.submit(next_energies(gsize))               # energies from host memory
+        scan.submit(*next_energies(gsize))              # energies from host memory
         n_done += len(scan.step(results=False))         # outputs back in pinned host memory
         out_bytes += scan.last_out_bytes
     torch.cuda.synchronize()
@@ -352,7 +362,7 @@ def main():
             "n_gpus": ws, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dev_s / a.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded H2O-like inputs of the benchmark shapes)"
-                    if a.config == "h2o_like" else "synthetic (seeded H2-like inputs of the benchmark shapes)",
+                    if cfg["builder"] == "h2o_like" else "synthetic (seeded H2-like inputs of the benchmark shapes)",
             "config": {**workload, "parallelism": f"energy-sharded x{ws}", "cuda_graphs": bool(graphs),
                        "fit": "window store and back sweep (fit residual diagnostics)" if a.keep_window else
                               "accumulated forward, [A; B] = G_A(N-1)^T Z_N (no window store; fit residual not computed)",
