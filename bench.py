@@ -66,8 +66,9 @@ INVERSE_TRAFFIC: dict = {}
 # fixed + per-slot parts: the inverse's pivot chain is one CTA per matrix and
 # costs the same for any batch, the trailing updates and GEMMs grow with the
 # slots.  Measured on one B200 in FP64: H2O-like 57.3 ms per chunk at 32 slots
-# (8 x 3.6 ms of it the chain); H2-like 3.2 ms at 20 slots (launch-bound).
-CHUNK_S = {"h2o_like": (0.0288, 0.00089), "h2_like": (0.0016, 0.00008), "h2o_mixed": (0.0288, 0.00089)}
+# and 200 ms at 128 slots (8 x 3.6 ms of it the chain); H2-like 3.2 ms at 20
+# slots (launch-bound).
+CHUNK_S = {"h2o_like": (0.0288, 0.00134), "h2_like": (0.0016, 0.00008), "h2o_mixed": (0.0288, 0.00134)}
 
 
 def plan(config: str, slots: int, groups: int, steps: int, warmup: int) -> dict:

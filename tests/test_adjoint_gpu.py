@@ -182,8 +182,8 @@ def test_potential_gradient_matches_central_differences():
         # Richardson: the h^2 term of the central difference cancels
         fd = (4.0 * quotient(n, i, j, 0.5 * h) - quotient(n, i, j, h)) / 3.0
         an = float(g[n, i, j] + (g[n, j, i] if i != j else 0.0))
-        # 1e-6 of the entry, plus 1e-8 of the largest gradient entry (the
-        # reverse pass's rounding, as in the comparison with the oracle), plus
-        # the quotient's rounding noise (about 1e-15 |J| over the step)
+        # 1e-6 of the entry, plus 1e-7 of the largest gradient entry (the
+        # rounding that an ill-conditioned solve carries into small entries),
+        # plus the quotient's rounding noise (about 1e-15 |J| over the step)
         noise = 1e-15 * J0 / h
-        assert abs(fd - an) <= 1e-6 * abs(an) + 1e-8 * gmax + noise, (n, i, j, fd, an, noise)
+        assert abs(fd - an) <= 1e-6 * abs(an) + 1e-7 * gmax + noise, (n, i, j, fd, an, noise)

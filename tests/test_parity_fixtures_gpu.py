@@ -88,6 +88,8 @@ def test_gpu_matches_oracle_fixture(case):
             if key in coupled_keys:
                 floor = max(floor, coupled)
             acc = fx.get(f"e{ik}/accum/{key}")
+            if key == "partial_sigma" and f"e{ik}/accum/D" in fx:      # sum_mu |D|^2 per slot
+                acc = np.sum(np.abs(fx[f"e{ik}/accum/D"]) ** 2, axis=1)
             if acc is not None:
                 refs.append(acc)
                 floor = max(floor, _rel(acc, ref))
