@@ -29,4 +29,4 @@ def test_driver_run_fits_with_margin():
 
 def test_default_run_is_short():
     c = bench.CONFIGS["h2o_like"]
-    assert bench.predict_seconds("h2o_like", c["slots"], c["groups"], steps=8, warmup=3) <= 600.0
+    assert bench.predict_seconds("h2o_like", c["slots"], c["groups"], steps=4, warmup=3) <= 600.0
