@@ -1,7 +1,7 @@
 """Benchmark: FP64 scan energies/sec of the per-energy scattering path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config h2o_like|h2_like] [--slots S] [--groups G]
+                    [--config h2o_like|h2_like|h2o_mixed|c8f8_like] [--slots S] [--groups G]
                     [--graphs 0|1] [--autotune 0|1]
 
 Workload (default): the H2O-like system -- O + 2 H, five doubly occupied
@@ -53,7 +53,17 @@ CONFIGS = {
     "h2o_mixed": dict(builder="h2o_like", kw=dict(Nr=12001, dr=0.005, l_cont=20, lmax_orb=40, n_orb=5),
                       ks=lambda: np.linspace(0.05, 2.0, 256), slots=128, groups=16, graphs=0,
                       l_conts=(12, 16, 20)),
+    # C8F8-like production shape: 36 occupied orbitals (N_f = 36 x 121 = 4356) and
+    # l_cont = 30 (961 continuum channels, the size of the ~950-channel symmetry
+    # block), N_t = 5317; 10001 points at dr = 0.01; one energy in flight
+    "c8f8_like": dict(builder="c8f8_like", kw=dict(Nr=10001, dr=0.01, l_cont=30, lmax_orb=40, n_orb=36),
+                      ks=lambda: np.linspace(0.1, 2.0, 50), slots=1, groups=1, graphs=0),
 }
+
+SEEDS = {"h2_like": 0, "h2o_like": 1, "c8f8_like": 4}
+DATA = {"h2_like": "synthetic (seeded H2-like inputs of the benchmark shapes)",
+        "h2o_like": "synthetic (seeded H2O-like inputs of the benchmark shapes)",
+        "c8f8_like": "synthetic (seeded C8F8-like inputs of the benchmark shapes)"}
 
 
 # DRAM bytes (read + write) per sampled R^-1 inversion of the scan, from one
@@ -68,7 +78,8 @@ INVERSE_TRAFFIC: dict = {}
 # slots.  Measured on one B200 in FP64: H2O-like 57.3 ms per chunk at 32 slots
 # and 200 ms at 128 slots (8 x 3.6 ms of it the chain); H2-like 3.2 ms at 20
 # slots (launch-bound).
-CHUNK_S = {"h2o_like": (0.0288, 0.00134), "h2_like": (0.0016, 0.00008), "h2o_mixed": (0.0288, 0.00134)}
+CHUNK_S = {"h2o_like": (0.0288, 0.00134), "h2_like": (0.0016, 0.00008), "h2o_mixed": (0.0288, 0.00134),
+           "c8f8_like": (0.0, 0.28)}
 
 
 def plan(config: str, slots: int, groups: int, steps: int, warmup: int) -> dict:
@@ -254,7 +265,7 @@ def main():
     graphs = cfg["graphs"] if a.graphs < 0 else a.graphs
     workload = {"workload": a.config, **cfg["kw"], "energies": int(len(ks)), "slots": slots, "groups": groups,
                 "energies_per_step": slots // groups,
-                "seed": synth.SEED_BASE + (1 if cfg["builder"] == "h2o_like" else 0)}
+                "seed": synth.SEED_BASE + SEEDS[cfg["builder"]]}
     if cfg.get("l_conts"):
         workload["l_cont_per_energy"] = list(cfg["l_conts"])
 
@@ -310,10 +321,12 @@ def main():
 
     tuned = []
     if a.autotune:
-        # the scan's batches: R^-1 of order N_t over the slots, and the Schur
-        # inverses of order Np over the slots' 8 radial steps of a chunk
+        # inverses of the scan's batches: R^-1 of order N_t over the slots, and the
+        # Schur inverses of order Np over the slots' 8 radial steps of a chunk
+        # (orders above 1280 have one blocking, the cluster panel: nothing to tune)
         for n, count in sorted({(sol.Np + sol.Nf, slots), (sol.Np, slots * 8)}):
-            tuned.append(_lib.autotune_inverse(n, count, device=local))
+            if n <= 1280:
+                tuned.append(_lib.autotune_inverse(n, count, device=local))
     peak = cuda_dgemm_peak(torch) if rank == 0 else None
     alloc, _keep = pinned_alloc(torch)
     opts = S.default_opts(allow_closed_channels=1, timing=1, use_graphs=graphs, keep_window=a.keep_window)
@@ -362,8 +375,7 @@ def main():
             "metric": "FP64 scan energies/sec", "value": n_total / dev_s, "unit": "energies/s",
             "n_gpus": ws, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dev_s / a.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded H2O-like inputs of the benchmark shapes)"
-                    if cfg["builder"] == "h2o_like" else "synthetic (seeded H2-like inputs of the benchmark shapes)",
+            "data": DATA[cfg["builder"]],
             "config": {**workload, "parallelism": f"energy-sharded x{ws}", "cuda_graphs": bool(graphs),
                        "fit": "window store and back sweep (fit residual diagnostics)" if a.keep_window else
                               "accumulated forward, [A; B] = G_A(N-1)^T Z_N (no window store; fit residual not computed)",

@@ -58,6 +58,9 @@ double scatt_riccati_y(int l, double x);
  * Batched inverse of `count` n x n matrices (contiguous, ld = n) with partial
  * pivoting; symmetrize != 0 returns 0.5 (X + X^T).  status (may be NULL)
  * receives 2 ints per matrix: device status code, first failing column.
+ * Orders up to 8192 under the automatic and row-contiguous schemes (above
+ * 1280 the panels run on a thread-block cluster of up to 8 CTAs per
+ * matrix); larger orders return SCATT_ERR_SIZE.
  * Replaces inverse_general / inverse_symmetric_indefinite
  * (src/scatt/LapackInverse.hpp:53-178). */
 int scatt_inverse_batched(int n, int count, const double* A, double* out,

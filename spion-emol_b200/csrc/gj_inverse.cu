@@ -28,6 +28,8 @@
 //            optionally 0.5 (X + X^T) in the same pass.
 #include "common.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <map>
@@ -749,6 +751,214 @@ gj2_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub, int la) {
     }
 }
 
+// Panel for orders above one CTA's registers (up to GJ4_CL_MAX x 1024 rows):
+// the same elimination as gj2_panel_kernel on the row-contiguous window,
+// spread over a thread-block cluster of CL CTAs per matrix.  CTA c keeps rows
+// [c RC, (c + 1) RC) of the 16-column panel in registers (RC = R x threads).
+// Per column every warp publishes its candidate (key, position) and the
+// candidate's panel row in its own shared memory; one cluster barrier
+// (arrive = release, wait = acquire) makes them visible cluster-wide; every
+// warp then reduces the CL x W candidates read through distributed shared
+// memory and reads the pivot row from the owning CTA.  Candidate slots
+// alternate by column parity: a slot is rewritten only after every CTA has
+// arrived at the barrier that follows its last read.  Every exit depends on
+// the matrix only, so it is uniform across the cluster, and a last cluster
+// barrier keeps each CTA's shared memory alive until its peers' reads are
+// done.  No column rotation here: the active column is picked by a
+// compile-time-unrolled select, which keeps every register index static.
+constexpr int GJ4_R = 4, GJ4_NW = 8;
+constexpr int GJ4_ROWS = GJ4_R * GJ4_NW * 32;        // rows per CTA
+constexpr int GJ4_CL_MAX = 8;                       // portable cluster size
+
+template <int R, int NW>
+__global__ void __launch_bounds__(NW * 32, 1)
+gj4_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub, int la) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int CL = (int)cluster.num_blocks();
+    const int crank = (int)cluster.block_rank();
+    const GjEntry e = entries[blockIdx.x / CL];
+    const int n = e.n;
+    const int k0o = K * OB;
+    if (k0o >= n) return;
+    const int nb64 = min(OB, n - k0o);
+    const int cs = sub * NB;
+    if (cs >= nb64) return;
+    const int nb = min(NB, nb64 - cs);
+    const int kr0 = k0o + cs;
+    int lds = e.ld;
+    const double* src = win_in_rm(e, K, sub, lds, la);
+    double* dst = win_out_rm(e, K, sub, la);
+    const size_t rs = (size_t)lds;
+    constexpr int T = NW * 32;
+    constexpr int RC = R * T;
+    const int rbase = crank * RC;
+    const bool first = (K == 0 && sub == 0);
+    const bool vrow = (rs % 2 == 0) && (nb % 2 == 0);
+
+    // candidate key of warp w for column parity p: x = hi, y = lo, z = position
+    __shared__ uint4 cand[2][NW];
+    __shared__ __align__(16) double cand_row[2][NW][NB];
+    __shared__ int lab_s[RC], stv_s[RC];   // labels of this CTA's rows (used at the ends only)
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int* sg = sigt_set(e, K, la);
+    const int* st_in = sg + (size_t)(sub & 1) * n;
+    int* st_out = sg + (size_t)((sub + 1) & 1) * n;
+    double v[R][NB];
+    int pos[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int li = tid + r * T, i = rbase + li;
+        const bool ok = i < n;
+        if (vrow) {
+            const double2* rp = reinterpret_cast<const double2*>(src + (size_t)i * rs + cs);
+#pragma unroll
+            for (int j = 0; j < NB / 2; ++j) {
+                const double2 x = (ok && 2 * j < nb) ? rp[j] : make_double2(0.0, 0.0);
+                v[r][2 * j] = x.x;
+                v[r][2 * j + 1] = x.y;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < NB; ++j) v[r][j] = (ok && j < nb) ? src[(size_t)i * rs + (size_t)(cs + j)] : 0.0;
+        }
+        pos[r] = ok ? i : -1;
+        if (ok) {
+            lab_s[li] = first ? i : e.rowid[i];
+            stv_s[li] = (sub == 0) ? i : st_in[i];
+        }
+    }
+    const bool leader = crank == 0 && tid == 0;
+    int st_code = 0, st_col = -1;
+    if (leader) st_code = first ? 0 : e.status[0];
+
+    // this warp's candidate for panel slot `slot` among positions >= `after`, into set `par`
+    auto publish = [&](int par, int slot, int after) {
+        double bv = -1.0;
+        int bi = -1;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            double x = 0.0;
+#pragma unroll
+            for (int c = 0; c < NB; ++c)
+                if (c == slot) x = v[r][c];
+            if (pos[r] >= after) better_key(bv, bi, fabs(x), pos[r]);
+        }
+        const PivKey wk = warp_best_key(piv_key(bv, bi));
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const bool mine = wk.pos >= 0 && pos[r] == wk.pos;
+            if (__any_sync(0xffffffffu, mine) && mine) {
+#pragma unroll
+                for (int c = 0; c < NB; ++c) cand_row[par][warp][c] = v[r][c];
+            }
+        }
+        if (lane == 0) cand[par][warp] = make_uint4(wk.hi, wk.lo, (unsigned)wk.pos, 0u);
+    };
+    publish(0, 0, kr0);
+
+#pragma unroll 1
+    for (int jj = 0; jj < nb; ++jj) {
+        const int k = kr0 + jj;
+        const int par = jj & 1;
+        cluster.sync();
+        // best of the cluster's CL x NW candidates, read through distributed shared memory
+        PivKey best{0u, 0u, -1};
+        int from = 0;                                // cta * NW + warp of best
+        for (int idx = lane; idx < CL * NW; idx += 32) {
+            const int c = idx / NW, w = idx - c * NW;
+            const uint4 x = *cluster.map_shared_rank(&cand[par][w], (unsigned)c);
+            const PivKey xk{x.x, x.y, (int)x.z};
+            const bool bt = xk.hi > best.hi || (xk.hi == best.hi && xk.lo > best.lo) ||
+                            (xk.hi == best.hi && xk.lo == best.lo && xk.pos >= 0 &&
+                             (best.pos < 0 || xk.pos < best.pos));
+            if (bt) { best = xk; from = idx; }
+        }
+        const PivKey gk = warp_best_key(best);
+        const bool have = gk.pos >= 0;
+        // positions are unique: one lane holds the winning candidate
+        const unsigned ob = __ballot_sync(0xffffffffu, have && best.pos == gk.pos);
+        const int src_idx = __shfl_sync(0xffffffffu, from, ob ? __ffs(ob) - 1 : 0);
+        const int oc = src_idx / NW, ow = src_idx - oc * NW;
+        const int p = have ? gk.pos : k;
+        double pr[NB];
+        {
+            const double2* prow = reinterpret_cast<const double2*>(
+                cluster.map_shared_rank(&cand_row[par][ow][0], (unsigned)oc));
+#pragma unroll
+            for (int c = 0; c < NB / 2; ++c) {
+                const double2 x = have ? prow[c] : make_double2(0.0, 0.0);
+                pr[2 * c] = x.x;
+                pr[2 * c + 1] = x.y;
+            }
+        }
+        double piv = 0.0;
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+            if (c == jj) piv = pr[c];
+        if (leader && st_code == 0) {
+            int s = 0;
+            if (!have || !(key_value(gk) < INFINITY)) s = DEV_NONFINITE;
+            else if (key_value(gk) == 0.0) s = DEV_SINGULAR;
+            if (s) { st_code = s; st_col = k; }
+        }
+        if (piv == 0.0) piv = 1.0;              // the status word records the failure
+        const double inv = 1.0 / piv;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            double vj = 0.0;
+#pragma unroll
+            for (int c = 0; c < NB; ++c)
+                if (c == jj) vj = v[r][c];
+            const double m = vj * inv;
+            const bool isp = have && pos[r] == p;
+            const int pp = pos[r];
+            pos[r] = (pp == p) ? k : (pp == k ? p : pp);
+            if (have) {
+#pragma unroll
+                for (int c = 0; c < NB; ++c)
+                    if (c != jj) v[r][c] = fma(-m, pr[c], v[r][c]);
+            }
+#pragma unroll
+            for (int c = 0; c < NB; ++c)
+                if (c == jj) v[r][c] = -m;
+            if (isp) {
+                // the pivot row becomes the scaled pivot row
+#pragma unroll
+                for (int c = 0; c < NB; ++c) v[r][c] = (c == jj) ? inv : pr[c] * inv;
+            }
+        }
+        if (jj + 1 < nb) publish(par ^ 1, jj + 1, k + 1);
+    }
+    // peers may still be reading this CTA's candidates
+    cluster.sync();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int ps = pos[r];
+        if (ps >= 0) {
+            if (vrow) {
+                double2* wp = reinterpret_cast<double2*>(dst + (size_t)ps * OB + cs);
+#pragma unroll
+                for (int j = 0; j < NB / 2; ++j)
+                    if (2 * j < nb) wp[j] = make_double2(v[r][2 * j], v[r][2 * j + 1]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < NB; ++j)
+                    if (j < nb) dst[(size_t)ps * OB + (cs + j)] = v[r][j];
+            }
+            const int li = tid + r * T;
+            e.sigma[ps] = rbase + li;
+            e.rowid[ps] = lab_s[li];
+            st_out[ps] = stv_s[li];
+        }
+    }
+    if (leader) {
+        e.status[0] = st_code;
+        if (st_col >= 0) e.status[1] = st_col;
+    }
+}
+
 // rank-16 update of the other columns of the 64-column window
 __global__ void __launch_bounds__(U2T)
 gj2_narrow_kernel(const GjEntry* __restrict__ entries, int K, int sub) {
@@ -1307,9 +1517,30 @@ gj_finalize_kernel(const GjEntry* __restrict__ entries, int nsteps_parity, int s
     }
 }
 
+// Cluster shape of the panel for orders above one CTA: CTAs per matrix.
+int gj4_cluster_size(int nmax) { return (nmax + GJ4_ROWS - 1) / GJ4_ROWS; }
+
+// pcfg GJ_PANEL_SHAPES: the cluster panel (RM only), gj4_cluster_size(nmax) CTAs per matrix
 template <bool RM>
 int launch_panel(int pcfg, int count, int pt, size_t smem, cudaStream_t stream, const GjEntry* ent, int K, int sub,
-                 int la) {
+                 int la, int nmax = 0) {
+    if (RM && pcfg == GJ_PANEL_SHAPES) {
+        const int cl = gj4_cluster_size(nmax);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(count * cl), 1, 1);
+        cfg.blockDim = dim3(GJ4_NW * 32, 1, 1);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)cl;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        SCATT_CUDA_TRY(cudaLaunchKernelEx(&cfg, gj4_panel_kernel<GJ4_R, GJ4_NW>, ent, K, sub, la));
+        return SCATT_OK;
+    }
     switch (pcfg) {
         case 0: gj2_panel_kernel<1, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
         case 1: gj2_panel_kernel<2, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
@@ -1353,6 +1584,22 @@ int look_ahead_resources(cudaStream_t main, LookAhead** out) {
 // that holds nmax.  pt = the threads of the launch: ceil(nmax / rows) rounded
 // up to whole warps, at most the shape's warps since nmax <= its capacity.
 int panel_shape(int nmax, int& pcfg, int& pt, int force = -1) {
+    if (nmax > gj_panel_capacity(GJ_PANEL_SHAPES - 1)) {
+        // beyond one CTA: the cluster panel
+        if (force >= 0 && force != GJ_PANEL_SHAPES) {
+            set_last_error("inverse: panel shape " + std::to_string(force) + " does not hold order " +
+                           std::to_string(nmax));
+            return SCATT_ERR_ARG;
+        }
+        if (nmax > GJ4_ROWS * GJ4_CL_MAX) {
+            set_last_error("inverse: order " + std::to_string(nmax) + " exceeds the cluster panel limit " +
+                           std::to_string(GJ4_ROWS * GJ4_CL_MAX));
+            return SCATT_ERR_SIZE;
+        }
+        pcfg = GJ_PANEL_SHAPES;
+        pt = GJ4_NW * 32;
+        return SCATT_OK;
+    }
     if (force >= 0) {
         if (force >= GJ_PANEL_SHAPES || nmax > gj_panel_capacity(force)) {
             set_last_error("inverse: panel shape " + std::to_string(force) + " does not hold order " +
@@ -1496,7 +1743,6 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax, bool sy
 int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax, bool symmetrize,
                         cudaStream_t stream, bool look_ahead, int force_pcfg) {
     if (count <= 0 || nmax <= 0) return SCATT_OK;
-    if (nmax > 1280) return gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream);
     SCATT_TRY(once_per_device(2, [&]() -> int {
         SCATT_CUDA_TRY(cudaFuncSetAttribute(gj3_narrow_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)NARROW3_SMEM));
@@ -1513,7 +1759,7 @@ int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax, bool sy
     int launches = 0;
     auto chain = [&](int K, cudaStream_t st, int la) -> int {
         for (int sub = 0; sub < OB / NB; ++sub) {
-            SCATT_TRY(launch_panel<true>(pcfg, count, pt, lab_smem, st, entries_dev, K, sub, la));
+            SCATT_TRY(launch_panel<true>(pcfg, count, pt, lab_smem, st, entries_dev, K, sub, la, nmax));
             gj3_narrow_kernel<<<dim3(tiles, 1, count), U2T, NARROW3_SMEM, st>>>(entries_dev, K, sub, la);
             launches += 2;
         }

@@ -93,3 +93,44 @@ def test_autotuned_inverse_is_kept_and_exact(n, count):
     for b in range(count):
         ref = np.linalg.inv(A[b])
         assert np.max(np.abs(got[b] - ref)) / np.max(np.abs(ref)) < 1e-12
+
+
+@pytest.mark.parametrize("n", [1281, 2048, 5306])
+def test_inverse_cluster_panel_orders(n):
+    """Orders above one CTA's panel run the cluster panel (CTAs of one
+    thread-block cluster share the pivot search through distributed shared
+    memory); a symmetric and a general batch against numpy."""
+    rng = np.random.default_rng(5000 + n)
+    M = rng.standard_normal((2, n, n))
+    A = M + np.transpose(M, (0, 2, 1)) + 4.0 * np.sqrt(n) * np.eye(n)
+    got, st = _lib.inverse_batched(A, symmetrize=True)
+    assert np.all(st == 0)
+    assert np.array_equal(got[0], got[0].T)
+    for b in range(2):
+        ref = np.linalg.inv(A[b])
+        assert np.max(np.abs(got[b] - ref)) / np.max(np.abs(ref)) < 1e-12, (n, b)
+    if n <= 2048:
+        G = rng.standard_normal((1, n, n)) + 4.0 * np.sqrt(n) * np.eye(n)
+        got, st = _lib.inverse_batched(G, symmetrize=False)
+        assert np.all(st == 0)
+        ref = np.linalg.inv(G[0])
+        assert np.max(np.abs(got[0] - ref)) / np.max(np.abs(ref)) < 1e-12
+
+
+def test_inverse_cluster_panel_pivots_across_ctas():
+    """Zero diagonal under a random row permutation: every pivot sits in a
+    row owned by some other CTA of the cluster than the column's own."""
+    rng = np.random.default_rng(77)
+    n = 2500
+    P = np.eye(n)[rng.permutation(n)]
+    A = P @ (np.diag(rng.uniform(1, 2, n)) + 0.01 * rng.standard_normal((n, n)))
+    A[np.diag_indices(n)] = 0.0
+    got, st = _lib.inverse_batched(A[None], symmetrize=False)
+    assert np.all(st == 0)
+    assert np.max(np.abs(got[0] @ A - np.eye(n))) < 1e-10
+
+
+def test_inverse_cluster_panel_singular_status():
+    inv, st = _lib.inverse_batched(np.ones((2, 1500, 1500)))
+    assert np.all(st[:, 0] == 1)
+    assert np.all(st[:, 1] == 1)

@@ -145,3 +145,18 @@ def test_batch_equals_single_energy_runs():
         one = sol.solve([E], opts=S.default_opts(allow_closed_channels=1, max_batch=1))[0]
         assert rel(one.K_kme, b.K_kme) < 1e-13
         assert rel(one.D, b.D) < 1e-13
+
+
+def test_order_above_one_cta_panel():
+    """N_t = 121 + 10 x 121 = 1331 (l_cont 10, ten occupied orbitals): the
+    R-ratio inverses run on the cluster panel, whose 16-column panels span
+    two CTAs of one thread-block cluster."""
+    inp = synth.h2o_like(Nr=121, dr=0.05, l_cont=10, lmax_orb=12, n_orb=10)
+    st = O.make_setup(inp)
+    sol = S.ScanSolver(inp)
+    E = 0.5
+    g = sol.solve([E], opts=S.default_opts(allow_closed_channels=1))[0]
+    assert g.status == 0
+    r, r2 = oracle_pair(st, E)
+    fails = compare(g, r, r2, "N_t 1331")
+    assert not fails, "\n".join(fails)
