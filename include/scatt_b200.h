@@ -103,23 +103,28 @@ int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call);
  * 1 = single-level (rank-16 updates, row pivoting),
  * 2 = two-level column-major (64-column windows, row pivoting),
  * 3 = two-level on the row-contiguous view of the buffer (pivots by columns
- *     of A, which for a symmetric A is the row-pivoting sequence).
+ *     of A, which for a symmetric A is the row-pivoting sequence),
+ * 4 = scheme 3 with 128-column outer windows (rank-128 trailing updates;
+ *     the allocation-free entry point keeps 64-column windows).
  * All give the same inverse up to rounding.  The setting is process-wide and
  * applies from the next inverse on, also in solves running on other threads. */
 int scatt_set_inverse_blocking(int scheme);
 
-/* Autotuner of the two-level inverses: times scheme 2 and scheme 3 (with and
- * without look-ahead) with every panel shape that holds order n, on a batch
- * of `count` seeded matrices of order n (reps timed calls each), and keeps
- * the fastest for (current device, n, count).  Under the automatic scheme
+/* Autotuner of the two-level inverses: times scheme 2 and scheme 3 (the
+ * latter with and without look-ahead, and with 64- and 128-column windows)
+ * with every panel shape that holds order n, on a batch of `count` seeded
+ * matrices of order n (reps timed calls each), and keeps the fastest for
+ * (current device, n, count).  Under the automatic scheme
  * (scatt_set_inverse_blocking(0)) every later inverse of exactly that order
  * and batch on that device -- the solver's Schur and R^-1 batches included
  * -- uses the kept choice.  Outputs (each may be NULL): the scheme (2 or 3),
- * the panel shape (0..4: 1x8, 2x8, 3x8, 3x12, 5x8 rows per thread x warps),
- * look-ahead (0/1) and the chosen configuration's milliseconds per call.
- * Orders 1..1280.  No counterpart in the reference. */
+ * the panel shape (0..4: 1x8, 2x8, 3x8, 3x12, 5x8 rows per thread x warps;
+ * 5: the cluster panel of orders above 1280), look-ahead (0/1), the window
+ * width (64 or 128) and the chosen configuration's milliseconds per call.
+ * Orders 1..8192 (above 1280 only scheme 3 runs).  No counterpart in the
+ * reference. */
 int scatt_autotune_inverse(int n, int count, int reps, int* scheme, int* panel, int* look_ahead,
-                           double* best_ms);
+                           int* window, double* best_ms);
 
 /* ------------------------------------------- per-step compatibility seam
  * The reference's per-radial-step device interface (GpuForwardStepper,

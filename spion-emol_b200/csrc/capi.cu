@@ -67,7 +67,7 @@ struct InverseBench {
         n = n_;
         count = count_;
         const size_t nn = (size_t)n * n;
-        SCATT_TRY(dP.alloc((size_t)4 * n * 64 * count));
+        SCATT_TRY(dP.alloc((size_t)4 * n * GJ_WINDOW_MAX * count));
         SCATT_TRY(dsg.alloc((size_t)4 * n * count));
         SCATT_TRY(dA.alloc(nn * count));
         SCATT_TRY(dS.alloc(nn * count));
@@ -82,7 +82,7 @@ struct InverseBench {
         for (int b = 0; b < count; ++b)
             ent[b] = GjEntry{dA.p + nn * b, dW.p + nn * b, dO.p + nn * b, dsig.p + (size_t)n * b,
                              drid.p + (size_t)n * b, dst.p + 2 * b, n, n, n,
-                             dP.p + (size_t)4 * n * 64 * b, dsg.p + (size_t)4 * n * b};
+                             dP.p + (size_t)4 * n * GJ_WINDOW_MAX * b, dsg.p + (size_t)4 * n * b};
         return dent.upload(ent);
     }
 
@@ -164,7 +164,7 @@ int scatt_inverse_batched(int n, int count, const double* A, double* out, int sy
     SCATT_TRY(dA.alloc(nn * count));
     SCATT_TRY(dW.alloc(nn * count));
     SCATT_TRY(dO.alloc(nn * count));
-    SCATT_TRY(dP.alloc((size_t)4 * n * 64 * count));
+    SCATT_TRY(dP.alloc((size_t)4 * n * GJ_WINDOW_MAX * count));
     SCATT_TRY(dsig.alloc((size_t)n * count));
     SCATT_TRY(drid.alloc((size_t)n * count));
     SCATT_TRY(dsg.alloc((size_t)4 * n * count));
@@ -175,7 +175,7 @@ int scatt_inverse_batched(int n, int count, const double* A, double* out, int sy
     for (int b = 0; b < count; ++b) {
         ent[b] = GjEntry{dA.p + nn * b, dW.p + nn * b, dO.p + nn * b, dsig.p + (size_t)n * b,
                          drid.p + (size_t)n * b, dst.p + 2 * b, n, n, n,
-                         dP.p + (size_t)4 * n * 64 * b, dsg.p + (size_t)4 * n * b};
+                         dP.p + (size_t)4 * n * GJ_WINDOW_MAX * b, dsg.p + (size_t)4 * n * b};
     }
     DevBuf<GjEntry> dent;
     SCATT_TRY(dent.upload(ent));
@@ -227,8 +227,8 @@ int scatt_dgemm(int opA, int opB, int M, int N, int K, double alpha, const doubl
 
 
 int scatt_set_inverse_blocking(int scheme) {
-    if (scheme < 0 || scheme > 3) {
-        set_last_error("scatt_set_inverse_blocking: scheme must be 0, 1, 2 or 3");
+    if (scheme < 0 || scheme > 4) {
+        set_last_error("scatt_set_inverse_blocking: scheme must be 0, 1, 2, 3 or 4");
         return SCATT_ERR_ARG;
     }
     g_inverse_scheme.store(scheme, std::memory_order_relaxed);
@@ -243,9 +243,10 @@ int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call) {
     return bench.time(reps, ms_per_call, [&]() { return gj_inverse_selected(bench.dent.p, count, n, true, 0, true); });
 }
 
-int scatt_autotune_inverse(int n, int count, int reps, int* scheme, int* panel, int* look_ahead, double* best_ms) {
-    if (n <= 0 || n > 1280 || count <= 0 || reps <= 0) {
-        set_last_error("scatt_autotune_inverse: order must be in [1, 1280], batch and reps positive");
+int scatt_autotune_inverse(int n, int count, int reps, int* scheme, int* panel, int* look_ahead, int* window,
+                           double* best_ms) {
+    if (n <= 0 || n > 8192 || count <= 0 || reps <= 0) {
+        set_last_error("scatt_autotune_inverse: order must be in [1, 8192], batch and reps positive");
         return SCATT_ERR_ARG;
     }
     SCATT_TRY(require_device());
@@ -255,27 +256,32 @@ int scatt_autotune_inverse(int n, int count, int reps, int* scheme, int* panel, 
     SCATT_TRY(bench.setup(n, count));
     InverseTune best;
     double best_t = 1e300;
-    for (int sch = 2; sch <= 3; ++sch)
-        for (int p = 0; p < GJ_PANEL_SHAPES; ++p) {
-            if (n > gj_panel_capacity(p)) continue;
-            for (int la = 0; la <= (sch == 3 ? 1 : 0); ++la) {
-                double ms = 0.0;
-                SCATT_TRY(bench.time(reps, &ms, [&]() {
-                    return sch == 3 ? gj_inverse_batched3(bench.dent.p, count, n, true, 0, la != 0, p)
-                                    : gj_inverse_batched2(bench.dent.p, count, n, true, 0, p);
-                }));
-                if (ms < best_t) {
-                    best_t = ms;
-                    best.scheme = sch;
-                    best.pcfg = p;
-                    best.look_ahead = la;
+    // above one CTA's panel (1280 rows) only the row-contiguous scheme with the cluster panel runs
+    const bool cluster = n > gj_panel_capacity(GJ_PANEL_SHAPES - 1);
+    for (int sch = cluster ? 3 : 2; sch <= 3; ++sch)
+        for (int p = 0; p <= GJ_PANEL_SHAPES; ++p) {
+            if (cluster ? p != GJ_PANEL_SHAPES : (p == GJ_PANEL_SHAPES || n > gj_panel_capacity(p))) continue;
+            for (int la = 0; la <= (sch == 3 ? 1 : 0); ++la)
+                for (int w = 64; w <= (sch == 3 ? GJ_WINDOW_MAX : 64); w *= 2) {
+                    double ms = 0.0;
+                    SCATT_TRY(bench.time(reps, &ms, [&]() {
+                        return sch == 3 ? gj_inverse_batched3(bench.dent.p, count, n, true, 0, la != 0, p, w)
+                                        : gj_inverse_batched2(bench.dent.p, count, n, true, 0, p);
+                    }));
+                    if (ms < best_t) {
+                        best_t = ms;
+                        best.scheme = sch;
+                        best.pcfg = p;
+                        best.look_ahead = la;
+                        best.window = w;
+                    }
                 }
-            }
         }
     inverse_tune_store(dev, n, count, best);
     if (scheme) *scheme = best.scheme;
     if (panel) *panel = best.pcfg;
     if (look_ahead) *look_ahead = best.look_ahead;
+    if (window) *window = best.window;
     if (best_ms) *best_ms = best_t;
     return SCATT_OK;
 }

@@ -89,7 +89,7 @@ struct GjEntry {
     int*    rowid;    // n ints: original row index at each position
     int*    status;   // 1 int: DeviceStatus (first failing column in status[1])
     int n, ld, ldo;
-    double* P = nullptr;   // optional panel-window buffers, 2 x (ld x 64) (4 x with look-ahead)
+    double* P = nullptr;   // optional panel-window buffers, 2 x (ld x window) (4 x with look-ahead)
     int*    sigt = nullptr; // optional composite row maps of the 64-column window (2 n, 4 n with look-ahead)
 };
 
@@ -113,12 +113,19 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax,
 // is treated as the row-major B = A^T (inv(A) = inv(B)^T), so pivot rows and
 // window rows are contiguous runs.  Pivoting is partial pivoting on B, i.e.
 // by columns of A; for symmetric A it is the row-pivoting sequence of A.
-// With look_ahead the 16-column panels of the next 64-column window run on a
-// high-priority side stream beside the trailing update of the current one;
-// then every entry needs P of 4 x ld x 64 doubles and sigt of 4 n ints
-// (without it, 2 x ld x 64 and 2 n as for gj_inverse_batched2).
+// `window` (64 or 128) is the width of the outer step: a 128-column window
+// halves the trailing updates' C-tile traffic per flop.  With look_ahead the
+// 16-column panels of the next window run on a high-priority side stream
+// beside the trailing update of the current one; then every entry needs P of
+// 4 x ld x window doubles and sigt of 4 n ints (without it, 2 x ld x window
+// and 2 n).  Orders above 1280 run the panels on a thread-block cluster.
 int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax,
-                        bool symmetrize, cudaStream_t stream, bool look_ahead, int pcfg = -1);
+                        bool symmetrize, cudaStream_t stream, bool look_ahead, int pcfg = -1,
+                        int window = 64);
+
+// Widest window of the two-level inverses; entries carrying P of 4 x ld x
+// GJ_WINDOW_MAX doubles fit every choice.
+constexpr int GJ_WINDOW_MAX = 128;
 
 // Panel shapes of the two-level inverses, as rows per thread x warps: 1x8,
 // 2x8, 3x8, 3x12, 5x8.  Shape p factors panels of up to gj_panel_capacity(p)
@@ -129,12 +136,13 @@ inline int gj_panel_capacity(int pcfg) {
     return cap[pcfg];
 }
 
-// A measured choice of scheme (2 or 3), panel shape and look-ahead for one
-// (device, order, batch).  The autotuner (scatt_autotune_inverse) stores
-// them; the automatic scheme uses a stored choice for an exact match of the
-// current device, order and batch, and its fixed rule otherwise.
+// A measured choice of scheme (2 or 3), panel shape, look-ahead and window
+// width for one (device, order, batch).  The autotuner
+// (scatt_autotune_inverse) stores them; the automatic scheme uses a stored
+// choice for an exact match of the current device, order and batch, and its
+// fixed rule otherwise.
 struct InverseTune {
-    int scheme = 0, pcfg = -1, look_ahead = 1;
+    int scheme = 0, pcfg = -1, look_ahead = 1, window = 64;
 };
 bool inverse_tune_lookup(int n, int count, InverseTune* out);
 void inverse_tune_store(int device, int n, int count, const InverseTune& t);
@@ -142,25 +150,31 @@ void inverse_tune_store(int device, int n, int count, const InverseTune& t);
 // Scheme of every dense inverse (entry points and solver): 0 = automatic
 // (row-contiguous two-level above order 512, where its contiguous pivot-row
 // tiles pay; column-major two-level below), 1 = single-level,
-// 2 = column-major two-level, 3 = row-contiguous two-level.  Process-wide;
+// 2 = column-major two-level, 3 = row-contiguous two-level, 4 = scheme 3
+// with 128-column windows (where the entries' buffers hold them).  Process-wide;
 // atomic because it may be set while another thread solves (a call reads it
 // once per inverse, so a change applies from the next inverse on).
 extern std::atomic<int> g_inverse_scheme;
 
 // The scheme selected by g_inverse_scheme (entries must carry P and sigt).
-// look_ahead: as for gj_inverse_batched3 (entries sized for it).
+// look_ahead: as for gj_inverse_batched3 (entries sized for it); wcap: the
+// widest window the entries' P holds (64 or GJ_WINDOW_MAX).
 inline int gj_inverse_selected(const GjEntry* entries_dev, int count, int nmax,
-                               bool symmetrize, cudaStream_t stream, bool look_ahead) {
+                               bool symmetrize, cudaStream_t stream, bool look_ahead,
+                               int wcap = GJ_WINDOW_MAX) {
     switch (g_inverse_scheme.load(std::memory_order_relaxed)) {
         case 1: return gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream);
         case 2: return gj_inverse_batched2(entries_dev, count, nmax, symmetrize, stream);
         case 3: return gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream, look_ahead);
+        case 4: return gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream, look_ahead, -1,
+                                           wcap >= 128 ? 128 : 64);
         default: {
             InverseTune t;
             if (inverse_tune_lookup(nmax, count, &t)) {
                 if (t.scheme == 3)
                     return gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream,
-                                               look_ahead && t.look_ahead, t.pcfg);
+                                               look_ahead && t.look_ahead, t.pcfg,
+                                               t.window <= wcap ? t.window : 64);
                 return gj_inverse_batched2(entries_dev, count, nmax, symmetrize, stream, t.pcfg);
             }
             return nmax > 512 ? gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream, look_ahead)

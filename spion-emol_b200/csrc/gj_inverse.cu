@@ -481,24 +481,28 @@ __device__ __forceinline__ double* win_out(const GjEntry& e, int s) {
 
 // Row-contiguous layout (RM): the column-major buffer of A is read as the
 // row-major B = A^T, so row i of B (column i of A) is contiguous.  A window is
-// 64 columns of B; the window buffers P hold it row-major with row stride OB.
+// W columns of B (W = 64 or 128); the window buffers P hold it row-major with
+// row stride W.
 // Element (row i, window column c) of the window input / output:
 // With look-ahead (la = 1) the window buffers and the composite row maps come
 // in two sets selected by the parity of the outer step, so the chain of the
 // next window never touches what the current trailing update reads.
+template <int W>
 __device__ __forceinline__ double* win_set_rm(const GjEntry& e, int K, int la) {
-    return e.P + (size_t)(la ? 2 * (K & 1) : 0) * e.ld * OB;
+    return e.P + (size_t)(la ? 2 * (K & 1) : 0) * e.ld * W;
 }
 __device__ __forceinline__ int* sigt_set(const GjEntry& e, int K, int la) {
     return e.sigt + (size_t)(la ? 2 * (K & 1) : 0) * e.n;
 }
+template <int W>
 __device__ __forceinline__ const double* win_in_rm(const GjEntry& e, int K, int s, int& lds, int la) {
-    if (s == 0) { lds = e.ld; return buf_of(e, K & 1) + (size_t)K * OB; }
-    lds = OB;
-    return win_set_rm(e, K, la) + (size_t)(s & 1) * e.ld * OB;
+    if (s == 0) { lds = e.ld; return buf_of(e, K & 1) + (size_t)K * W; }
+    lds = W;
+    return win_set_rm<W>(e, K, la) + (size_t)(s & 1) * e.ld * W;
 }
+template <int W>
 __device__ __forceinline__ double* win_out_rm(const GjEntry& e, int K, int s, int la) {
-    return win_set_rm(e, K, la) + (size_t)((s + 1) & 1) * e.ld * OB;
+    return win_set_rm<W>(e, K, la) + (size_t)((s + 1) & 1) * e.ld * W;
 }
 
 // Panel of 16 columns of the 64-column window, one CTA (NW warps) per matrix.
@@ -544,24 +548,24 @@ __device__ __forceinline__ double key_value(const PivKey& k) {
     return __longlong_as_double(static_cast<long long>((static_cast<unsigned long long>(k.hi - 1u) << 32) | k.lo));
 }
 
-template <int R, int NW, bool RM>
+template <int R, int NW, bool RM, int WIN>
 __global__ void __launch_bounds__(NW * 32, 1)
 gj2_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub, int la) {
     const GjEntry e = entries[blockIdx.x];
     const int n = e.n;
-    const int k0o = K * OB;
+    const int k0o = K * WIN;
     if (k0o >= n) return;
-    const int nb64 = min(OB, n - k0o);
+    const int nb64 = min(WIN, n - k0o);
     const int cs = sub * NB;
     if (cs >= nb64) return;
     const int nb = min(NB, nb64 - cs);
     const int kr0 = k0o + cs;
     int lds = e.ld;
-    const double* src = RM ? win_in_rm(e, K, sub, lds, la) : win_in(e, K, sub);
-    double* dst = RM ? win_out_rm(e, K, sub, la) : win_out(e, sub);
+    const double* src = RM ? win_in_rm<WIN>(e, K, sub, lds, la) : win_in(e, K, sub);
+    double* dst = RM ? win_out_rm<WIN>(e, K, sub, la) : win_out(e, sub);
     // (row i, window column c) -> element offset
     const size_t rs = RM ? (size_t)lds : 1, cst = RM ? 1 : (size_t)lds;
-    const size_t drs = RM ? (size_t)OB : 1, dcs = RM ? 1 : (size_t)e.ld;
+    const size_t drs = RM ? (size_t)WIN : 1, dcs = RM ? 1 : (size_t)e.ld;
     const int T = blockDim.x, W = T >> 5;
     const bool first = (K == 0 && sub == 0);
     // row-contiguous view: whole 16-byte pairs when the row stride and the column count are even
@@ -770,7 +774,7 @@ constexpr int GJ4_R = 4, GJ4_NW = 8;
 constexpr int GJ4_ROWS = GJ4_R * GJ4_NW * 32;        // rows per CTA
 constexpr int GJ4_CL_MAX = 8;                       // portable cluster size
 
-template <int R, int NW>
+template <int R, int NW, int W>
 __global__ void __launch_bounds__(NW * 32, 1)
 gj4_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub, int la) {
     namespace cg = cooperative_groups;
@@ -779,16 +783,16 @@ gj4_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub, int la) {
     const int crank = (int)cluster.block_rank();
     const GjEntry e = entries[blockIdx.x / CL];
     const int n = e.n;
-    const int k0o = K * OB;
+    const int k0o = K * W;
     if (k0o >= n) return;
-    const int nb64 = min(OB, n - k0o);
+    const int nb64 = min(W, n - k0o);
     const int cs = sub * NB;
     if (cs >= nb64) return;
     const int nb = min(NB, nb64 - cs);
     const int kr0 = k0o + cs;
     int lds = e.ld;
-    const double* src = win_in_rm(e, K, sub, lds, la);
-    double* dst = win_out_rm(e, K, sub, la);
+    const double* src = win_in_rm<W>(e, K, sub, lds, la);
+    double* dst = win_out_rm<W>(e, K, sub, la);
     const size_t rs = (size_t)lds;
     constexpr int T = NW * 32;
     constexpr int RC = R * T;
@@ -938,14 +942,14 @@ gj4_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub, int la) {
         const int ps = pos[r];
         if (ps >= 0) {
             if (vrow) {
-                double2* wp = reinterpret_cast<double2*>(dst + (size_t)ps * OB + cs);
+                double2* wp = reinterpret_cast<double2*>(dst + (size_t)ps * W + cs);
 #pragma unroll
                 for (int j = 0; j < NB / 2; ++j)
                     if (2 * j < nb) wp[j] = make_double2(v[r][2 * j], v[r][2 * j + 1]);
             } else {
 #pragma unroll
                 for (int j = 0; j < NB; ++j)
-                    if (j < nb) dst[(size_t)ps * OB + (cs + j)] = v[r][j];
+                    if (j < nb) dst[(size_t)ps * W + (cs + j)] = v[r][j];
             }
             const int li = tid + r * T;
             e.sigma[ps] = rbase + li;
@@ -1185,27 +1189,31 @@ constexpr int N3S = 20;      // row stride of the 64 x 16 multiplier tile (= 4 m
 constexpr int T3R = 68;      // row stride of the 64-wide tiles (= 4 mod 16)
 constexpr size_t NARROW3_SMEM = (64 * T3R + 64 * N3S + NB * T3R) * sizeof(double);
 
-// rank-16 update of the other columns of the 64-column window (RM layout):
+// rank-16 update of the other columns of the W-column window (RM layout),
+// one 64 x 64 tile (rows blockIdx.x, window columns blockIdx.y) per CTA:
 //   out[i, c] = (i a pivot position of this panel ? 0 : in[sigma(i), c])
 //               + sum_j Mp[i, j] in[sigma(kr0 + j), c]
+template <int W>
 __global__ void __launch_bounds__(U2T)
 gj3_narrow_kernel(const GjEntry* __restrict__ entries, int K, int sub, int la) {
     const GjEntry e = entries[blockIdx.z];
     const int n = e.n;
-    const int k0o = K * OB;
+    const int k0o = K * W;
     if (k0o >= n) return;
-    const int nb64 = min(OB, n - k0o);
+    const int nbw = min(W, n - k0o);
     const int cs = sub * NB;
-    if (cs >= nb64) return;
-    const int nb = min(NB, nb64 - cs);
+    if (cs >= nbw) return;
+    const int nb = min(NB, nbw - cs);
     const int kr0 = k0o + cs;
     const int r0 = blockIdx.x * 64;
-    if (r0 >= n) return;
+    const int cw = blockIdx.y * 64;           // first window column of this tile
+    if (r0 >= n || cw >= nbw) return;
+    const int nb64 = min(64, nbw - cw);       // window columns of this tile
     int lds;
-    const double* src = win_in_rm(e, K, sub, lds, la);
-    double* dst = win_out_rm(e, K, sub, la);
+    const double* src = win_in_rm<W>(e, K, sub, lds, la) + cw;
+    double* dst = win_out_rm<W>(e, K, sub, la);
     // 16-byte rows need an even stride; the big buffer also needs whole pairs inside the window
-    const bool v16 = (lds % 2 == 0) && (sub > 0 || nb64 % 2 == 0);
+    const bool v16 = (lds % 2 == 0) && (sub > 0 || nbw % 2 == 0);
 
     extern __shared__ double n3smem[];
     double (*Cs)[T3R] = reinterpret_cast<double (*)[T3R]>(n3smem);
@@ -1254,12 +1262,12 @@ gj3_narrow_kernel(const GjEntry* __restrict__ entries, int K, int sub, int la) {
         }
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {                  // Mp: 64 rows x 16 (panel output, stride OB)
+    for (int u = 0; u < 4; ++u) {                  // Mp: 64 rows x 16 (panel output, stride W)
         const int idx = tid + u * U2T;
         const int m = idx >> 4, j = idx & 15;
         const int gi = r0 + m;
         const bool ok = gi < n && j < nb;
-        cp_async8(&Ms[m][j], dst + (ok ? (size_t)gi * OB + cs + j : 0), ok);
+        cp_async8(&Ms[m][j], dst + (ok ? (size_t)gi * W + cs + j : 0), ok);
     }
     cp_async_wait_all();
     __syncthreads();
@@ -1297,7 +1305,8 @@ gj3_narrow_kernel(const GjEntry* __restrict__ entries, int K, int sub, int la) {
             for (int v = 0; v < 4; ++v) {
                 const int gi = r0 + wm + i * 16 + g + ((v >> 1) << 3);
                 const int c = wn + jn * 8 + 2 * t + (v & 1);
-                if (gi < n && c < nb64 && !(c >= cs && c < cs + nb)) dst[(size_t)gi * OB + c] = acc[i][jn][v];
+                if (gi < n && c < nb64 && !(cw + c >= cs && cw + c < cs + nb))
+                    dst[(size_t)gi * W + cw + c] = acc[i][jn][v];
             }
 }
 
@@ -1327,7 +1336,7 @@ gj3_trail_kernel(const GjEntry* __restrict__ entries, int K, int la, int cols) {
     const size_t ld = e.ld;
     const double* src = buf_of(e, K & 1);
     double* dst = buf_of(e, (K + 1) & 1);
-    const double* Mw = win_set_rm(e, K, la) + (size_t)(nsub & 1) * e.ld * OB;
+    const double* Mw = win_set_rm<OB>(e, K, la) + (size_t)(nsub & 1) * e.ld * OB;
     const int* st = sigt_set(e, K, la) + (size_t)(nsub & 1) * n;
     const int tid = threadIdx.x;
     if (c0 == k0) {
@@ -1468,17 +1477,194 @@ gj3_trail_kernel(const GjEntry* __restrict__ entries, int K, int la, int cols) {
         }
 }
 
+// rank-128 update for 128-column windows (RM layout), one 128 x 64 C tile per
+// CTA, 8 warps of 32 x 32 DMMA, 2 CTAs per SM.  Twice the flops of the
+// rank-64 update for the same C-tile load and store.  The k dimension (the
+// window's columns) streams through a two-stage cp.async ring of 32-column
+// stages (M: 128 x 32, X: 32 x 64), so a stage lands while the previous one
+// is multiplied; the C tile goes straight from the old matrix into the
+// accumulators meanwhile.
+// Column tiles: blockIdx.y + ct_lo, moved past [skip_lo, skip_lo + skip_n).
+constexpr int T3K = 32;                      // window columns per stage
+constexpr int T3KS = 36;                     // row stride of the M stage (= 4 mod 16)
+constexpr int T3STAGE = T3M * T3KS + T3K * T3R;
+constexpr size_t TRAIL128_SMEM = 2 * (size_t)T3STAGE * sizeof(double);
+
+__global__ void __launch_bounds__(U2T, 2)
+gj3_trail128_kernel(const GjEntry* __restrict__ entries, int K, int la, int ct_lo, int skip_lo, int skip_n) {
+    constexpr int W = 128;
+    const GjEntry e = entries[blockIdx.z];
+    const int n = e.n;
+    const int k0 = K * W;
+    if (k0 >= n) return;
+    const int nbw = min(W, n - k0);
+    const int nsub = (nbw + NB - 1) / NB;
+    int ct = ct_lo + (int)blockIdx.y;
+    if (skip_n > 0 && ct >= skip_lo) ct += skip_n;
+    const int r0 = blockIdx.x * T3M, c0 = ct * 64;
+    if (r0 >= n || c0 >= n) return;
+    const size_t ld = e.ld;
+    const double* src = buf_of(e, K & 1);
+    double* dst = buf_of(e, (K + 1) & 1);
+    const double* Mw = win_set_rm<W>(e, K, la) + (size_t)(nsub & 1) * e.ld * W;
+    const int* st = sigt_set(e, K, la) + (size_t)(nsub & 1) * n;
+    const int tid = threadIdx.x;
+    if (c0 >= k0 && c0 < k0 + nbw) {
+        // a column tile of the window itself: the transformed window
+        const int cw = c0 - k0;
+        for (int idx = tid; idx < T3M * 64; idx += U2T) {
+            const int row = idx >> 6, col = idx & 63;
+            const int gi = r0 + row;
+            if (gi < n && cw + col < nbw) dst[gi * ld + c0 + col] = Mw[(size_t)gi * W + cw + col];
+        }
+        return;
+    }
+    const bool v16 = (ld % 2 == 0);          // n even: pairs never straddle a row end
+    const bool m16 = (nbw % 2 == 0);         // whole pairs inside the window
+    extern __shared__ double t128smem[];
+    __shared__ int srow[T3M];
+    __shared__ int xrow[W];
+    if (tid < T3M) srow[tid] = (r0 + tid < n) ? st[r0 + tid] : 0;
+    else if (tid < T3M + W) {
+        const int j = tid - T3M;
+        xrow[j] = (j < nbw) ? st[k0 + j] : 0;
+    }
+    __syncthreads();
+    const int nch = (nbw + T3K - 1) / T3K;
+    // stage s: M rows at t128smem + s * T3STAGE (stride T3KS), X rows after them (stride T3R)
+    auto issue = [&](int ch) {
+        double* Ms = t128smem + (size_t)(ch & 1) * T3STAGE;
+        double* Xs = Ms + T3M * T3KS;
+        const int kb = ch * T3K;
+        if (m16) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {          // M: 128 rows x 16 pairs
+                const int idx = tid + u * U2T;
+                const int m = idx >> 4, j = 2 * (idx & 15);
+                const int gi = r0 + m;
+                const bool ok = gi < n && kb + j < nbw;
+                cp_async16(Ms + m * T3KS + j, Mw + (ok ? (size_t)gi * W + kb + j : 0), ok);
+            }
+        } else {
+#pragma unroll 4
+            for (int u = 0; u < 16; ++u) {
+                const int idx = tid + u * U2T;
+                const int m = idx >> 5, j = idx & 31;
+                const int gi = r0 + m;
+                const bool ok = gi < n && kb + j < nbw;
+                cp_async8(Ms + m * T3KS + j, Mw + (ok ? (size_t)gi * W + kb + j : 0), ok);
+            }
+        }
+        if (v16) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {          // X: 32 pivot rows x 32 pairs
+                const int idx = tid + u * U2T;
+                const int j = idx >> 5, c = 2 * (idx & 31);
+                const bool ok = kb + j < nbw && c0 + c < n;
+                cp_async16(Xs + j * T3R + c, src + (ok ? (size_t)xrow[kb + j] * ld + c0 + c : 0), ok);
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int idx = tid + u * U2T;
+                const int j = idx >> 6, c = idx & 63;
+                const bool ok = kb + j < nbw && c0 + c < n;
+                cp_async8(Xs + j * T3R + c, src + (ok ? (size_t)xrow[kb + j] * ld + c0 + c : 0), ok);
+            }
+        }
+        cp_async_commit();
+    };
+    issue(0);
+    if (nch > 1) issue(1);
+    const int lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
+    double acc[2][4][4];
+    // C tile straight from the old matrix into the accumulators
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int rl = wm + i * 16 + g + 8 * h;
+            const int gi = r0 + rl;
+            const bool rok = gi < n && !(gi >= k0 && gi < k0 + nbw);
+            const double* rowp = src + (size_t)srow[rl] * ld + c0;
+#pragma unroll
+            for (int jn = 0; jn < 4; ++jn) {
+                const int c = wn + jn * 8 + 2 * t;
+                double x0 = 0.0, x1 = 0.0;
+                if (rok && c0 + c < n) {
+                    if (v16) {
+                        const double2 p2 = *reinterpret_cast<const double2*>(rowp + c);
+                        x0 = p2.x; x1 = p2.y;
+                    } else {
+                        x0 = rowp[c];
+                        if (c0 + c + 1 < n) x1 = rowp[c + 1];
+                    }
+                }
+                acc[i][jn][2 * h] = x0;
+                acc[i][jn][2 * h + 1] = x1;
+            }
+        }
+#pragma unroll 1
+    for (int ch = 0; ch < nch; ++ch) {
+        if (ch + 1 < nch) cp_async_wait<1>();
+        else cp_async_wait<0>();
+        __syncthreads();
+        const double* Ms = t128smem + (size_t)(ch & 1) * T3STAGE;
+        const double* Xs = Ms + T3M * T3KS;
+#pragma unroll
+        for (int kq = 0; kq < T3K; kq += 4) {
+            double a[2][2], b[4];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                a[i][0] = Ms[(wm + i * 16 + g) * T3KS + kq + t];
+                a[i][1] = Ms[(wm + i * 16 + g + 8) * T3KS + kq + t];
+            }
+#pragma unroll
+            for (int jn = 0; jn < 4; ++jn) b[jn] = Xs[(kq + t) * T3R + wn + jn * 8 + g];
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int jn = 0; jn < 4; ++jn) dmma_16x8x4(acc[i][jn], a[i][0], a[i][1], b[jn]);
+        }
+        if (ch + 2 < nch) {
+            __syncthreads();                         // every warp is done with this stage
+            issue(ch + 2);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int gi = r0 + wm + i * 16 + g + 8 * h;
+            if (gi >= n) continue;
+            double* rowp = dst + (size_t)gi * ld + c0;
+#pragma unroll
+            for (int jn = 0; jn < 4; ++jn) {
+                const int c = wn + jn * 8 + 2 * t;
+                if (c0 + c >= n) continue;
+                if (v16) {
+                    *reinterpret_cast<double2*>(rowp + c) = make_double2(acc[i][jn][2 * h], acc[i][jn][2 * h + 1]);
+                } else {
+                    rowp[c] = acc[i][jn][2 * h];
+                    if (c0 + c + 1 < n) rowp[c + 1] = acc[i][jn][2 * h + 1];
+                }
+            }
+        }
+}
+
 constexpr int FT = 32;
 
 __global__ void __launch_bounds__(FT * 8)
-gj_finalize_kernel(const GjEntry* __restrict__ entries, int nsteps_parity, int symmetrize, int rm) {
-    // nsteps_parity: 0 = single-level (16-column steps), 1 = two-level (64-column steps)
+gj_finalize_kernel(const GjEntry* __restrict__ entries, int wstep, int symmetrize, int rm) {
+    // wstep: columns per block step (16 single-level, 64 or 128 two-level)
     const GjEntry e = entries[blockIdx.z];
     const int n = e.n;
     const int i0 = blockIdx.x * FT, j0 = blockIdx.y * FT;
     if (i0 >= n || j0 >= n) return;
     // the result of the last block step lives in buffer (number of steps of this matrix) % 2
-    const int steps = nsteps_parity ? (n + OB - 1) / OB : (n + NB - 1) / NB;
+    const int steps = (n + wstep - 1) / wstep;
     const double* X = buf_of(e, steps & 1);
 
     __shared__ int pi_i[FT], pi_j[FT];
@@ -1520,8 +1706,9 @@ gj_finalize_kernel(const GjEntry* __restrict__ entries, int nsteps_parity, int s
 // Cluster shape of the panel for orders above one CTA: CTAs per matrix.
 int gj4_cluster_size(int nmax) { return (nmax + GJ4_ROWS - 1) / GJ4_ROWS; }
 
-// pcfg GJ_PANEL_SHAPES: the cluster panel (RM only), gj4_cluster_size(nmax) CTAs per matrix
-template <bool RM>
+// pcfg GJ_PANEL_SHAPES: the cluster panel (RM only), gj4_cluster_size(nmax) CTAs per matrix;
+// W: window width (64 for the column-major scheme)
+template <bool RM, int W>
 int launch_panel(int pcfg, int count, int pt, size_t smem, cudaStream_t stream, const GjEntry* ent, int K, int sub,
                  int la, int nmax = 0) {
     if (RM && pcfg == GJ_PANEL_SHAPES) {
@@ -1538,15 +1725,15 @@ int launch_panel(int pcfg, int count, int pt, size_t smem, cudaStream_t stream, 
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        SCATT_CUDA_TRY(cudaLaunchKernelEx(&cfg, gj4_panel_kernel<GJ4_R, GJ4_NW>, ent, K, sub, la));
+        SCATT_CUDA_TRY(cudaLaunchKernelEx(&cfg, gj4_panel_kernel<GJ4_R, GJ4_NW, W>, ent, K, sub, la));
         return SCATT_OK;
     }
     switch (pcfg) {
-        case 0: gj2_panel_kernel<1, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
-        case 1: gj2_panel_kernel<2, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
-        case 2: gj2_panel_kernel<3, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
-        case 3: gj2_panel_kernel<3, 12, RM><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
-        default: gj2_panel_kernel<5, 8, RM><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
+        case 0: gj2_panel_kernel<1, 8, RM, W><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
+        case 1: gj2_panel_kernel<2, 8, RM, W><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
+        case 2: gj2_panel_kernel<3, 8, RM, W><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
+        case 3: gj2_panel_kernel<3, 12, RM, W><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
+        default: gj2_panel_kernel<5, 8, RM, W><<<count, pt, smem, stream>>>(ent, K, sub, la); break;
     }
     return SCATT_OK;
 }
@@ -1687,7 +1874,7 @@ int gj_inverse_batched(const GjEntry* entries_dev, int count, int nmax,
         gj_update2_kernel<<<ugrid, U2T, U2_SMEM, stream>>>(entries_dev, kb);
     }
     const int ft = (nmax + FT - 1) / FT;
-    gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, 0, symmetrize ? 1 : 0, 0);
+    gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, NB, symmetrize ? 1 : 0, 0);
     SCATT_CUDA_TRY(cudaGetLastError());
     SCATT_COUNT_LAUNCH(2 * steps + 1);
     return SCATT_OK;
@@ -1726,7 +1913,7 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax, bool sy
     int launches = 0;
     for (int K = 0; K < outer; ++K) {
         for (int sub = 0; sub < OB / NB; ++sub) {
-            SCATT_TRY(launch_panel<false>(pcfg, count, pt, lab_smem, stream, entries_dev, K, sub, 0));
+            SCATT_TRY((launch_panel<false, OB>(pcfg, count, pt, lab_smem, stream, entries_dev, K, sub, 0)));
             gj2_narrow_kernel<<<dim3(tiles, 1, count), U2T, U2_SMEM, stream>>>(entries_dev, K, sub);
             launches += 2;
         }
@@ -1734,42 +1921,51 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax, bool sy
         ++launches;
     }
     const int ft = (nmax + FT - 1) / FT;
-    gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, 1, symmetrize ? 1 : 0, 0);
+    gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, OB, symmetrize ? 1 : 0, 0);
     SCATT_CUDA_TRY(cudaGetLastError());
     SCATT_COUNT_LAUNCH(launches + 1);
     return SCATT_OK;
 }
 
-int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax, bool symmetrize,
-                        cudaStream_t stream, bool look_ahead, int force_pcfg) {
-    if (count <= 0 || nmax <= 0) return SCATT_OK;
-    SCATT_TRY(once_per_device(2, [&]() -> int {
-        SCATT_CUDA_TRY(cudaFuncSetAttribute(gj3_narrow_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)NARROW3_SMEM));
-        SCATT_CUDA_TRY(cudaFuncSetAttribute(gj3_trail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)TRAIL3_SMEM));
-        return SCATT_OK;
-    }));
-    const int outer = (nmax + OB - 1) / OB;
+namespace {
+
+// The row-contiguous two-level inverse with W-column windows.
+template <int W>
+int batched3_window(const GjEntry* entries_dev, int count, int nmax, bool symmetrize, cudaStream_t stream,
+                    bool look_ahead, int force_pcfg) {
+    const int outer = (nmax + W - 1) / W;
     const int tiles = (nmax + 63) / 64;
     const int mtiles = (nmax + T3M - 1) / T3M;
+    constexpr int WT = W / 64;                   // 64-column tiles per window
     int pcfg, pt;
     SCATT_TRY(panel_shape(nmax, pcfg, pt, force_pcfg));
     const size_t lab_smem = 2 * (size_t)nmax * sizeof(int);
     int launches = 0;
     auto chain = [&](int K, cudaStream_t st, int la) -> int {
-        for (int sub = 0; sub < OB / NB; ++sub) {
-            SCATT_TRY(launch_panel<true>(pcfg, count, pt, lab_smem, st, entries_dev, K, sub, la, nmax));
-            gj3_narrow_kernel<<<dim3(tiles, 1, count), U2T, NARROW3_SMEM, st>>>(entries_dev, K, sub, la);
+        for (int sub = 0; sub < W / NB; ++sub) {
+            SCATT_TRY((launch_panel<true, W>(pcfg, count, pt, lab_smem, st, entries_dev, K, sub, la, nmax)));
+            gj3_narrow_kernel<W><<<dim3(tiles, WT, count), U2T, NARROW3_SMEM, st>>>(entries_dev, K, sub, la);
             launches += 2;
         }
         return SCATT_OK;
     };
+    // trailing update of window K over column tiles [lo, lo + cnt), skipping [skip_lo, skip_lo + skip_n)
+    auto trail = [&](int K, int la, int lo, int cnt, int skip_lo, int skip_n, cudaStream_t st) {
+        if (cnt <= 0) return;
+        if (W == 64) {
+            // -1: every column tile; t >= 0: only tile t; -2 - t: every tile but t
+            const int cols = skip_n > 0 ? -2 - skip_lo : (cnt == tiles ? -1 : lo);
+            gj3_trail_kernel<<<dim3(mtiles, cnt, count), U2T, TRAIL3_SMEM, st>>>(entries_dev, K, la, cols);
+        } else {
+            gj3_trail128_kernel<<<dim3(mtiles, cnt, count), U2T, TRAIL128_SMEM, st>>>(entries_dev, K, la, lo,
+                                                                                    skip_lo, skip_n);
+        }
+        ++launches;
+    };
     if (!look_ahead || outer < 2) {
         for (int K = 0; K < outer; ++K) {
             SCATT_TRY(chain(K, stream, 0));
-            gj3_trail_kernel<<<dim3(mtiles, tiles, count), U2T, TRAIL3_SMEM, stream>>>(entries_dev, K, 0, -1);
-            ++launches;
+            trail(K, 0, 0, tiles, 0, 0, stream);
         }
     } else {
         std::lock_guard<std::mutex> lock(g_la_mutex);
@@ -1778,27 +1974,49 @@ int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax, bool sy
         SCATT_TRY(chain(0, stream, 1));
         for (int K = 0; K < outer; ++K) {
             if (K + 1 < outer) {
-                // the next window's columns first, then its chain beside the rest of the update
-                gj3_trail_kernel<<<dim3(mtiles, 1, count), U2T, TRAIL3_SMEM, stream>>>(entries_dev, K, 1, K + 1);
+                // the next window's column tiles first, then its chain beside the rest of the update
+                const int nlo = (K + 1) * WT, ncnt = std::min(WT, tiles - nlo);
+                trail(K, 1, nlo, ncnt, 0, 0, stream);
                 SCATT_CUDA_TRY(cudaEventRecord(la->ev_main, stream));
                 SCATT_CUDA_TRY(cudaStreamWaitEvent(la->side, la->ev_main, 0));
                 SCATT_TRY(chain(K + 1, la->side, 1));
                 SCATT_CUDA_TRY(cudaEventRecord(la->ev_side, la->side));
-                gj3_trail_kernel<<<dim3(mtiles, tiles - 1, count), U2T, TRAIL3_SMEM, stream>>>(
-                    entries_dev, K, 1, -2 - (K + 1));
+                trail(K, 1, 0, tiles - ncnt, nlo, ncnt, stream);
                 SCATT_CUDA_TRY(cudaStreamWaitEvent(stream, la->ev_side, 0));
-                launches += 2;
             } else {
-                gj3_trail_kernel<<<dim3(mtiles, tiles, count), U2T, TRAIL3_SMEM, stream>>>(entries_dev, K, 1, -1);
-                ++launches;
+                trail(K, 1, 0, tiles, 0, 0, stream);
             }
         }
     }
     const int ft = (nmax + FT - 1) / FT;
-    gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, 1, symmetrize ? 1 : 0, 1);
+    gj_finalize_kernel<<<dim3(ft, ft, count), FT * 8, 0, stream>>>(entries_dev, W, symmetrize ? 1 : 0, 1);
     SCATT_CUDA_TRY(cudaGetLastError());
     SCATT_COUNT_LAUNCH(launches + 1);
     return SCATT_OK;
+}
+
+}  // namespace
+
+int gj_inverse_batched3(const GjEntry* entries_dev, int count, int nmax, bool symmetrize,
+                        cudaStream_t stream, bool look_ahead, int force_pcfg, int window) {
+    if (count <= 0 || nmax <= 0) return SCATT_OK;
+    if (window != 64 && window != 128) {
+        set_last_error("inverse: window width must be 64 or 128, got " + std::to_string(window));
+        return SCATT_ERR_ARG;
+    }
+    SCATT_TRY(once_per_device(2, [&]() -> int {
+        SCATT_CUDA_TRY(cudaFuncSetAttribute(gj3_narrow_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)NARROW3_SMEM));
+        SCATT_CUDA_TRY(cudaFuncSetAttribute(gj3_narrow_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)NARROW3_SMEM));
+        SCATT_CUDA_TRY(cudaFuncSetAttribute(gj3_trail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)TRAIL3_SMEM));
+        SCATT_CUDA_TRY(cudaFuncSetAttribute(gj3_trail128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)TRAIL128_SMEM));
+        return SCATT_OK;
+    }));
+    return window == 128 ? batched3_window<128>(entries_dev, count, nmax, symmetrize, stream, look_ahead, force_pcfg)
+                         : batched3_window<64>(entries_dev, count, nmax, symmetrize, stream, look_ahead, force_pcfg);
 }
 
 }  // namespace scatt

@@ -153,7 +153,7 @@ int scatt_inverse_batched_noalloc(int n, int count, const double* A, double* out
     SCATT_CUDA_TRY(cudaGetLastError());
     SCATT_COUNT_LAUNCH(1);
     const GjEntry* ent = reinterpret_cast<const GjEntry*>(base + c.ent);
-    SCATT_TRY(gj_inverse_selected(ent, count, n, symmetrize != 0, s, false));
+    SCATT_TRY(gj_inverse_selected(ent, count, n, symmetrize != 0, s, false, 64));
     SCATT_CUDA_TRY(cudaMemcpyAsync(out, base + c.O, nbytes, cudaMemcpyDeviceToHost, s));
     int st[2 * NOALLOC_MAX_COUNT];
     SCATT_CUDA_TRY(cudaMemcpyAsync(st, base + c.st, (size_t)2 * count * sizeof(int), cudaMemcpyDeviceToHost, s));

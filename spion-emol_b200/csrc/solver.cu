@@ -250,7 +250,7 @@ __global__ void k_prepare_schur(BatchDev b) {
                       : none;
     b.gjS[idx] = GjEntry{S, d.Sw + j * np2, sinv_at(b, d, n, j), d.sigS + (size_t)j * Np,
                          d.ridS + (size_t)j * Np, d.stS + 4 * j, Np, Np, Np,
-                         d.PS + (size_t)j * 4 * 64 * Np, d.sgS + (size_t)j * 4 * Np};
+                         d.PS + (size_t)j * 4 * GJ_WINDOW_MAX * Np, d.sgS + (size_t)j * 4 * Np};
 }
 
 // Fills the per-step GEMM / GJ entry arrays of chunk position j (pointer
@@ -1024,13 +1024,33 @@ struct Launcher {
         SCATT_TRY(gemm_batched(ge.p, (int)v.size(), mM, mN, opA, opB, s));
         return SCATT_CUDA_TRY_RET(cudaStreamSynchronize(s));
     }
+    DevBuf<double> gp;   // panel windows for orders above the single-level limit
+    DevBuf<int> gs;
     int gj(const std::vector<GjEntry>& v, bool sym) {
         if (v.empty()) return SCATT_OK;
         int mn = 0;
         for (auto& e : v) mn = std::max(mn, e.n);
         if (je.n < v.size()) SCATT_TRY(je.alloc(v.size()));
-        SCATT_CUDA_TRY(cudaMemcpyAsync(je.p, v.data(), v.size() * sizeof(GjEntry), cudaMemcpyHostToDevice, s));
-        SCATT_TRY(gj_inverse_batched(je.p, (int)v.size(), mn, sym, s));
+        if (mn <= 1280) {
+            SCATT_CUDA_TRY(cudaMemcpyAsync(je.p, v.data(), v.size() * sizeof(GjEntry), cudaMemcpyHostToDevice, s));
+            SCATT_TRY(gj_inverse_batched(je.p, (int)v.size(), mn, sym, s));
+            return SCATT_CUDA_TRY_RET(cudaStreamSynchronize(s));
+        }
+        // the row-contiguous two-level inverse (cluster panels), 64-column windows, no look-ahead
+        size_t pd = 0, si = 0;
+        for (auto& e : v) { pd += 2 * (size_t)e.ld * 64; si += 2 * (size_t)e.n; }
+        if (gp.n < pd) SCATT_TRY(gp.alloc(pd));
+        if (gs.n < si) SCATT_TRY(gs.alloc(si));
+        std::vector<GjEntry> w(v);
+        pd = si = 0;
+        for (auto& e : w) {
+            e.P = gp.p + pd;
+            e.sigt = gs.p + si;
+            pd += 2 * (size_t)e.ld * 64;
+            si += 2 * (size_t)e.n;
+        }
+        SCATT_CUDA_TRY(cudaMemcpyAsync(je.p, w.data(), w.size() * sizeof(GjEntry), cudaMemcpyHostToDevice, s));
+        SCATT_TRY(gj_inverse_batched3(je.p, (int)w.size(), mn, sym, s, false, -1, 64));
         return SCATT_CUDA_TRY_RET(cudaStreamSynchronize(s));
     }
     int copy(const std::vector<CopyEntry>& v) {
@@ -1358,8 +1378,8 @@ size_t slot_doubles(const BatchDev& b, int Np, int Nt, int l_cont, bool keep_win
     auto al = [](size_t c) { return (c + 31) & ~size_t(31); };
     const size_t np2 = (size_t)Np * Np, nt2 = (size_t)Nt * Nt;
     const size_t base = 3 * al(SCHUR_CHUNK * np2) + al((size_t)Np * b.Nf) + al((size_t)b.Nf * b.Nf) +
-                        4 * al(nt2) + 2 * al((size_t)b.Krows * Nt) + al((size_t)SCHUR_CHUNK * 4 * 64 * Np) +
-                        al((size_t)4 * 64 * Nt);
+                        4 * al(nt2) + 2 * al((size_t)b.Krows * Nt) + al((size_t)SCHUR_CHUNK * 4 * GJ_WINDOW_MAX * Np) +
+                        al((size_t)4 * GJ_WINDOW_MAX * Nt);
     if (keep_window) return base + al((size_t)nslots * nt2) + 2 * al((size_t)nslots * np2);
     return base + 2 * al((size_t)2 * Np * Nt) + al((size_t)b.nfit * 2 * Np) + al((size_t)8 * (l_cont + 1));
 }
@@ -1547,8 +1567,8 @@ int scan_open(Context& ctx, const scatt_solve_opts& o, int slots, int ngroups, i
             d.wAB = take((size_t)b.nfit * 2 * sc.Np_cap);
             d.Mab = take((size_t)8 * (l_cap + 1));
         }
-        d.PS = take((size_t)SCHUR_CHUNK * 4 * 64 * sc.Np_cap);
-        d.PR = take((size_t)4 * 64 * sc.Nt_cap);
+        d.PS = take((size_t)SCHUR_CHUNK * 4 * GJ_WINDOW_MAX * sc.Np_cap);
+        d.PR = take((size_t)4 * GJ_WINDOW_MAX * sc.Nt_cap);
         int* q = sc.iarena.p + slot_ints(sc.Np_cap, sc.Nt_cap) * e;
         const int Np = sc.Np_cap, Nt = sc.Nt_cap;
         d.sigS = q; q += SCHUR_CHUNK * Np;

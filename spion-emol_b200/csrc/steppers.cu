@@ -48,7 +48,7 @@ struct Inverter {
         const size_t nn = (size_t)n * n;
         SCATT_TRY(A.alloc(nn));
         SCATT_TRY(W.alloc(nn));
-        SCATT_TRY(P.alloc((size_t)4 * n * 64));
+        SCATT_TRY(P.alloc((size_t)4 * n * GJ_WINDOW_MAX));
         SCATT_TRY(sig.alloc(n));
         SCATT_TRY(rid.alloc(n));
         SCATT_TRY(st.alloc(2));

@@ -134,15 +134,15 @@ def autotune_inverse(n: int, count: int, reps: int = 3, device: int | None = Non
     if device is not None:
         import torch
         torch.cuda.set_device(device)
-    sc, pc, la = C.c_int(0), C.c_int(0), C.c_int(0)
+    sc, pc, la, win = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
     ms = C.c_double(0.0)
     check(lib().scatt_autotune_inverse(int(n), int(count), int(reps), C.byref(sc), C.byref(pc), C.byref(la),
-                                       C.byref(ms)))
+                                       C.byref(win), C.byref(ms)))
     return {"n": int(n), "count": int(count), "scheme": sc.value, "panel": pc.value,
-            "look_ahead": la.value, "ms": ms.value}
+            "look_ahead": la.value, "window": win.value, "ms": ms.value}
 
 
 def set_inverse_blocking(scheme: int):
     """0: automatic (default); 1: single-level; 2: two-level column-major;
-    3: two-level row-contiguous."""
+    3: two-level row-contiguous; 4: as 3 with 128-column windows."""
     check(lib().scatt_set_inverse_blocking(int(scheme)))

@@ -1,6 +1,6 @@
 """Device timing of the batched FP64 inverse (the per-step R^-1 / Sinv kernels).
 
-    python -m scatt_b200.inverse_bench --n 1046 --count 32 [--reps 5] [--scheme 0|1|2|3]
+    python -m scatt_b200.inverse_bench --n 1046 --count 32 [--reps 5] [--scheme 0|1|2|3|4]
 
 Seeded well-conditioned matrices are generated on the device; CUDA events
 bracket the inverse kernels only (scatt_bench_inverse).  Prints one JSON line
@@ -22,7 +22,7 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--scheme", type=int, default=0,
                     help="0 automatic (default), 1 single-level, 2 two-level column-major, "
-                         "3 two-level row-contiguous")
+                         "3 two-level row-contiguous, 4 as 3 with 128-column windows")
     a = ap.parse_args(argv)
     _lib.set_inverse_blocking(a.scheme)
     for n in a.n:

@@ -60,11 +60,12 @@ def test_dgemm_matches_numpy(opA, opB, M, N, K):
     assert np.max(np.abs(out - ref)) <= 1e-13 * max(1.0, np.max(np.abs(ref))) * np.sqrt(K + 1)
 
 
-@pytest.mark.parametrize("scheme", [1, 2, 3])
+@pytest.mark.parametrize("scheme", [1, 2, 3, 4])
 @pytest.mark.parametrize("n", [77, 441, 600, 1046])
 def test_inverse_every_scheme(scheme, n):
     """Single-level, column-major two-level and row-contiguous two-level
-    inverses against numpy; odd orders take the 8-byte copy paths."""
+    inverses (64- and 128-column windows) against numpy; odd orders take the
+    8-byte copy paths."""
     rng = np.random.default_rng(1000 + n)
     A = rng.standard_normal((2, n, n)) + 4.0 * np.sqrt(n) * np.eye(n)
     try:
@@ -84,6 +85,7 @@ def test_autotuned_inverse_is_kept_and_exact(n, count):
     of exactly that order and batch then run it and still equal numpy's."""
     t = _lib.autotune_inverse(n, count, reps=1)
     assert t["scheme"] in (2, 3) and 0 <= t["panel"] <= 4 and t["look_ahead"] in (0, 1) and t["ms"] > 0
+    assert t["window"] == 64 or (t["scheme"] == 3 and t["window"] == 128)
     assert n <= (256, 512, 768, 1152, 1280)[t["panel"]]
     rng = np.random.default_rng(n + count)
     M = rng.standard_normal((count, n, n))
@@ -95,14 +97,23 @@ def test_autotuned_inverse_is_kept_and_exact(n, count):
         assert np.max(np.abs(got[b] - ref)) / np.max(np.abs(ref)) < 1e-12
 
 
-@pytest.mark.parametrize("n", [1281, 2048, 5306])
-def test_inverse_cluster_panel_orders(n):
+@pytest.mark.parametrize("n,scheme", [(1281, 0), (1281, 4), (2048, 0), (2048, 4), (5306, 0), (5306, 4)])
+def test_inverse_cluster_panel_orders(n, scheme):
     """Orders above one CTA's panel run the cluster panel (CTAs of one
     thread-block cluster share the pivot search through distributed shared
-    memory); a symmetric and a general batch against numpy."""
+    memory), with 64- (scheme 0 picks scheme 3) and 128-column windows; a
+    symmetric and a general batch against numpy."""
     rng = np.random.default_rng(5000 + n)
     M = rng.standard_normal((2, n, n))
     A = M + np.transpose(M, (0, 2, 1)) + 4.0 * np.sqrt(n) * np.eye(n)
+    try:
+        _lib.set_inverse_blocking(scheme)
+        _cluster_checks(rng, n, A)
+    finally:
+        _lib.set_inverse_blocking(0)
+
+
+def _cluster_checks(rng, n, A):
     got, st = _lib.inverse_batched(A, symmetrize=True)
     assert np.all(st == 0)
     assert np.array_equal(got[0], got[0].T)

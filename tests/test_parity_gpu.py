@@ -160,3 +160,23 @@ def test_order_above_one_cta_panel():
     r, r2 = oracle_pair(st, E)
     fails = compare(g, r, r2, "N_t 1331")
     assert not fails, "\n".join(fails)
+
+
+def test_inverse_window_widths_agree_in_the_solver():
+    """The R-ratio and Schur inverses with 64- and 128-column outer windows
+    (schemes 3 and 4) give the same scan to rounding."""
+    from scatt_b200 import _lib
+    inp = synth.h2o_like(Nr=301, dr=0.05, l_cont=11, lmax_orb=8, n_orb=2)
+    sol = S.ScanSolver(inp)
+    Es = [0.3, 1.1]
+    out = {}
+    try:
+        for scheme in (3, 4):
+            _lib.set_inverse_blocking(scheme)
+            out[scheme] = sol.solve(Es, opts=S.default_opts(allow_closed_channels=1))
+    finally:
+        _lib.set_inverse_blocking(0)
+    for a, b in zip(out[3], out[4]):
+        assert a.status == 0 and b.status == 0
+        assert rel(b.K_kme, a.K_kme) < 1e-9
+        assert rel(b.D, a.D) < 1e-9
