@@ -164,7 +164,12 @@ def test_order_above_one_cta_panel():
 
 def test_inverse_window_widths_agree_in_the_solver():
     """The R-ratio and Schur inverses with 64- and 128-column outer windows
-    (schemes 3 and 4) give the same scan to rounding."""
+    (schemes 3 and 4) give the same scan to rounding.  The two inverses
+    round differently, and this case amplifies rounding: noise of
+    1e-16 x max|Rinv(n)| on every entry of every Rinv(n) moves the oracle's K
+    by 1e-8 and its dipoles by 1e-9 (tests/test_oracle_conditioning.py), and
+    the two windows' results differ by 2e-8 in D.  The bounds are 1e-8 (K)
+    and 1e-7 (D), against O(1) for a wrong inverse."""
     from scatt_b200 import _lib
     inp = synth.h2o_like(Nr=301, dr=0.05, l_cont=11, lmax_orb=8, n_orb=2)
     sol = S.ScanSolver(inp)
@@ -178,5 +183,5 @@ def test_inverse_window_widths_agree_in_the_solver():
         _lib.set_inverse_blocking(0)
     for a, b in zip(out[3], out[4]):
         assert a.status == 0 and b.status == 0
-        assert rel(b.K_kme, a.K_kme) < 1e-9
-        assert rel(b.D, a.D) < 1e-9
+        assert rel(b.K_kme, a.K_kme) < 1e-8
+        assert rel(b.D, a.D) < 1e-7
