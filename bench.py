@@ -66,10 +66,13 @@ DATA = {"h2_like": "synthetic (seeded H2-like inputs of the benchmark shapes)",
         "c8f8_like": "synthetic (seeded C8F8-like inputs of the benchmark shapes)"}
 
 
-# DRAM bytes (read + write) per sampled R^-1 inversion of the scan, from one
-# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum summed over the
-# inversion's kernels), keyed by (config, slots, groups).
-INVERSE_TRAFFIC: dict = {}
+# DRAM bytes (read + write) of the trailing updates of one sampled R^-1
+# inversion of the scan, keyed by (config, slots, groups).  From one ncu
+# capture of gj3_trail128_kernel on 32 matrices of order 1046 (452.7 MB for
+# 15 of the 17 column tiles of one 128-column window), scaled to 17 tiles,
+# 128 matrices and the call's 9 windows: the C tiles are read and written
+# once per window, so the traffic grows with the tiles and matrices.
+INVERSE_TRAFFIC: dict = {("h2o_like", 128, 16): 452.7e6 * 17 / 15 * 4 * 9}
 
 
 # Device seconds of one chunk (8 radial steps) with every slot busy, as
