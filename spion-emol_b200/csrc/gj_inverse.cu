@@ -1574,13 +1574,12 @@ gj3_trail128_kernel(const GjEntry* __restrict__ entries, int K, int la, int ct_l
         }
         cp_async_commit();
     };
-    issue(0);
-    if (nch > 1) issue(1);
     const int lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
     const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
     double acc[2][4][4];
-    // C tile straight from the old matrix into the accumulators
+    // C tile straight from the old matrix into the accumulators: issued
+    // first, its HBM latency is the longest; the first two k stages follow
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -1606,6 +1605,8 @@ gj3_trail128_kernel(const GjEntry* __restrict__ entries, int K, int la, int ct_l
                 acc[i][jn][2 * h + 1] = x1;
             }
         }
+    issue(0);
+    if (nch > 1) issue(1);
 #pragma unroll 1
     for (int ch = 0; ch < nch; ++ch) {
         if (ch + 1 < nch) cp_async_wait<1>();
