@@ -105,7 +105,9 @@ int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call);
  * 3 = two-level on the row-contiguous view of the buffer (pivots by columns
  *     of A, which for a symmetric A is the row-pivoting sequence),
  * 4 = scheme 3 with 128-column outer windows (rank-128 trailing updates;
- *     the allocation-free entry point keeps 64-column windows).
+ *     the allocation-free entry point keeps 64-column windows),
+ * 5, 6 = schemes 3 and 4 with the small cluster panel (clusters of
+ *     384-row CTAs, small enough to share an SM with the trailing update).
  * All give the same inverse up to rounding.  The setting is process-wide and
  * applies from the next inverse on, also in solves running on other threads. */
 int scatt_set_inverse_blocking(int scheme);
@@ -119,7 +121,8 @@ int scatt_set_inverse_blocking(int scheme);
  * and batch on that device -- the solver's Schur and R^-1 batches included
  * -- uses the kept choice.  Outputs (each may be NULL): the scheme (2 or 3),
  * the panel shape (0..4: 1x8, 2x8, 3x8, 3x12, 5x8 rows per thread x warps;
- * 5: the cluster panel of orders above 1280), look-ahead (0/1), the window
+ * 5: the cluster panel of orders above 1280; 6: the small cluster panel,
+ * row-contiguous scheme, orders up to 3072), look-ahead (0/1), the window
  * width (64 or 128) and the chosen configuration's milliseconds per call.
  * Orders 1..8192 (above 1280 only scheme 3 runs).  No counterpart in the
  * reference. */

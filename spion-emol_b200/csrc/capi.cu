@@ -227,8 +227,8 @@ int scatt_dgemm(int opA, int opB, int M, int N, int K, double alpha, const doubl
 
 
 int scatt_set_inverse_blocking(int scheme) {
-    if (scheme < 0 || scheme > 4) {
-        set_last_error("scatt_set_inverse_blocking: scheme must be 0, 1, 2, 3 or 4");
+    if (scheme < 0 || scheme > 6) {
+        set_last_error("scatt_set_inverse_blocking: scheme must be in 0..6");
         return SCATT_ERR_ARG;
     }
     g_inverse_scheme.store(scheme, std::memory_order_relaxed);
@@ -259,8 +259,12 @@ int scatt_autotune_inverse(int n, int count, int reps, int* scheme, int* panel, 
     // above one CTA's panel (1280 rows) only the row-contiguous scheme with the cluster panel runs
     const bool cluster = n > gj_panel_capacity(GJ_PANEL_SHAPES - 1);
     for (int sch = cluster ? 3 : 2; sch <= 3; ++sch)
-        for (int p = 0; p <= GJ_PANEL_SHAPES; ++p) {
-            if (cluster ? p != GJ_PANEL_SHAPES : (p == GJ_PANEL_SHAPES || n > gj_panel_capacity(p))) continue;
+        for (int p = 0; p <= GJ_PANEL_SMALL_CLUSTER; ++p) {
+            if (p == GJ_PANEL_SMALL_CLUSTER) {
+                if (sch != 3 || n > 3072) continue;       // the small cluster panel: row-contiguous only
+            } else if (cluster ? p != GJ_PANEL_SHAPES : (p == GJ_PANEL_SHAPES || n > gj_panel_capacity(p))) {
+                continue;
+            }
             for (int la = 0; la <= (sch == 3 ? 1 : 0); ++la)
                 for (int w = 64; w <= (sch == 3 ? GJ_WINDOW_MAX : 64); w *= 2) {
                     double ms = 0.0;

@@ -131,6 +131,11 @@ constexpr int GJ_WINDOW_MAX = 128;
 // 2x8, 3x8, 3x12, 5x8.  Shape p factors panels of up to gj_panel_capacity(p)
 // rows; the default is the smallest shape that holds the order.
 constexpr int GJ_PANEL_SHAPES = 5;
+// Two more panel configurations of the row-contiguous scheme: GJ_PANEL_SHAPES
+// itself (a cluster of 1024-row CTAs, orders above 1280) and the small
+// cluster panel (384-row CTAs that fit beside the trailing update, any order
+// up to 3072).
+constexpr int GJ_PANEL_SMALL_CLUSTER = GJ_PANEL_SHAPES + 1;
 inline int gj_panel_capacity(int pcfg) {
     constexpr int cap[GJ_PANEL_SHAPES] = {256, 512, 768, 1152, 1280};
     return cap[pcfg];
@@ -151,7 +156,8 @@ void inverse_tune_store(int device, int n, int count, const InverseTune& t);
 // (row-contiguous two-level above order 512, where its contiguous pivot-row
 // tiles pay; column-major two-level below), 1 = single-level,
 // 2 = column-major two-level, 3 = row-contiguous two-level, 4 = scheme 3
-// with 128-column windows (where the entries' buffers hold them).  Process-wide;
+// with 128-column windows (where the entries' buffers hold them), 5 / 6 =
+// schemes 3 / 4 with the small cluster panel.  Process-wide;
 // atomic because it may be set while another thread solves (a call reads it
 // once per inverse, so a change applies from the next inverse on).
 extern std::atomic<int> g_inverse_scheme;
@@ -168,6 +174,10 @@ inline int gj_inverse_selected(const GjEntry* entries_dev, int count, int nmax,
         case 3: return gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream, look_ahead);
         case 4: return gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream, look_ahead, -1,
                                            wcap >= 128 ? 128 : 64);
+        case 5: return gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream, look_ahead,
+                                           GJ_PANEL_SMALL_CLUSTER, 64);
+        case 6: return gj_inverse_batched3(entries_dev, count, nmax, symmetrize, stream, look_ahead,
+                                           GJ_PANEL_SMALL_CLUSTER, wcap >= 128 ? 128 : 64);
         default: {
             InverseTune t;
             if (inverse_tune_lookup(nmax, count, &t)) {

@@ -773,9 +773,15 @@ gj2_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub, int la) {
 constexpr int GJ4_R = 4, GJ4_NW = 8;
 constexpr int GJ4_ROWS = GJ4_R * GJ4_NW * 32;        // rows per CTA
 constexpr int GJ4_CL_MAX = 8;                       // portable cluster size
+// The small cluster panel (any order up to 8 x 384): 2 rows per thread, 6
+// warps, at most 170 registers, so that a CTA fits on an SM beside one CTA of
+// the trailing update (122 registers x 256 threads) and the panel chain can
+// run while the trailing update holds the GPU.
+constexpr int GJ4S_R = 2, GJ4S_NW = 6;
+constexpr int GJ4S_ROWS = GJ4S_R * GJ4S_NW * 32;
 
-template <int R, int NW, int W>
-__global__ void __launch_bounds__(NW * 32, 1)
+template <int R, int NW, int W, int MINB = 1>
+__global__ void __launch_bounds__(NW * 32, MINB)
 gj4_panel_kernel(const GjEntry* __restrict__ entries, int K, int sub, int la) {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
@@ -1705,18 +1711,23 @@ gj_finalize_kernel(const GjEntry* __restrict__ entries, int wstep, int symmetriz
 }
 
 // Cluster shape of the panel for orders above one CTA: CTAs per matrix.
-int gj4_cluster_size(int nmax) { return (nmax + GJ4_ROWS - 1) / GJ4_ROWS; }
+int gj4_cluster_size(int nmax, int pcfg) {
+    const int rows = pcfg == GJ_PANEL_SMALL_CLUSTER ? GJ4S_ROWS : GJ4_ROWS;
+    return (nmax + rows - 1) / rows;
+}
 
-// pcfg GJ_PANEL_SHAPES: the cluster panel (RM only), gj4_cluster_size(nmax) CTAs per matrix;
+// pcfg GJ_PANEL_SHAPES: the cluster panel (RM only), gj4_cluster_size CTAs per matrix;
+// pcfg GJ_PANEL_SMALL_CLUSTER: the small cluster panel (RM only);
 // W: window width (64 for the column-major scheme)
 template <bool RM, int W>
 int launch_panel(int pcfg, int count, int pt, size_t smem, cudaStream_t stream, const GjEntry* ent, int K, int sub,
                  int la, int nmax = 0) {
-    if (RM && pcfg == GJ_PANEL_SHAPES) {
-        const int cl = gj4_cluster_size(nmax);
+    if (RM && (pcfg == GJ_PANEL_SHAPES || pcfg == GJ_PANEL_SMALL_CLUSTER)) {
+        const bool small = pcfg == GJ_PANEL_SMALL_CLUSTER;
+        const int cl = gj4_cluster_size(nmax, pcfg);
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)(count * cl), 1, 1);
-        cfg.blockDim = dim3(GJ4_NW * 32, 1, 1);
+        cfg.blockDim = dim3((small ? GJ4S_NW : GJ4_NW) * 32, 1, 1);
         cfg.dynamicSmemBytes = 0;
         cfg.stream = stream;
         cudaLaunchAttribute attr[1];
@@ -1726,7 +1737,10 @@ int launch_panel(int pcfg, int count, int pt, size_t smem, cudaStream_t stream, 
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        SCATT_CUDA_TRY(cudaLaunchKernelEx(&cfg, gj4_panel_kernel<GJ4_R, GJ4_NW, W>, ent, K, sub, la));
+        if (small)
+            SCATT_CUDA_TRY(cudaLaunchKernelEx(&cfg, gj4_panel_kernel<GJ4S_R, GJ4S_NW, W, 2>, ent, K, sub, la));
+        else
+            SCATT_CUDA_TRY(cudaLaunchKernelEx(&cfg, gj4_panel_kernel<GJ4_R, GJ4_NW, W>, ent, K, sub, la));
         return SCATT_OK;
     }
     switch (pcfg) {
@@ -1772,6 +1786,15 @@ int look_ahead_resources(cudaStream_t main, LookAhead** out) {
 // that holds nmax.  pt = the threads of the launch: ceil(nmax / rows) rounded
 // up to whole warps, at most the shape's warps since nmax <= its capacity.
 int panel_shape(int nmax, int& pcfg, int& pt, int force = -1) {
+    if (force == GJ_PANEL_SMALL_CLUSTER) {
+        if (nmax > GJ4S_ROWS * GJ4_CL_MAX) {
+            set_last_error("inverse: the small cluster panel does not hold order " + std::to_string(nmax));
+            return SCATT_ERR_ARG;
+        }
+        pcfg = force;
+        pt = GJ4S_NW * 32;
+        return SCATT_OK;
+    }
     if (nmax > gj_panel_capacity(GJ_PANEL_SHAPES - 1)) {
         // beyond one CTA: the cluster panel
         if (force >= 0 && force != GJ_PANEL_SHAPES) {
@@ -1901,6 +1924,10 @@ int gj_inverse_batched2(const GjEntry* entries_dev, int count, int nmax, bool sy
                         cudaStream_t stream, int force_pcfg) {
     if (count <= 0 || nmax <= 0) return SCATT_OK;
     if (nmax > 1280) return gj_inverse_batched(entries_dev, count, nmax, symmetrize, stream);
+    if (force_pcfg >= GJ_PANEL_SHAPES) {
+        set_last_error("inverse: the cluster panels run on the row-contiguous scheme only");
+        return SCATT_ERR_ARG;
+    }
     SCATT_TRY(once_per_device(1, [&]() -> int {
         SCATT_CUDA_TRY(cudaFuncSetAttribute(gj2_narrow_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)U2_SMEM));

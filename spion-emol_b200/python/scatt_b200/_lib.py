@@ -144,5 +144,6 @@ def autotune_inverse(n: int, count: int, reps: int = 3, device: int | None = Non
 
 def set_inverse_blocking(scheme: int):
     """0: automatic (default); 1: single-level; 2: two-level column-major;
-    3: two-level row-contiguous; 4: as 3 with 128-column windows."""
+    3: two-level row-contiguous; 4: as 3 with 128-column windows; 5, 6: as 3, 4
+    with the small cluster panel."""
     check(lib().scatt_set_inverse_blocking(int(scheme)))

@@ -61,12 +61,12 @@ def test_dgemm_matches_numpy(opA, opB, M, N, K):
     assert np.max(np.abs(out - ref)) <= 1e-13 * max(1.0, np.max(np.abs(ref))) * np.sqrt(K + 1)
 
 
-@pytest.mark.parametrize("scheme", [1, 2, 3, 4])
+@pytest.mark.parametrize("scheme", [1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("n", [77, 441, 600, 1046])
 def test_inverse_every_scheme(scheme, n):
     """Single-level, column-major two-level and row-contiguous two-level
-    inverses (64- and 128-column windows) against numpy; odd orders take the
-    8-byte copy paths."""
+    inverses (64- and 128-column windows, single-CTA and small cluster
+    panels) against numpy; odd orders take the 8-byte copy paths."""
     rng = np.random.default_rng(1000 + n)
     A = rng.standard_normal((2, n, n)) + 4.0 * np.sqrt(n) * np.eye(n)
     try:
@@ -85,9 +85,9 @@ def test_autotuned_inverse_is_kept_and_exact(n, count):
     """The autotuner keeps a valid configuration for (order, batch); inverses
     of exactly that order and batch then run it and still equal numpy's."""
     t = _lib.autotune_inverse(n, count, reps=1)
-    assert t["scheme"] in (2, 3) and 0 <= t["panel"] <= 4 and t["look_ahead"] in (0, 1) and t["ms"] > 0
+    assert t["scheme"] in (2, 3) and 0 <= t["panel"] <= 6 and t["look_ahead"] in (0, 1) and t["ms"] > 0
     assert t["window"] == 64 or (t["scheme"] == 3 and t["window"] == 128)
-    assert n <= (256, 512, 768, 1152, 1280)[t["panel"]]
+    assert t["panel"] == 6 or n <= (256, 512, 768, 1152, 1280)[t["panel"]]
     rng = np.random.default_rng(n + count)
     M = rng.standard_normal((count, n, n))
     A = M + np.transpose(M, (0, 2, 1)) + 2.0 * np.sqrt(n) * np.eye(n)
