@@ -164,7 +164,8 @@ def test_order_above_one_cta_panel():
 
 def test_inverse_window_widths_agree_in_the_solver():
     """The R-ratio and Schur inverses with 64- and 128-column outer windows
-    (schemes 3 and 4) give the same scan to rounding.  The two inverses
+    and with single-CTA or small cluster panels (schemes 3 to 6) give the
+    same scan to rounding.  The two inverses
     round differently, and this case amplifies rounding: noise of
     1e-16 x max|Rinv(n)| on every entry of every Rinv(n) moves the oracle's K
     by 1e-8 and its dipoles by 1e-9 (tests/test_oracle_conditioning.py), and
@@ -176,12 +177,13 @@ def test_inverse_window_widths_agree_in_the_solver():
     Es = [0.3, 1.1]
     out = {}
     try:
-        for scheme in (3, 4):
+        for scheme in (3, 4, 5, 6):
             _lib.set_inverse_blocking(scheme)
             out[scheme] = sol.solve(Es, opts=S.default_opts(allow_closed_channels=1))
     finally:
         _lib.set_inverse_blocking(0)
-    for a, b in zip(out[3], out[4]):
-        assert a.status == 0 and b.status == 0
-        assert rel(b.K_kme, a.K_kme) < 1e-8
-        assert rel(b.D, a.D) < 1e-7
+    for scheme in (4, 5, 6):
+        for a, b in zip(out[3], out[scheme]):
+            assert a.status == 0 and b.status == 0
+            assert rel(b.K_kme, a.K_kme) < 1e-8, scheme
+            assert rel(b.D, a.D) < 1e-7, scheme
