@@ -98,6 +98,13 @@ int scatt_dgemm(int opA, int opB, int M, int N, int K, double alpha,
  * matrices (CUDA events around the kernels only); used by the inverse
  * benchmark (python -m scatt_b200.inverse_bench). */
 int scatt_bench_inverse(int n, int count, int reps, double* ms_per_call);
+/* Device-resident timing of one batched GEMM call (count products
+ * C = op(A) op(B), M x N x K, seeded operands; sym != 0 computes the lower
+ * triangle and mirrors it, M == N) by CUDA events around the call, mean of
+ * reps calls after one untimed call; used by the GEMM benchmark
+ * (python -m scatt_b200.gemm_bench).  No counterpart in the reference. */
+int scatt_bench_gemm(int opA, int opB, int M, int N, int K, int count, int sym, int reps,
+                     double* ms_per_call);
 /* Blocking scheme of every dense inverse (the entry points and the solver):
  * 0 = automatic (default): scheme 3 above order 512, scheme 2 below,
  * 1 = single-level (rank-16 updates, row pivoting),

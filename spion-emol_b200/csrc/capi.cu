@@ -225,6 +225,52 @@ int scatt_dgemm(int opA, int opB, int M, int N, int K, double alpha, const doubl
     return SCATT_OK;
 }
 
+int scatt_bench_gemm(int opA, int opB, int M, int N, int K, int count, int sym, int reps, double* ms_per_call) {
+    if (M <= 0 || N <= 0 || K <= 0 || count <= 0 || reps <= 0 || !ms_per_call || (sym && M != N) ||
+        opA < 0 || opA > 1 || opB < 0 || opB > 1) {
+        set_last_error("scatt_bench_gemm: bad arguments");
+        return SCATT_ERR_ARG;
+    }
+    SCATT_TRY(require_device());
+    const size_t sa = (size_t)M * K, sb = (size_t)K * N, sc = (size_t)M * N;
+    DevBuf<double> dA, dB, dC;
+    SCATT_TRY(dA.alloc(sa * count));
+    SCATT_TRY(dB.alloc(sb * count));
+    SCATT_TRY(dC.alloc(sc * count));
+    fill_test_matrices<<<1024, 256>>>(dA.p, 1, (int)std::min<size_t>(sa * count, 1u << 30), 7u);
+    fill_test_matrices<<<1024, 256>>>(dB.p, 1, (int)std::min<size_t>(sb * count, 1u << 30), 11u);
+    SCATT_CUDA_TRY(cudaMemset(dC.p, 0, sc * count * sizeof(double)));
+    std::vector<GemmEntry> ent(count);
+    for (int b = 0; b < count; ++b)
+        ent[b] = GemmEntry{dA.p + sa * b, dB.p + sb * b, dC.p + sc * b, M, N, K,
+                           opA ? K : M, opB ? N : K, M, 1.0, 0.0, sym ? 1 : 0};
+    DevBuf<GemmEntry> de;
+    SCATT_TRY(de.upload(ent));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    SCATT_CUDA_TRY(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return cuda_status(cudaErrorMemoryAllocation, "cudaEventCreate");
+    }
+    double total = 0.0;
+    int st = SCATT_OK;
+    for (int r = 0; r < reps + 1 && st == SCATT_OK; ++r) {
+        cudaError_t ce = cudaEventRecord(e0, 0);
+        if (ce != cudaSuccess) { st = cuda_status(ce, "gemm timing"); break; }
+        st = gemm_batched(de.p, count, M, N, opA, opB, 0);
+        if (st != SCATT_OK) break;
+        ce = cudaEventRecord(e1, 0);
+        if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+        if (ce != cudaSuccess) { st = cuda_status(ce, "gemm timing"); break; }
+        if (r > 0) total += ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st == SCATT_OK) *ms_per_call = total / reps;
+    return st;
+}
 
 int scatt_set_inverse_blocking(int scheme) {
     if (scheme < 0 || scheme > 6) {

@@ -62,6 +62,7 @@ def lib():
     L.scatt_dgemm.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                               dptr, C.c_int, dptr, C.c_int, C.c_double, dptr, C.c_int]
     L.scatt_bench_inverse.argtypes = [C.c_int, C.c_int, C.c_int, dptr]
+    L.scatt_bench_gemm.argtypes = [C.c_int] * 8 + [dptr]
     L.scatt_set_inverse_blocking.argtypes = [C.c_int]
     _lib = L
     return L
@@ -124,6 +125,14 @@ def dgemm(A, B, C=None, alpha=1.0, beta=0.0, opA=0, opB=0):
 def bench_inverse(n: int, count: int, reps: int = 5) -> float:
     ms = C.c_double(0.0)
     check(lib().scatt_bench_inverse(n, count, reps, C.byref(ms)))
+    return ms.value
+
+
+def bench_gemm(opA: int, opB: int, M: int, N: int, K: int, count: int, sym: bool = False, reps: int = 5) -> float:
+    """Milliseconds of one batched GEMM call on device-resident operands (scatt_bench_gemm)."""
+    ms = C.c_double(0.0)
+    check(lib().scatt_bench_gemm(int(opA), int(opB), int(M), int(N), int(K), int(count), 1 if sym else 0,
+                                 int(reps), C.byref(ms)))
     return ms.value
 
 

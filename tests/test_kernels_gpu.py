@@ -50,7 +50,8 @@ def test_inverse_singular_reports_status():
 
 @pytest.mark.parametrize("opA,opB", [(0, 0), (1, 0), (0, 1), (1, 1)])
 @pytest.mark.parametrize("M,N,K", [(1, 1, 1), (7, 13, 5), (11, 1046, 1046), (16, 130, 77), (17, 70, 33), (64, 64, 16),
-                                   (65, 63, 17), (200, 130, 441), (441, 605, 441)])
+                                   (65, 63, 17), (128, 64, 32), (129, 65, 33), (256, 192, 96), (200, 130, 441),
+                                   (441, 605, 441)])
 def test_dgemm_matches_numpy(opA, opB, M, N, K):
     rng = np.random.default_rng(M * 1000 + N + K)
     A = rng.standard_normal((K, M) if opA else (M, K))
