@@ -80,3 +80,54 @@ def test_two_rank_sharding_and_max_reduction():
         assert p.exitcode == 0
     assert got == list(range(50))
     assert t == [2.0, 20.0]
+
+
+def _tau_worker(rank, world, port, sizes, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    k, D = _smooth_dipoles(sum(sizes))
+    lo = sum(sizes[:rank])
+    mine = slice(lo, lo + sizes[rank])
+    tau = shard.halo_time_delay(k[mine], D[mine])
+    q.put((rank, tau.tolist()))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def _smooth_dipoles(n):
+    """An uneven k grid and smooth complex dipoles of 5 channels on it."""
+    k = np.sort(np.random.default_rng(7).uniform(0.05, 2.0, n))
+    ch = np.arange(5)[None, :]
+    D = (1.0 + 0.3 * ch) * np.exp(1j * (0.8 * k[:, None] + 0.2 * ch * k[:, None] ** 2)) / (1.0 + k[:, None])
+    return k, D
+
+
+@pytest.mark.parametrize("sizes", [(13, 17), (9, 0, 11), (1, 1, 12)])
+def test_time_delay_with_k_halo_equals_whole_grid(sizes):
+    """Ranks holding contiguous blocks of the k grid (some of one energy, one
+    empty) get, with the one-point halo, the whole grid's delay at every
+    energy: the finite difference at a block edge uses the neighbour's edge
+    energy."""
+    from scatt_b200.observables import time_delay
+    world = len(sizes)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_tau_worker, args=(r, world, port, list(sizes), q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    parts = dict(q.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    got = np.concatenate([np.array(parts[r]) for r in range(world)])
+    k, D = _smooth_dipoles(sum(sizes))
+    ref = time_delay(k, D)
+    assert got.shape == ref.shape
+    assert np.max(np.abs(got - ref)) <= 1e-14 * np.max(np.abs(ref))
+    # without the halo the block edges differ (one-sided differences there)
+    own = np.concatenate([time_delay(k[a:a + s], D[a:a + s]) for a, s in
+                          zip(np.cumsum((0,) + sizes[:-1]), sizes) if s >= 2])
+    if sizes == (13, 17):
+        assert np.max(np.abs(own - ref)) > 1e-6 * np.max(np.abs(ref))
