@@ -371,6 +371,26 @@ int scatt_adjoint_view_of(scatt_adjoint* adj, int i, scatt_adjoint_view* view);
 int scatt_adjoint_reverse(scatt_adjoint* adj, double* vtr, double* vfull_device);
 int scatt_adjoint_close(scatt_adjoint* adj);
 
+/* ------------------------------------------------------ psi reconstruction
+ * BackPropagator::run + get_psi (src/scatt/BackPropagator.cpp:199-802):
+ * psi(n) = (W^-1(n) Z_n)_psi with Z_n = Rinv(n) Z_{n+1} from the outer
+ * boundary Z_N, over any range n_lo <= n < n_hi of the grid (the reference
+ * keeps [0, n_transition) and the 300-point asymptotic tail).  Solves
+ * n_energy energies as one lock-step batch (results into `outputs` as
+ * scatt_solve_batch, with the fit accumulated forward: keep_window and
+ * use_graphs of `opts` are ignored), keeping Rinv(a - 1) at every segment
+ * start a, then sweeps back from N - 1 to n_lo, recomputing each segment's
+ * Sinv and Rinv from its checkpoint.  psi(n) of energy i (submission order)
+ * lands at psi_out + (i * (n_hi - n_lo) + n - n_lo) * Np_max^2, column-major
+ * Np x Np with ld Np_max (zero outside an energy's own Np x Np block).
+ * psi_out is host memory; when it is page-locked the copies of one segment
+ * run while the next segment is recomputed.  segment: a positive multiple of
+ * 8 radial steps.  Device memory per energy, besides the scan state: about
+ * (Nr / segment + segment) N_t^2 + segment (Np^2 + 2 Np_max^2) doubles. */
+int scatt_psi_sweep(scatt_ctx* ctx, const scatt_solve_opts* opts, int n_energy, const double* energies,
+                    const int* l_cont, int segment, int n_lo, int n_hi, const scatt_outputs* outputs,
+                    double* psi_out);
+
 /* ------------------------------------------------------ file formats
  * Host-only entry points (no device work, no GPU needed) for the files
  * around the path, on an HDF5 subset written from the public file-format

@@ -3154,6 +3154,242 @@ int adj_reverse(Adjoint& A, double* vtr_host, double* vfull) {
     return SCATT_OK;
 }
 
+// ---------------------------------------------------------------- psi sweep
+// BackPropagator::run (BackPropagator.cpp:533-703) with get_psi (:760-802)
+// over any range [n_lo, n_hi) of the grid, for a lock-step batch of
+// energies.  The forward sweep keeps R^-1(a - 1) at every segment start a;
+// the post stages leave Z_N (the outer boundary, BackPropagator.cpp:127-197)
+// in the post buffers.  The sweep then walks back from N - 1: each
+// segment's Sinv(n) and R^-1(n) are recomputed from its checkpoint into the
+// segment stores, and Z_n = R^-1(n) Z_{n+1}, psi(n) = (W^-1(n) Z_n)_psi
+// (WInverseOperator.cpp:75-200: rhs = Z_psi - Bs(n) Z_f and psi = Sinv(n) rhs
+// inside the exchange region, Sinv(n) Z_psi past it) -- the arithmetic of
+// the post stages' window sweep.  A segment's psi goes to one of two device
+// staging slabs (Np_max^2 per point, zero outside the energy's block) and
+// from there to the caller's host buffer on a copy stream, so with
+// page-locked host memory the copies of one segment overlap the
+// recomputation of the next.
+namespace {
+
+struct StreamGuard {
+    cudaStream_t s = nullptr;
+    ~StreamGuard() { if (s) cudaStreamDestroy(s); }
+};
+struct EventGuard {
+    cudaEvent_t e = nullptr;
+    ~EventGuard() { if (e) cudaEventDestroy(e); }
+};
+
+}  // namespace
+
+int psi_sweep(Context& ctx, const scatt_solve_opts& o_in, int n, const double* E, const int* lc, int segment,
+              int n_lo, int n_hi, const scatt_outputs* out, double* psi_host) {
+    ScanTables& t = *ctx.tab;
+    cudaStream_t s = ctx.stream;
+    if (n < 1 || segment < SCHUR_CHUNK || segment % SCHUR_CHUNK || n_lo < 0 || n_hi > t.Nr || n_lo >= n_hi ||
+        !psi_host || !out) {
+        set_last_error("scatt_psi_sweep: need n_energy >= 1, a segment that is a positive multiple of " +
+                       std::to_string(SCHUR_CHUNK) + ", 0 <= n_lo < n_hi <= Nr and the output buffers");
+        return SCATT_ERR_ARG;
+    }
+    int l_cap = 0;
+    for (int e = 0; e < n; ++e) l_cap = std::max(l_cap, lc ? lc[e] : t.l_max);
+    scatt_solve_opts o = o_in;
+    o.use_graphs = 0;
+    o.keep_window = 0;                   // the fit accumulates forward: no window store
+    Scan sc;
+    SCATT_TRY(scan_open(ctx, o, n, 1, l_cap, sc));
+    BatchDev& b = sc.b;
+    const int K = b.Krows, Nf = b.Nf, N = b.N, Npm = b.Np_max;
+    const size_t npm2 = (size_t)Npm * Npm;
+    const int nseg = (N + segment - 1) / segment;          // segments [a, min(a + segment, N)), a < N
+    const size_t R = (size_t)(n_hi - n_lo);
+    for (int e = 0; e < n; ++e) sc.queue.push_back(Job{E[e], lc ? lc[e] : t.l_max, e});
+    sc.submitted = n;
+    SCATT_TRY(load_group(sc, 0));
+    std::vector<int> slot_of(n, -1);
+    for (int e = 0; e < n; ++e) slot_of[sc.job_of[e]] = e;
+    // ---- per slot: checkpoints, segment stores, the second Z buffer, rhs, staging
+    struct PsiSlot {
+        double *ck, *Z1, *rhs, *stg[2], *top;
+    };
+    std::vector<PsiSlot> ps(n);
+    auto al = [](size_t c) { return (c + 31) & ~size_t(31); };
+    const size_t seg = segment;
+    size_t total = 0;
+    for (int e = 0; e < n; ++e) {
+        const size_t Np = sc.ed[e].Np, Nt = sc.ed[e].Nt;
+        total += nseg * al(Nt * Nt) + al(seg * Nt * Nt) + al(seg * Np * Np) + al(seg * K * Nt) + al(Nt * Np) +
+                 al(Np * Np) + 2 * al(seg * npm2) + al(npm2);
+    }
+    DevBuf<double> arena;
+    SCATT_TRY(arena.alloc(total));
+    SCATT_CUDA_TRY(cudaMemsetAsync(arena.p, 0, total * sizeof(double), s));
+    double* p = arena.p;
+    auto take = [&p, &al](size_t c) { double* r = p; p += al(c); return r; };
+    for (int e = 0; e < n; ++e) {
+        EnergyDev& d = sc.ed[e];
+        const size_t Np = d.Np, Nt = d.Nt;
+        ps[e].ck = take(nseg * al(Nt * Nt));
+        d.segR = take(seg * Nt * Nt);
+        d.segS = take(seg * Np * Np);
+        d.segH = take(seg * K * Nt);
+        ps[e].Z1 = take(Nt * Np);
+        ps[e].rhs = take(Np * Np);
+        ps[e].stg[0] = take(seg * npm2);
+        ps[e].stg[1] = take(seg * npm2);
+        ps[e].top = take(npm2);
+        d.seg_lo = d.seg_hi = 0;
+    }
+    SCATT_CUDA_TRY(cudaMemcpyAsync(sc.d_ed.p, sc.ed.data(), n * sizeof(EnergyDev), cudaMemcpyHostToDevice, s));
+    // ---- the forward sweep, with R^-1(a - 1) kept at every segment start a (ping-pong buffer of a - 1:
+    // the window store is off)
+    while (sc.grp[0].n0 >= 0) {
+        const int next = sc.grp[0].n0 + sc.grp[0].C;
+        SCATT_TRY(run_chunk(sc, nullptr));
+        if (next % segment == 0 && next < N) {
+            const int si = next / segment;
+            for (int e = 0; e < n; ++e) {
+                const EnergyDev& d = sc.ed[e];
+                const size_t nt2 = (size_t)d.Nt * d.Nt;
+                SCATT_CUDA_TRY(cudaMemcpyAsync(ps[e].ck + si * al(nt2), ((next - 1) & 1) ? d.Rinv1 : d.Rinv0,
+                                               nt2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            }
+        }
+    }
+    // ---- post stages: K, the fit, the dipoles into `out`; Z_N stays in P[e].Z0, psi(N) in P[e].psibc
+    std::vector<int> sel(n);
+    std::vector<long> rows(n);
+    for (int e = 0; e < n; ++e) { sel[e] = e; rows[e] = sc.job_of[e]; }
+    int first = SCATT_OK;
+    std::string msg;
+    SCATT_TRY(post_slots(sc, sel, rows, out, &first, &msg));
+    sc.grp[0].n0 = -1;
+    StreamGuard cs;                       // device-to-host copies of the staging slabs
+    SCATT_CUDA_TRY(cudaStreamCreateWithFlags(&cs.s, cudaStreamNonBlocking));
+    EventGuard ev_done[2], ev_copied[2];
+    for (int i = 0; i < 2; ++i) {
+        SCATT_CUDA_TRY(cudaEventCreateWithFlags(&ev_done[i].e, cudaEventDisableTiming));
+        SCATT_CUDA_TRY(cudaEventCreateWithFlags(&ev_copied[i].e, cudaEventDisableTiming));
+    }
+    bool pending[2] = {false, false};
+    if (n_lo <= N && N < n_hi) {          // psi(N) = the boundary value
+        std::vector<CopyEntry> ct(n);
+        for (int e = 0; e < n; ++e) {
+            const int Np = sc.ed[e].Np;
+            ct[e] = CopyEntry{sc.P[e].psibc, ps[e].top, Np, Np, Np, Npm, 1.0};
+        }
+        SCATT_TRY(sc.L.copy(ct));
+        for (int i = 0; i < n; ++i)
+            SCATT_CUDA_TRY(cudaMemcpyAsync(psi_host + ((size_t)i * R + (size_t)(N - n_lo)) * npm2, ps[slot_of[i]].top,
+                                           npm2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    // ---- the backward sweep, segment by segment, last to first, down to n_lo
+    const int Ntc = sc.Nt_cap, Npc = sc.Np_cap;
+    std::vector<double*> zc(n), zn(n);
+    for (int e = 0; e < n; ++e) { zc[e] = sc.P[e].Z0; zn[e] = ps[e].Z1; }
+    const size_t ne = seg * (size_t)n;
+    DevBuf<GemmEntry> dmz, dmr, dmp;
+    DevBuf<CopyEntry> dcr;
+    SCATT_TRY(dmz.alloc(ne));
+    SCATT_TRY(dmr.alloc(ne));
+    SCATT_TRY(dmp.alloc(ne));
+    SCATT_TRY(dcr.alloc(ne));
+    std::vector<GemmEntry> hmz(ne), hmr(ne), hmp(ne);
+    std::vector<CopyEntry> hcr(ne, CopyEntry{nullptr, nullptr, 0, 0, 1, 1, 0.0});
+    for (int si = nseg - 1; si >= 0; --si) {
+        const int a = si * segment, bnd = std::min(a + segment, N);
+        if (bnd <= n_lo) break;
+        // recompute Sinv(n), R^-1(n) of [a, bnd) from the checkpoint into the segment stores
+        for (int e = 0; e < n; ++e) {
+            EnergyDev& d = sc.ed[e];
+            const size_t nt2 = (size_t)d.Nt * d.Nt;
+            if (a >= 1)
+                SCATT_CUDA_TRY(cudaMemcpyAsync(((a - 1) & 1) ? d.Rinv1 : d.Rinv0, ps[e].ck + si * al(nt2),
+                                               nt2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            d.seg_lo = a;
+            d.seg_hi = bnd;
+        }
+        SCATT_CUDA_TRY(cudaMemcpyAsync(sc.d_ed.p, sc.ed.data(), n * sizeof(EnergyDev), cudaMemcpyHostToDevice, s));
+        b.n_stop = bnd;
+        k_set_group<<<1, 1, 0, s>>>(b, 0, a);
+        SCATT_COUNT_LAUNCH(1);
+        sc.grp[0].n0 = a;
+        sc.grp[0].C = std::min(SCHUR_CHUNK, bnd - a);
+        while (sc.grp[0].n0 >= 0) SCATT_TRY(run_chunk(sc, nullptr));
+        sc.grp[0].n0 = -1;
+        // this segment's staging slab is free once its previous copies are done
+        const int par = si & 1;
+        if (pending[par]) {
+            SCATT_CUDA_TRY(cudaStreamWaitEvent(s, ev_copied[par].e, 0));
+            pending[par] = false;
+        }
+        // the entries of the segment's steps n = bnd - 1 .. max(a, n_lo), in launch order
+        const int m_lo = std::max(a, n_lo);
+        const int steps = bnd - m_lo;
+        for (int k = 0; k < steps; ++k) {
+            const int m = bnd - 1 - k;
+            const bool exch = m < b.n_tr && Nf > 0;
+            for (int e = 0; e < n; ++e) {
+                const EnergyDev& d = sc.ed[e];
+                const int Np = d.Np, Nt = d.Nt;
+                const size_t i = (size_t)k * n + e;
+                hmz[i] = GemmEntry{d.segR + (size_t)(m - a) * Nt * Nt, zc[e], zn[e], Nt, Np, Nt, Nt, Nt, Nt, 1.0, 0.0};
+                const double* sinv = d.segS + (size_t)(m - a) * Np * Np;
+                double* dst = ps[e].stg[par] + (size_t)(m - a) * npm2;
+                if (exch) {
+                    hcr[i] = CopyEntry{zn[e], ps[e].rhs, Np, Np, Nt, Np, 1.0};
+                    hmr[i] = GemmEntry{sc.vb.Bs.p, zn[e] + Np, ps[e].rhs, Np, Np, Nf, Npm, Nt, Np, -1.0, 1.0};
+                    hmp[i] = GemmEntry{sinv, ps[e].rhs, dst, Np, Np, Np, Np, Np, Npm, 1.0, 0.0};
+                } else {
+                    hmp[i] = GemmEntry{sinv, zn[e], dst, Np, Np, Np, Np, Nt, Npm, 1.0, 0.0};
+                }
+            }
+            std::swap(zc, zn);
+        }
+        if (steps > 0) {
+            const size_t cnt = (size_t)steps * n;
+            SCATT_CUDA_TRY(cudaMemcpyAsync(dmz.p, hmz.data(), cnt * sizeof(GemmEntry), cudaMemcpyHostToDevice, s));
+            SCATT_CUDA_TRY(cudaMemcpyAsync(dmr.p, hmr.data(), cnt * sizeof(GemmEntry), cudaMemcpyHostToDevice, s));
+            SCATT_CUDA_TRY(cudaMemcpyAsync(dmp.p, hmp.data(), cnt * sizeof(GemmEntry), cudaMemcpyHostToDevice, s));
+            SCATT_CUDA_TRY(cudaMemcpyAsync(dcr.p, hcr.data(), cnt * sizeof(CopyEntry), cudaMemcpyHostToDevice, s));
+        }
+        for (int k = 0; k < steps; ++k) {
+            const int m = bnd - 1 - k;
+            const bool exch = m < b.n_tr && Nf > 0;
+            SCATT_TRY(gemm_batched(dmz.p + (size_t)k * n, n, Ntc, Npc, 0, 0, s));       // Z_m = R^-1(m) Z_{m+1}
+            if (m >= n_hi) continue;
+            if (exch) {
+                sc.vb.build(b, m, s);                                                     // Bs(m)
+                k_copy<<<dim3(64, n), TPB, 0, s>>>(dcr.p + (size_t)k * n);                // rhs = Z_psi
+                SCATT_COUNT_LAUNCH(1);
+                SCATT_TRY(gemm_batched(dmr.p + (size_t)k * n, n, Npc, Npc, 0, 0, s));   // rhs -= Bs(m) Z_f
+            }
+            SCATT_TRY(gemm_batched(dmp.p + (size_t)k * n, n, Npc, Npc, 0, 0, s));       // psi(m) = Sinv(m) rhs
+        }
+        SCATT_CUDA_TRY(cudaGetLastError());
+        // rows [r0, r1) of the staging slab go to the host on the copy stream
+        const int r0 = m_lo, r1 = std::min(bnd, n_hi);
+        if (r1 > r0) {
+            SCATT_CUDA_TRY(cudaEventRecord(ev_done[par].e, s));
+            SCATT_CUDA_TRY(cudaStreamWaitEvent(cs.s, ev_done[par].e, 0));
+            for (int i = 0; i < n; ++i)
+                SCATT_CUDA_TRY(cudaMemcpyAsync(psi_host + ((size_t)i * R + (size_t)(r0 - n_lo)) * npm2,
+                                               ps[slot_of[i]].stg[par] + (size_t)(r0 - a) * npm2,
+                                               (size_t)(r1 - r0) * npm2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                               cs.s));
+            SCATT_CUDA_TRY(cudaEventRecord(ev_copied[par].e, cs.s));
+            pending[par] = true;
+        }
+    }
+    for (int e = 0; e < n; ++e) sc.ed[e].seg_lo = sc.ed[e].seg_hi = 0;
+    b.n_stop = b.Nr;
+    SCATT_CUDA_TRY(cudaStreamSynchronize(s));
+    SCATT_CUDA_TRY(cudaStreamSynchronize(cs.s));
+    if (first != SCATT_OK) set_last_error(msg);
+    return first;
+}
+
 }  // namespace scatt
 
 // ================================================================ C ABI
@@ -3447,6 +3683,27 @@ int scatt_adjoint_close(scatt_adjoint* h) {
     cudaSetDevice(h->ctx->c.device);
     delete h;
     return SCATT_OK;
+}
+
+// ---------------------------------------------------------------- psi sweep
+int scatt_psi_sweep(scatt_ctx* ctx, const scatt_solve_opts* opts, int n_energy, const double* energies,
+                    const int* l_cont, int segment, int n_lo, int n_hi, const scatt_outputs* outputs,
+                    double* psi_out) {
+    if (!ctx || !energies || !outputs || !psi_out || n_energy < 1) {
+        set_last_error("scatt_psi_sweep: null argument or no energies");
+        return SCATT_ERR_ARG;
+    }
+    if (!ctx->c.tab || !ctx->c.tab->ready) {
+        set_last_error("scatt_psi_sweep: upload the static inputs first");
+        return SCATT_ERR_STATE;
+    }
+    SCATT_TRY(require_device());
+    SCATT_CUDA_TRY(cudaSetDevice(ctx->c.device));
+    SCATT_TRY(check_energies(*ctx->c.tab, n_energy, energies, l_cont, "scatt_psi_sweep"));
+    scatt_solve_opts o;
+    if (opts) o = *opts;
+    else scatt_default_opts(&o);
+    return psi_sweep(ctx->c, o, n_energy, energies, l_cont, segment, n_lo, n_hi, outputs, psi_out);
 }
 
 }  // extern "C"

@@ -74,6 +74,8 @@ def _bind():
     L.scatt_scan_pending.argtypes = [C.c_void_p, iptr, iptr]
     L.scatt_scan_shape.argtypes = [C.c_void_p, iptr, iptr]
     L.scatt_scan_close.argtypes = [C.c_void_p]
+    L.scatt_psi_sweep.argtypes = [C.c_void_p, C.POINTER(SolveOpts), C.c_int, dptr, iptr, C.c_int, C.c_int, C.c_int,
+                                  C.POINTER(Outputs), dptr]
     _bound = True
 
 
@@ -203,6 +205,39 @@ class ScanSolver:
             check(code)
         return [result_of(arr, status, e, float(E[e]), int(lc[e]) if lc is not None else None, self.Np)
                 for e in range(nE)]
+
+    def psi_sweep(self, energies, n_lo: int = 0, n_hi: int | None = None, segment: int = 64, l_cont=None,
+                  opts: SolveOpts | None = None, alloc=None, raise_on_error=True):
+        """psi(n) for n_lo <= n < n_hi (default: the whole grid) of every
+        energy, by the back-propagation of BackPropagator::run / get_psi
+        (scatt_psi_sweep), with the energies' results.
+
+        Returns (results, psi): psi[i, r] is psi(n_lo + r) of energy i as an
+        Np_max x Np_max array, rows = channel, columns = solution (zero
+        outside the energy's own block).  alloc(shape, dtype) may supply the
+        host buffer -- page-locked memory lets the device-to-host copies
+        overlap the sweep."""
+        E = np.ascontiguousarray(energies, dtype=np.float64).reshape(-1)
+        nE = E.size
+        n_hi = self.inp.Nr if n_hi is None and self.inp is not None else n_hi
+        if n_hi is None:
+            n_hi = int(self.preproc["Nr"])
+        lc = None
+        if l_cont is not None:
+            lc = np.ascontiguousarray(np.broadcast_to(np.asarray(l_cont, dtype=np.int32), (nE,)))
+        arr, status, out = output_arrays(nE, self.Np, self.n_occ)
+        mk = alloc or (lambda shape, dtype=np.float64: np.zeros(shape, dtype=dtype))
+        buf = mk((nE, n_hi - n_lo, self.Np, self.Np))
+        o = opts if opts is not None else default_opts()
+        code = lib().scatt_psi_sweep(self._ctx, C.byref(o), nE, as_dptr(E),
+                                     lc.ctypes.data_as(iptr) if lc is not None else None,
+                                     int(segment), int(n_lo), int(n_hi), C.byref(out), as_dptr(buf))
+        if code != 0 and raise_on_error:
+            check(code)
+        res = [result_of(arr, status, e, float(E[e]), int(lc[e]) if lc is not None else None, self.Np)
+               for e in range(nE)]
+        # column-major matrices: the transposed view of each C-order slab
+        return res, np.swapaxes(buf, 2, 3)
 
     def scan(self, slots: int = 0, groups: int = 1, l_cont_max: int | None = None,
              opts: SolveOpts | None = None, alloc=None) -> "Scan":
