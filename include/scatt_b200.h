@@ -391,6 +391,23 @@ int scatt_psi_sweep(scatt_ctx* ctx, const scatt_solve_opts* opts, int n_energy, 
                     const int* l_cont, int segment, int n_lo, int n_hi, const scatt_outputs* outputs,
                     double* psi_out);
 
+/* Continuum-continuum dipole, the consumer of the psi store
+ * (postprocessing/two_photon_delay/cc_dipole/src/CCDipole.cpp:294-334 and
+ * its range-accumulating API, include/CCDipole.hpp): for one final state
+ * kappa and n_nu intermediate states nu, length gauge,
+ *   cc_nu[beta, alpha] = sum_i w_i r_i psi_kappa(i)[:, beta]^T A^q psi_nu(i)[:, alpha]
+ * over the radial points ir0 .. ir0 + n_pts - 1 (n_pts >= 5), r_i =
+ * (ir0 + i + 1) dr (r_min = dr, CCDipole.cpp:236), w_i the window's Simpson
+ * weights (:100-122), A^q = sqrt(4 pi / 3) gaunt_real(l_mu, m_mu, 1, q,
+ * l_nu, m_nu) with q = +1 / -1 / 0 for x / y / z (:135-160).  psi_kappa:
+ * n_pts column-major n_mu x n_mu matrices with leading dimension ld, ld^2
+ * apart (one energy of scatt_psi_sweep's output, ld = Np_max); psi_nu: n_nu
+ * such stacks one after another; cc: n_nu column-major n_mu x n_mu
+ * matrices (ld n_mu).  Host buffers; the points stream through the device
+ * in chunks, each psi_kappa chunk read once for all nu. */
+int scatt_cc_dipole(int n_mu, int ld, int n_pts, int ir0, double dr, int q, const double* psi_kappa,
+                    int n_nu, const double* psi_nu, double* cc);
+
 /* ------------------------------------------------------ file formats
  * Host-only entry points (no device work, no GPU needed) for the files
  * around the path, on an HDF5 subset written from the public file-format

@@ -64,6 +64,7 @@ def lib():
     L.scatt_bench_inverse.argtypes = [C.c_int, C.c_int, C.c_int, dptr]
     L.scatt_bench_gemm.argtypes = [C.c_int] * 8 + [dptr]
     L.scatt_set_inverse_blocking.argtypes = [C.c_int]
+    L.scatt_cc_dipole.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, dptr, C.c_int, dptr, dptr]
     _lib = L
     return L
 
@@ -156,3 +157,32 @@ def set_inverse_blocking(scheme: int):
     3: two-level row-contiguous; 4: as 3 with 128-column windows; 5, 6: as 3, 4
     with the small cluster panel."""
     check(lib().scatt_set_inverse_blocking(int(scheme)))
+
+
+CC_Q = {"x": 1, "y": -1, "z": 0}       # CCDipole.cpp: q of each polarisation
+
+
+def cc_dipole(psi_kappa, psi_nu, ir0: int, dr: float, pol: str, n_mu: int | None = None) -> np.ndarray:
+    """Continuum-continuum dipoles of one final state against n_nu
+    intermediate states on the device (scatt_cc_dipole), length gauge.
+
+    psi_kappa: (n_pts, L, L) with psi_kappa[i] = psi(ir0 + i) (rows =
+    channel, columns = solution; one energy of ScanSolver.psi_sweep's
+    output); psi_nu: (n_nu, n_pts, L, L) or (n_pts, L, L).  n_mu (default
+    L): the leading block used.  Returns (n_nu, n_mu, n_mu) with
+    cc[v][beta, alpha] = sum_i w_i r_i psi_kappa(i)[:, beta] . A^q psi_nu_v(i)[:, alpha]."""
+    pk = np.asarray(psi_kappa, dtype=np.float64)
+    pn = np.asarray(psi_nu, dtype=np.float64)
+    if pn.ndim == 3:
+        pn = pn[None]
+    n_pts, L = pk.shape[0], pk.shape[1]
+    if pn.shape[1:] != pk.shape:
+        raise ValueError("psi_nu stacks must match psi_kappa's shape")
+    n_mu = L if n_mu is None else int(n_mu)
+    # column-major matrices: the C-order buffers of the transposed views
+    ck = np.ascontiguousarray(np.swapaxes(pk, -1, -2))
+    cn = np.ascontiguousarray(np.swapaxes(pn, -1, -2))
+    out = np.zeros((pn.shape[0], n_mu, n_mu))
+    check(lib().scatt_cc_dipole(n_mu, L, n_pts, int(ir0), float(dr), CC_Q[pol], as_dptr(ck), pn.shape[0],
+                                as_dptr(cn), as_dptr(out)))
+    return np.swapaxes(out, 1, 2)
