@@ -192,10 +192,23 @@ def oracle_baseline_mix(sts, ks, budget_s=20.0):
         return oracle_baseline(sts, ks, budget_s)
     parts = [oracle_baseline(st, ks, budget_s / len(sts)) for st in sts]
     t = float(np.mean([p["sec_per_energy"] for p in parts]))
-    return {"value": 1.0 / t, "unit": "energies/s", "cores": parts[0]["cores"], "kind": "port",
+    return {"value": 1.0 / t, "unit": "energies/s", "cores": parts[0]["cores"], "cpu_model": parts[0]["cpu_model"],
+            "kind": "port",
             "sample": " | ".join(f"l_cont {st.l_cont}: " + p["sample"] for st, p in zip(sts, parts))
                       + "; seconds per energy averaged over the cutoffs",
             "sec_per_energy": t}
+
+
+def cpu_model() -> str:
+    """The host CPU's model name (first entry of /proc/cpuinfo), for the baseline's record."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def oracle_baseline(st, ks, budget_s=20.0):
@@ -237,6 +250,7 @@ def oracle_baseline(st, ks, budget_s=20.0):
         "value": 1.0 / t_energy,
         "unit": "energies/s",
         "cores": nthreads,
+        "cpu_model": cpu_model(),
         "kind": "port",
         "sample": (f"oracle (numpy/scipy-OpenBLAS, {nthreads} threads): {c_in} radial steps at n={n_in} "
                    f"(exchange region) and {c_out} at n={n_out} of one energy (k={np.sqrt(2 * E):.3f}); "
@@ -303,7 +317,7 @@ def main():
                 "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
                 "config": workload,
-                "cpu_baseline": {k: timed[-1][k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "cpu_baseline": {k: timed[-1][k] for k in ("value", "unit", "cores", "cpu_model", "kind", "sample")},
                 "e2e": {"value": v, "unit": "energies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -417,7 +431,7 @@ def main():
             try:
                 line["cpu_baseline"] = {k: v for k, v in oracle_baseline_mix(oracle_setup(inp, cfg.get("l_conts")), ks,
                                                                              a.cpu_budget).items()
-                                        if k in ("value", "unit", "cores", "kind", "sample")}
+                                        if k in ("value", "unit", "cores", "cpu_model", "kind", "sample")}
             except Exception as ex:          # the baseline is reported, never required
                 line["cpu_baseline"] = {"value": None, "error": str(ex)}
         print(json.dumps(line))

@@ -30,3 +30,16 @@ def pytest_collection_modifyitems(config, items):
     for it in items:
         if "gpu" in it.keywords:
             it.add_marker(skip)
+
+
+def pytest_sessionfinish(session, exitstatus):
+    """Release what the tests left for the garbage collector (solvers, scans
+    and adjoints in reference cycles hold device memory and library handles)
+    while the CUDA runtime and torch are still fully alive, instead of at
+    interpreter shutdown, and let the device finish its queued work."""
+    import gc
+    gc.collect()
+    if "torch" in sys.modules:
+        torch = sys.modules["torch"]
+        if torch.cuda.is_available() and torch.cuda.is_initialized():
+            torch.cuda.synchronize()
