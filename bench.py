@@ -108,6 +108,30 @@ def predict_seconds(config: str, slots: int, groups: int, steps: int, warmup: in
     return setup_s + cpu_s + plan(config, slots, groups, steps, warmup)["chunks_total"] * (fixed + per_slot * slots)
 
 
+def job_grid(config: str, world: int) -> np.ndarray:
+    """The k grid of the whole job: the workload's grid at one GPU; at N
+    ranks the same k range with N times the points, so that every rank
+    streams as many energies as one GPU does (weak scaling: the per-rank
+    work is fixed as N grows)."""
+    ks = CONFIGS[config]["ks"]()
+    if world <= 1:
+        return ks
+    return np.linspace(ks[0], ks[-1], ks.size * world)
+
+
+def rank_block(config: str, world: int, rank: int, n_f: int):
+    """This rank's contiguous, cost-balanced block of the job's k grid: the
+    momenta and each energy's continuum cutoff."""
+    from scatt_b200 import shard
+    cfg = CONFIGS[config]
+    ks = job_grid(config, world)
+    lcs = cfg.get("l_conts")
+    lc_all = (np.array([lcs[i % len(lcs)] for i in range(ks.size)], dtype=np.int32) if lcs
+              else np.full(ks.size, cfg["kw"]["l_cont"], dtype=np.int32))
+    blocks = shard.partition(shard.energy_cost(lc_all, n_f), world)
+    return ks[blocks[rank]], lc_all[blocks[rank]]
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -293,7 +317,7 @@ def main():
     ws, rank, local = dist_env()
     cfg = CONFIGS[a.config]
     from scatt_b200 import synth
-    ks = cfg["ks"]()
+    ks = job_grid(a.config, ws)
     slots = a.slots or cfg["slots"]
     groups = a.groups or cfg["groups"]
     graphs = cfg["graphs"] if a.graphs < 0 else a.graphs
@@ -335,14 +359,9 @@ def main():
     t0 = time.time()
     sol = S.ScanSolver(inp, device=local)
     setup_s = time.time() - t0
-    # this rank's contiguous block of the k grid (cost-balanced; one l_cont here)
-    from scatt_b200 import shard
-    lcs = cfg.get("l_conts")
-    lc_all = (np.array([lcs[i % len(lcs)] for i in range(len(ks))], dtype=np.int32) if lcs
-              else np.full(len(ks), cfg["kw"]["l_cont"], dtype=np.int32))
-    blocks = shard.partition(shard.energy_cost(lc_all, sol.Nf), ws)
-    Es_all = 0.5 * ks[blocks[rank]] ** 2
-    lc_mine = lc_all[blocks[rank]]
+    # this rank's contiguous block of the job's k grid (cost-balanced)
+    k_mine, lc_mine = rank_block(a.config, ws, rank, sol.Nf)
+    Es_all = 0.5 * k_mine ** 2
     if slots > len(Es_all):
         raise SystemExit(f"--slots {slots} exceeds this rank's {len(Es_all)} energies")
     gsize = slots // groups

@@ -30,3 +30,23 @@ def test_driver_run_fits_with_margin():
 def test_default_run_is_short():
     c = bench.CONFIGS["h2o_like"]
     assert bench.predict_seconds("h2o_like", c["slots"], c["groups"], steps=4, warmup=3) <= 600.0
+
+
+def test_every_rank_streams_a_full_block():
+    """Weak scaling: at N ranks the job's k grid has N times the points of
+    the one-GPU workload over the same range, and every rank's cost-balanced
+    block holds at least the slots it streams, so `bench.py --gpus N` runs
+    the one-GPU per-rank workload at every N."""
+    import numpy as np
+    for cfg in ("h2o_like", "h2o_mixed", "h2_like"):
+        c = bench.CONFIGS[cfg]
+        one = c["ks"]()
+        assert np.array_equal(bench.job_grid(cfg, 1), one)
+        for world in (1, 2, 4, 8):
+            ks = bench.job_grid(cfg, world)
+            assert ks.size == one.size * world and ks[0] == one[0] and ks[-1] == one[-1]
+            got = [bench.rank_block(cfg, world, r, 605) for r in range(world)]
+            assert np.array_equal(np.concatenate([k for k, _ in got]), ks)
+            for k, lc in got:
+                assert k.size >= c["slots"], (cfg, world, k.size)
+                assert lc.size == k.size
