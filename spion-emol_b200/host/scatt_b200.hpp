@@ -13,6 +13,7 @@
 // the header needs nothing beyond the standard library and scatt_b200.h.
 #pragma once
 
+#include <algorithm>
 #include <array>
 #include <chrono>
 #include <complex>
@@ -205,6 +206,37 @@ public:
         return res;
     }
 
+    // psi(n) for n_lo <= n < n_hi of every energy, by the back-propagation of
+    // BackPropagator::run / get_psi (src/scatt/BackPropagator.cpp:199-802)
+    // through scatt_psi_sweep: psi[e][n - n_lo] is Np x Np (rows = channel,
+    // columns = solution).  The energies' other results are not kept here
+    // (solve() returns them).  Throws on a failing energy.
+    std::vector<std::vector<Matrix>> psi(const std::vector<double>& E, int n_lo, int n_hi, int segment = 64,
+                                         bool allow_closed_channels = false) {
+        std::vector<double> buf;
+        psi_into(E, n_lo, n_hi, segment, allow_closed_channels, buf);
+        const size_t n2 = (size_t)Np_ * Np_;
+        std::vector<std::vector<Matrix>> out(E.size());
+        for (size_t e = 0; e < E.size(); ++e)
+            for (int n = n_lo; n < n_hi; ++n)
+                out[e].push_back(block(buf.data() + (e * (size_t)(n_hi - n_lo) + (size_t)(n - n_lo)) * n2, Np_, Np_));
+        return out;
+    }
+    // The same into one flat buffer in the C ABI's layout: energy-major, then
+    // point, each Np x Np column-major.  Page-locked memory (cudaHostAlloc or
+    // cudaHostRegister on out.data()) lets the copies overlap the sweep.
+    void psi_into(const std::vector<double>& E, int n_lo, int n_hi, int segment, bool allow_closed_channels,
+                  std::vector<double>& out) {
+        scatt_solve_opts o;
+        scatt_default_opts(&o);
+        o.allow_closed_channels = allow_closed_channels ? 1 : 0;
+        std::vector<int> st(E.size());
+        scatt_outputs res{};
+        res.status = st.data();
+        out.assign(E.size() * (size_t)std::max(0, n_hi - n_lo) * Np_ * Np_, 0.0);
+        check(scatt_psi_sweep(ctx_, &o, (int)E.size(), E.data(), nullptr, segment, n_lo, n_hi, &res, out.data()));
+    }
+
 private:
     static Matrix block(const double* p, int r, int c) {
         Matrix m(r, c);
@@ -215,6 +247,31 @@ private:
     scatt_ctx* ctx_ = nullptr;
     int n_transition_ = 0, Np_ = 0;
 };
+
+// cc_raw of one final state kappa against one intermediate state nu
+// (cc_dipole::compute_cc_dipole, postprocessing/two_photon_delay/cc_dipole/
+// include/CCDipole.hpp; CCDipole.cpp:294-334), length gauge, on the device
+// through scatt_cc_dipole: psi_kappa[i], psi_nu[i] are psi at radial index
+// ir0 + i (as ScanSolver::psi returns them, all N_psi x N_psi), pol one of
+// 'x', 'y', 'z'.  Simpson weights over the whole window, r = (ir0 + i + 1) dr.
+inline Matrix compute_cc_dipole(const std::vector<Matrix>& psi_kappa, const std::vector<Matrix>& psi_nu, int ir0,
+                                double dr, char pol) {
+    if (psi_kappa.empty() || psi_kappa.size() != psi_nu.size())
+        throw std::runtime_error("compute_cc_dipole: psi_kappa and psi_nu need the same non-empty window");
+    const int n = psi_kappa[0].rows;
+    const size_t n2 = (size_t)n * n;
+    std::vector<double> k(psi_kappa.size() * n2), v(psi_nu.size() * n2);
+    for (size_t i = 0; i < psi_kappa.size(); ++i) {
+        if (psi_kappa[i].rows != n || psi_kappa[i].cols != n || psi_nu[i].rows != n || psi_nu[i].cols != n)
+            throw std::runtime_error("compute_cc_dipole: every psi must be N_psi x N_psi");
+        std::copy(psi_kappa[i].data.begin(), psi_kappa[i].data.end(), k.begin() + i * n2);
+        std::copy(psi_nu[i].data.begin(), psi_nu[i].data.end(), v.begin() + i * n2);
+    }
+    const int q = pol == 'x' ? 1 : pol == 'y' ? -1 : pol == 'z' ? 0 : 2;
+    Matrix cc(n, n);
+    check(scatt_cc_dipole(n, n, (int)psi_kappa.size(), ir0, dr, q, k.data(), 1, v.data(), cc.data.data()));
+    return cc;
+}
 
 // ------------------------------------------------------------ per-step seam
 // The reference's device seam -- GpuContext and the Sinv, forward and back

@@ -145,3 +145,19 @@ def test_seam_headers_take_the_reference_calls(tmp_path):
     assert r.returncode == 0, r.stderr
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, (r.stdout, r.stderr)
+
+
+def test_psi_and_cc_dipole_calls_compile(tmp_path):
+    """tests/host_psi_check.cpp calls ScanSolver::psi, psi_into and
+    compute_cc_dipole of the C++ interface: warning-free, and without a GPU
+    each throws the library's no-device error."""
+    _driver()
+    exe = tmp_path / "psi_check"
+    cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror",
+           "-I", os.path.join(ROOT, "include"), "-I", os.path.join(PKG, "host"),
+           os.path.join(ROOT, "tests", "host_psi_check.cpp"),
+           "-L", PKG, "-lscatt_b200", f"-Wl,-rpath,{PKG}", "-o", str(exe)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
