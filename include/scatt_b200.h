@@ -408,6 +408,19 @@ int scatt_psi_sweep(scatt_ctx* ctx, const scatt_solve_opts* opts, int n_energy, 
 int scatt_cc_dipole(int n_mu, int ld, int n_pts, int ir0, double dr, int q, const double* psi_kappa,
                     int n_nu, const double* psi_nu, double* cc);
 
+/* ------------------------------------------------------ preprocessing
+ * Hartree potential from the density's single-centre multipoles by the
+ * radial Poisson integrals (preprocessing/src/potential/Hartree.hpp:71-246,
+ * build_V_H):  V_lm(r) = 4 pi / (2l + 1) [ r^-(l+1) int_0^r rho_lm r'^(l+2)
+ * + r^l int_r^R rho_lm r'^(1-l) ] on r_k = r0 + k dr, k < Nr, with the
+ * cumulative integrator of preprocessing/src/sce/RadialGrid.hpp:84-100 and
+ * the reference's guards (channels above the overflow-safe l or with
+ * max |rho_lm| < 1e-12 stay 0; non-finite values become 0; V_00(0) =
+ * 4 pi int rho_00 r').  rho_lm: n_rows >= (l_max + 1)^2 rows of Nr points,
+ * row-major (channel idx = l^2 + l + m); V_H: (l_max + 1)^2 rows of Nr,
+ * row-major -- the layout scatt_scan_desc.V_H takes.  Host buffers. */
+int scatt_hartree(int l_max, int n_rows, int Nr, double r0, double dr, const double* rho_lm, double* V_H);
+
 /* ------------------------------------------------------ file formats
  * Host-only entry points (no device work, no GPU needed) for the files
  * around the path, on an HDF5 subset written from the public file-format

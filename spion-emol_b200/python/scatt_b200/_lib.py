@@ -64,6 +64,7 @@ def lib():
     L.scatt_bench_inverse.argtypes = [C.c_int, C.c_int, C.c_int, dptr]
     L.scatt_bench_gemm.argtypes = [C.c_int] * 8 + [dptr]
     L.scatt_set_inverse_blocking.argtypes = [C.c_int]
+    L.scatt_hartree.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, dptr, dptr]
     L.scatt_cc_dipole.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, dptr, C.c_int, dptr, dptr]
     _lib = L
     return L
@@ -186,3 +187,15 @@ def cc_dipole(psi_kappa, psi_nu, ir0: int, dr: float, pol: str, n_mu: int | None
     check(lib().scatt_cc_dipole(n_mu, L, n_pts, int(ir0), float(dr), CC_Q[pol], as_dptr(ck), pn.shape[0],
                                 as_dptr(cn), as_dptr(out)))
     return np.swapaxes(out, 1, 2)
+
+
+def hartree(rho_lm, dr: float, l_max: int, r0: float = 0.0) -> np.ndarray:
+    """V_H multipoles ((l_max + 1)^2, Nr) from the density multipoles rho_lm
+    (>= (l_max + 1)^2 rows, Nr columns) by the radial Poisson integrals of
+    the preprocessing step, on the device (scatt_hartree)."""
+    rho = np.ascontiguousarray(rho_lm, dtype=np.float64)
+    n_lm = (int(l_max) + 1) ** 2
+    out = np.zeros((n_lm, rho.shape[1]))
+    check(lib().scatt_hartree(int(l_max), rho.shape[0], rho.shape[1], float(r0), float(dr), as_dptr(rho),
+                              as_dptr(out)))
+    return out
