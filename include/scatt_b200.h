@@ -421,6 +421,20 @@ int scatt_cc_dipole(int n_mu, int ld, int n_pts, int ir0, double dr, int q, cons
  * row-major -- the layout scatt_scan_desc.V_H takes.  Host buffers. */
 int scatt_hartree(int l_max, int n_rows, int Nr, double r0, double dr, const double* rho_lm, double* V_H);
 
+/* Single-centre expansion (preprocessing/src/sce/SCE.hpp:122-266, project):
+ * F_lm(r_k) = int F(r_k, Omega) Y^R_lm(Omega) dOmega, l <= Lmax, on the grid
+ * of preprocessing/src/angular/Grid.hpp: n_theta = Lmax + 1 Gauss-Legendre
+ * nodes in cos(theta), ascending; n_phi = 2 (Lmax + 1) nodes
+ * phi_j = 2 pi j / n_phi.  scatt_sce_grid returns the grid (cos_theta and
+ * weights: n_theta each; phi: n_phi), host-only.  scatt_sce_project takes
+ * the samples F(r_k, theta_i, phi_j) at samples[(k n_theta + i) n_phi + j]
+ * for Nr radial points and writes F_lm row-major [(Lmax + 1)^2][Nr]
+ * (channel l^2 + l + m, Y^R of SCE.hpp:11-15).  The Fourier and Legendre
+ * steps run as DMMA GEMMs over chunks of `chunk` radial points (<= 0:
+ * chosen to hold a chunk's buffers in 512 MB).  Host buffers. */
+int scatt_sce_grid(int Lmax, double* cos_theta, double* weights, double* phi);
+int scatt_sce_project(int Lmax, int Nr, int chunk, const double* samples, double* F_lm);
+
 /* ------------------------------------------------------ file formats
  * Host-only entry points (no device work, no GPU needed) for the files
  * around the path, on an HDF5 subset written from the public file-format

@@ -64,6 +64,8 @@ def lib():
     L.scatt_bench_inverse.argtypes = [C.c_int, C.c_int, C.c_int, dptr]
     L.scatt_bench_gemm.argtypes = [C.c_int] * 8 + [dptr]
     L.scatt_set_inverse_blocking.argtypes = [C.c_int]
+    L.scatt_sce_grid.argtypes = [C.c_int, dptr, dptr, dptr]
+    L.scatt_sce_project.argtypes = [C.c_int, C.c_int, C.c_int, dptr, dptr]
     L.scatt_hartree.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, dptr, dptr]
     L.scatt_cc_dipole.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, dptr, C.c_int, dptr, dptr]
     _lib = L
@@ -198,4 +200,23 @@ def hartree(rho_lm, dr: float, l_max: int, r0: float = 0.0) -> np.ndarray:
     out = np.zeros((n_lm, rho.shape[1]))
     check(lib().scatt_hartree(int(l_max), rho.shape[0], rho.shape[1], float(r0), float(dr), as_dptr(rho),
                               as_dptr(out)))
+    return out
+
+
+def sce_grid(Lmax: int):
+    """(cos_theta, weights, phi) of the single-centre expansion's angular grid."""
+    x, w, p = np.zeros(Lmax + 1), np.zeros(Lmax + 1), np.zeros(2 * (Lmax + 1))
+    check(lib().scatt_sce_grid(int(Lmax), as_dptr(x), as_dptr(w), as_dptr(p)))
+    return x, w, p
+
+
+def sce_project(samples, Lmax: int, chunk: int = 0) -> np.ndarray:
+    """F_lm ((Lmax + 1)^2, Nr) from samples (Nr, n_theta, n_phi) of F on the
+    grid of sce_grid(Lmax), on the device (scatt_sce_project)."""
+    X = np.ascontiguousarray(samples, dtype=np.float64)
+    Nr = X.shape[0]
+    if X.shape[1:] != (Lmax + 1, 2 * (Lmax + 1)):
+        raise ValueError("samples must be (Nr, Lmax + 1, 2 (Lmax + 1))")
+    out = np.zeros(((Lmax + 1) ** 2, Nr))
+    check(lib().scatt_sce_project(int(Lmax), Nr, int(chunk), as_dptr(X), as_dptr(out)))
     return out
