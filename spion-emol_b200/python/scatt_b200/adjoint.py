@@ -374,9 +374,12 @@ class Dipoles(torch.autograd.Function):
         return ga, gr, gdV, None, None, None, None, None
 
 
-def observables(energies, D, e_homo: float):
-    """sigma_{length,velocity}_{x,y,z} and tau_* (scatt_b200.observables in
-    torch) from D = Dipoles output (energies ascending)."""
+def observables(energies, D, e_homo: float, n_theta: int = 40, n_phi: int = 80):
+    """The scan observables of scatt_b200.observables in torch, on D's device
+    and inside the autograd graph, from D = Dipoles output (energies
+    ascending): sigma_{length,velocity}_{x,y,z}, tau_* (two or more
+    energies), q_{x,y,z}, dphi_rms_{x,y,z} and beta_{length,velocity}
+    (postprocessing/cross_section_delay.py:195-430)."""
     Es = [float(x) for x in energies]
     k = torch.tensor([math.sqrt(2.0 * E) for E in Es], dtype=F64, device=D.device)
     om = torch.tensor([E - e_homo for E in Es], dtype=F64, device=D.device)
@@ -393,7 +396,39 @@ def observables(energies, D, e_homo: float):
             out[f"sigma_{gauge}_{pol}"] = 8.0 * math.pi / (C_AU * k * om) * s2
         if len(Es) > 1:
             out[f"tau_{gauge}_{pol}"] = torch.sum(torch.conj(Ds) * _d_dk(k, Ds) / k[:, None], dim=1).imag / s2
+    for p, pol in enumerate("xyz"):
+        DL, DV = Dc[:, p, :], Dc[:, 3 + p, :]
+        sL, sV = torch.sum(torch.abs(DL) ** 2, dim=1), torch.sum(torch.abs(DV) ** 2, dim=1)
+        out[f"q_{pol}"] = sV / (om ** 2 * sL)
+        dphi = torch.angle(DV * torch.conj(DL))
+        w = torch.abs(DL) * torch.abs(DV)
+        out[f"dphi_rms_{pol}"] = torch.sqrt(torch.sum(w * dphi ** 2, dim=1) / torch.sum(w, dim=1))
+    Y, weights, kx, ky, kz = _beta_grid(Dc.shape[2], n_theta, n_phi, D.device)
+    for g, gauge in enumerate(("length", "velocity")):
+        maps = [torch.tensordot(Dc[:, 3 * g + q, :], Y, dims=([1], [0])) for q in range(3)]
+        sig = torch.sum((torch.abs(maps[0]) ** 2 + torch.abs(maps[1]) ** 2 + torch.abs(maps[2]) ** 2) * weights,
+                        dim=(1, 2)) / 3.0
+        n1 = torch.sum(torch.abs(maps[0] * kx + maps[1] * ky + maps[2] * kz) ** 2 * weights, dim=(1, 2))
+        out[f"beta_{gauge}"] = n1 / sig - 1.0
     return out
+
+
+def _beta_grid(n_ch: int, n_theta: int, n_phi: int, device):
+    """Real Y_lm of channels 0 .. n_ch - 1 on the Gauss-Legendre (cos theta) x
+    trapezoid (phi) grid of observables.beta, its weights and k-hat."""
+
+    from .observables import real_ylm
+    x, w = np.polynomial.legendre.leggauss(n_theta)
+    theta = np.arccos(x)
+    phi = np.arange(n_phi) * (2.0 * math.pi / n_phi)
+    TH, PH = np.meshgrid(theta, phi, indexing="ij")
+    Y = np.empty((n_ch, n_theta, n_phi))
+    for mu in range(n_ch):
+        l = math.isqrt(mu)
+        Y[mu] = real_ylm(l, mu - l * l - l, TH, PH)
+    t = lambda a: torch.tensor(a, dtype=F64, device=device)
+    return (t(Y).to(torch.complex128), t(w[:, None] * (2.0 * math.pi / n_phi)),
+            t(np.sin(TH) * np.cos(PH)), t(np.sin(TH) * np.sin(PH)), t(np.cos(TH)))
 
 
 def _d_dk(k, f):
