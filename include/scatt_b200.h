@@ -434,6 +434,24 @@ int scatt_hartree(int l_max, int n_rows, int Nr, double r0, double dr, const dou
  * chosen to hold a chunk's buffers in 512 MB).  Host buffers. */
 int scatt_sce_grid(int Lmax, double* cos_theta, double* weights, double* phi);
 int scatt_sce_project(int Lmax, int Nr, int chunk, const double* samples, double* F_lm);
+/* The molecular orbitals and the density of a contracted spherical-Gaussian
+ * basis, sampled on the same grid around `origin` (radial points
+ * r_k = r0 + k dr, k < Nr) and projected: the reference's build_basis /
+ * evaluate_mo / evaluate_density (preprocessing/src/basis/MoldenBasis.hpp:
+ * 48-229, the normalisation of SphericalGaussian.hpp and Primitive.hpp)
+ * followed by project.  Shell i: centre shell_center[3i..3i+2] (bohr),
+ * angular momentum shell_l[i], shell_nprim[i] primitives whose exponents
+ * and raw contraction coefficients follow the previous shells' in exps /
+ * coefs; its 2l + 1 AOs in molden order (p: m = +1, -1, 0; l >= 2:
+ * m = 0, +1, -1, +2, -2, ...).  C: n_mo x nbf row-major MO coefficients,
+ * occ: n_mo occupations.  orb_lm: [n_mo][(Lmax + 1)^2][Nr], rho_lm:
+ * [(Lmax + 1)^2][Nr] (either may be NULL).  The AO values (a kernel per
+ * point and shell), the orbitals (Phi^T C^T, a DMMA GEMM), the density and
+ * the projections run on the device over chunks of `chunk` radial points
+ * (<= 0: automatic).  Host buffers. */
+int scatt_sce_basis(int Lmax, int Nr, double r0, double dr, const double* origin, int n_shell, const int* shell_l,
+                    const int* shell_nprim, const double* shell_center, const double* exps, const double* coefs,
+                    int n_mo, const double* C, const double* occ, int chunk, double* orb_lm, double* rho_lm);
 
 /* ------------------------------------------------------ file formats
  * Host-only entry points (no device work, no GPU needed) for the files

@@ -66,6 +66,8 @@ def lib():
     L.scatt_set_inverse_blocking.argtypes = [C.c_int]
     L.scatt_sce_grid.argtypes = [C.c_int, dptr, dptr, dptr]
     L.scatt_sce_project.argtypes = [C.c_int, C.c_int, C.c_int, dptr, dptr]
+    L.scatt_sce_basis.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, dptr, C.c_int, iptr, iptr, dptr, dptr,
+                                  dptr, C.c_int, dptr, dptr, C.c_int, dptr, dptr]
     L.scatt_hartree.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, dptr, dptr]
     L.scatt_cc_dipole.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, dptr, C.c_int, dptr, dptr]
     _lib = L
@@ -220,3 +222,27 @@ def sce_project(samples, Lmax: int, chunk: int = 0) -> np.ndarray:
     out = np.zeros(((Lmax + 1) ** 2, Nr))
     check(lib().scatt_sce_project(int(Lmax), Nr, int(chunk), as_dptr(X), as_dptr(out)))
     return out
+
+
+def sce_basis(shells, C_mo, occ, Lmax: int, Nr: int, r0: float, dr: float, origin=(0.0, 0.0, 0.0),
+              chunk: int = 0):
+    """(orb_lm (n_mo, Nlm, Nr), rho_lm (Nlm, Nr)): the single-centre
+    expansions of the molecular orbitals and the density of a contracted
+    spherical-Gaussian basis on the device (scatt_sce_basis).  shells: a
+    list of (center (3,), l, exponents, raw coefficients); C_mo: (n_mo, nbf)
+    in molden AO order; occ: (n_mo,)."""
+    sl = np.array([int(s[1]) for s in shells], dtype=np.int32)
+    sn = np.array([len(s[2]) for s in shells], dtype=np.int32)
+    sc = np.ascontiguousarray([np.asarray(s[0], dtype=np.float64) for s in shells])
+    ex = np.ascontiguousarray(np.concatenate([np.asarray(s[2], dtype=np.float64) for s in shells]))
+    cf = np.ascontiguousarray(np.concatenate([np.asarray(s[3], dtype=np.float64) for s in shells]))
+    Cm = np.ascontiguousarray(C_mo, dtype=np.float64)
+    oc = np.ascontiguousarray(occ, dtype=np.float64)
+    o = np.ascontiguousarray(origin, dtype=np.float64)
+    n_lm = (Lmax + 1) ** 2
+    orb = np.zeros((Cm.shape[0], n_lm, Nr))
+    rho = np.zeros((n_lm, Nr))
+    check(lib().scatt_sce_basis(int(Lmax), int(Nr), float(r0), float(dr), as_dptr(o), len(shells), as_iptr(sl),
+                                as_iptr(sn), as_dptr(sc), as_dptr(ex), as_dptr(cf), Cm.shape[0], as_dptr(Cm),
+                                as_dptr(oc), int(chunk), as_dptr(orb), as_dptr(rho)))
+    return orb, rho
