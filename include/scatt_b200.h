@@ -444,14 +444,19 @@ int scatt_sce_project(int Lmax, int Nr, int chunk, const double* samples, double
  * and raw contraction coefficients follow the previous shells' in exps /
  * coefs; its 2l + 1 AOs in molden order (p: m = +1, -1, 0; l >= 2:
  * m = 0, +1, -1, +2, -2, ...).  C: n_mo x nbf row-major MO coefficients,
- * occ: n_mo occupations.  orb_lm: [n_mo][(Lmax + 1)^2][Nr], rho_lm:
- * [(Lmax + 1)^2][Nr] (either may be NULL).  The AO values (a kernel per
- * point and shell), the orbitals (Phi^T C^T, a DMMA GEMM), the density and
- * the projections run on the device over chunks of `chunk` radial points
- * (<= 0: automatic).  Host buffers. */
+ * occ: n_mo occupations.  vx_form: 0 none, 1 the Slater local exchange
+ * -(3/pi)^(1/3) rho^(1/3), 2 the Kohn-Sham one, 1.5 times that
+ * (preprocessing/src/potential/LocalExchange.hpp), projected into vx_lm
+ * (given exactly when vx_form != 0).  orb_lm: [n_mo][(Lmax + 1)^2][Nr],
+ * rho_lm and vx_lm: [(Lmax + 1)^2][Nr] (orb_lm and rho_lm may be NULL).
+ * The AO values (a kernel per point and shell), the orbitals (Phi^T C^T, a
+ * DMMA GEMM), the density, the local exchange and the projections run on
+ * the device over chunks of `chunk` radial points (<= 0: automatic).
+ * Host buffers. */
 int scatt_sce_basis(int Lmax, int Nr, double r0, double dr, const double* origin, int n_shell, const int* shell_l,
                     const int* shell_nprim, const double* shell_center, const double* exps, const double* coefs,
-                    int n_mo, const double* C, const double* occ, int chunk, double* orb_lm, double* rho_lm);
+                    int n_mo, const double* C, const double* occ, int vx_form, int chunk, double* orb_lm,
+                    double* rho_lm, double* vx_lm);
 
 /* ------------------------------------------------------ file formats
  * Host-only entry points (no device work, no GPU needed) for the files

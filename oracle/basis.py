@@ -3,8 +3,9 @@ sampled on the single-centre expansion's grid.  TEST INFRASTRUCTURE ONLY
 (the oracle for scatt_sce_basis).
 
 Restates preprocessing/src/basis/MoldenBasis.hpp:48-229 (AtomicOrbital::eval,
-molden_index_to_m, build_basis, evaluate_mo, evaluate_density) and
-SphericalGaussian.hpp / Primitive.hpp (the normalisation):
+molden_index_to_m, build_basis, evaluate_mo, evaluate_density),
+SphericalGaussian.hpp / Primitive.hpp (the normalisation) and
+potential/LocalExchange.hpp (the local exchange of the density):
 
     chi_lm(r) = |r - A|^l Y^R_lm(r - A) sum_a c~_a exp(-alpha_a |r - A|^2)
     c~_a = s c_a N_sph(alpha_a, l),  N_sph^2 = 2^(2l + 7/2) alpha^(l + 3/2) / (sqrt(pi) (2l + 1)!!)
@@ -80,13 +81,24 @@ def grid_points(Lmax: int, radii: np.ndarray, origin) -> np.ndarray:
     return (np.asarray(origin)[None, None, :] + radii[:, None, None] * dirs[None]).reshape(-1, 3)
 
 
-def sce_of_basis(shells, C, occ, Lmax: int, radii: np.ndarray, origin):
-    """(orb_lm (n_mo, Nlm, Nr), rho_lm (Nlm, Nr)): the SCE projections
-    (oracle.sce.project) of every MO and of the density."""
+def v_x_local(rho: np.ndarray, form: int) -> np.ndarray:
+    """LocalExchange.hpp:28-47: -(3/pi)^(1/3) rho^(1/3) (form 1, Slater) or
+    1.5 times that (form 2, Kohn-Sham), rho clamped at 0."""
+    c = (3.0 / math.pi) ** (1.0 / 3.0) * (1.0 if form == 1 else 1.5)
+    return -c * np.cbrt(np.maximum(0.0, rho))
+
+
+def sce_of_basis(shells, C, occ, Lmax: int, radii: np.ndarray, origin, vx_form: int = 0):
+    """(orb_lm (n_mo, Nlm, Nr), rho_lm (Nlm, Nr)), with vx_lm (Nlm, Nr) when
+    vx_form is 1 or 2: the SCE projections (oracle.sce.project) of every MO,
+    of the density and of the local exchange."""
     pts = grid_points(Lmax, radii, origin)
     chi = ao_values(shells, pts)                               # (nbf, P)
     psi = np.asarray(C) @ chi                                  # (n_mo, P)
     rho = np.asarray(occ) @ (psi * psi)
     shape = (radii.size, Lmax + 1, 2 * (Lmax + 1))
     orb = np.stack([SC.project(psi[i].reshape(shape), Lmax) for i in range(psi.shape[0])])
-    return orb, SC.project(rho.reshape(shape), Lmax)
+    rho_lm = SC.project(rho.reshape(shape), Lmax)
+    if vx_form:
+        return orb, rho_lm, SC.project(v_x_local(rho, vx_form).reshape(shape), Lmax)
+    return orb, rho_lm

@@ -283,8 +283,12 @@ __global__ void k_ao_eval(const ShellDev* __restrict__ sh, int n_shell, const do
     }
 }
 
-// rho[p] = sum_i occ_i Psi[p + i Pc]^2, into column n_mo of Psi
-__global__ void k_density(double* __restrict__ Psi, const double* __restrict__ occ, int n_mo, long Pc) {
+// rho[p] = sum_i occ_i Psi[p + i Pc]^2 into column n_mo of Psi; with
+// vx_coef != 0 the local exchange potential -vx_coef rho^(1/3)
+// (LocalExchange.hpp: (3/pi)^(1/3) for Slater, 1.5 (3/pi)^(1/3) for
+// Kohn-Sham) into column n_mo + 1
+__global__ void k_density(double* __restrict__ Psi, const double* __restrict__ occ, int n_mo, long Pc,
+                          double vx_coef) {
     for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < Pc; p += (long)gridDim.x * blockDim.x) {
         double rho = 0.0;
         for (int i = 0; i < n_mo; ++i) {
@@ -292,6 +296,7 @@ __global__ void k_density(double* __restrict__ Psi, const double* __restrict__ o
             rho += occ[i] * v * v;
         }
         Psi[p + (size_t)n_mo * Pc] = rho;
+        if (vx_coef != 0.0) Psi[p + (size_t)(n_mo + 1) * Pc] = -vx_coef * cbrt(fmax(0.0, rho));
     }
 }
 
@@ -351,10 +356,13 @@ int scatt_sce_project(int Lmax, int Nr, int chunk, const double* samples, double
 
 int scatt_sce_basis(int Lmax, int Nr, double r0, double dr, const double* origin, int n_shell, const int* shell_l,
                     const int* shell_nprim, const double* shell_center, const double* exps, const double* coefs,
-                    int n_mo, const double* C, const double* occ, int chunk, double* orb_lm, double* rho_lm) {
+                    int n_mo, const double* C, const double* occ, int vx_form, int chunk, double* orb_lm,
+                    double* rho_lm, double* vx_lm) {
     if (Lmax < 0 || Nr < 1 || !(dr > 0.0) || !origin || n_shell < 1 || !shell_l || !shell_nprim || !shell_center ||
-        !exps || !coefs || n_mo < 1 || !C || !occ || (!orb_lm && !rho_lm)) {
-        set_last_error("scatt_sce_basis: need Lmax >= 0, Nr >= 1, dr > 0, shells, orbitals and an output");
+        !exps || !coefs || n_mo < 1 || !C || !occ || vx_form < 0 || vx_form > 2 || (vx_form > 0) != (vx_lm != nullptr) ||
+        (!orb_lm && !rho_lm && !vx_lm)) {
+        set_last_error("scatt_sce_basis: need Lmax >= 0, Nr >= 1, dr > 0, shells, orbitals, vx_form 0 / 1 / 2 "
+                       "with vx_lm given exactly when it is not 0, and an output");
         return SCATT_ERR_ARG;
     }
     // the normalised contraction of every shell (MoldenBasis.hpp:129-190, SphericalGaussian.hpp)
@@ -390,8 +398,10 @@ int scatt_sce_basis(int Lmax, int Nr, double r0, double dr, const double* origin
         nbf += l == 0 ? 1 : 2 * l + 1;
     }
     SCATT_TRY(require_device());
-    const int nT = Lmax + 1, nP = 2 * (Lmax + 1), nM = 2 * Lmax + 1, n_fn = n_mo + 1;
+    const int nT = Lmax + 1, nP = 2 * (Lmax + 1), nM = 2 * Lmax + 1, n_fn = n_mo + (vx_form ? 2 : 1);
     const long n_lm = (long)(Lmax + 1) * (Lmax + 1), nTP = (long)nT * nP;
+    const double cbrt3pi = std::cbrt(3.0 / SCE_PI);
+    const double vx_coef = vx_form == 1 ? cbrt3pi : vx_form == 2 ? 1.5 * cbrt3pi : 0.0;
     const long per_pt = nTP * (nbf + n_fn) + (long)n_fn * (nT * nM + 2 * n_lm);
     int R = chunk > 0 ? chunk : (int)std::max<long>(1, (64L << 20) / per_pt);
     R = std::min(R, Nr);
@@ -439,12 +449,12 @@ int scatt_sce_basis(int Lmax, int Nr, double r0, double dr, const double* origin
         SCATT_CUDA_TRY(cudaMemcpyAsync(dent.p, &e, sizeof(GemmEntry), cudaMemcpyHostToDevice, s));
         SCATT_TRY(gemm_batched(dent.p, 1, (int)Pc, n_mo, 1, 0, s));
         k_density<<<(int)std::max<long>(1, std::min<long>((Pc + 255) / 256, 148L * 8)), 256, 0, s>>>(dPsi.p, docc.p,
-                                                                                                    n_mo, Pc);
+                                                                                                    n_mo, Pc, vx_coef);
         SCATT_COUNT_LAUNCH(1);
         SCATT_CUDA_TRY(cudaGetLastError());
         SCATT_TRY(pj.run(dPsi.p, Pc, Rc, dOut.p, s));
         for (int f = 0; f < n_fn; ++f) {
-            double* dst = f < n_mo ? (orb_lm ? orb_lm + (size_t)f * n_lm * Nr : nullptr) : rho_lm;
+            double* dst = f < n_mo ? (orb_lm ? orb_lm + (size_t)f * n_lm * Nr : nullptr) : (f == n_mo ? rho_lm : vx_lm);
             if (!dst) continue;
             SCATT_CUDA_TRY(cudaMemcpy2DAsync(dst + c0, (size_t)Nr * sizeof(double), dOut.p + (size_t)f * n_lm * Rc,
                                              (size_t)Rc * sizeof(double), (size_t)Rc * sizeof(double), (size_t)n_lm,

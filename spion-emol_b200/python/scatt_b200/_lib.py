@@ -67,7 +67,7 @@ def lib():
     L.scatt_sce_grid.argtypes = [C.c_int, dptr, dptr, dptr]
     L.scatt_sce_project.argtypes = [C.c_int, C.c_int, C.c_int, dptr, dptr]
     L.scatt_sce_basis.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, dptr, C.c_int, iptr, iptr, dptr, dptr,
-                                  dptr, C.c_int, dptr, dptr, C.c_int, dptr, dptr]
+                                  dptr, C.c_int, dptr, dptr, C.c_int, C.c_int, dptr, dptr, dptr]
     L.scatt_hartree.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, dptr, dptr]
     L.scatt_cc_dipole.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, dptr, C.c_int, dptr, dptr]
     _lib = L
@@ -225,12 +225,13 @@ def sce_project(samples, Lmax: int, chunk: int = 0) -> np.ndarray:
 
 
 def sce_basis(shells, C_mo, occ, Lmax: int, Nr: int, r0: float, dr: float, origin=(0.0, 0.0, 0.0),
-              chunk: int = 0):
-    """(orb_lm (n_mo, Nlm, Nr), rho_lm (Nlm, Nr)): the single-centre
-    expansions of the molecular orbitals and the density of a contracted
-    spherical-Gaussian basis on the device (scatt_sce_basis).  shells: a
-    list of (center (3,), l, exponents, raw coefficients); C_mo: (n_mo, nbf)
-    in molden AO order; occ: (n_mo,)."""
+              chunk: int = 0, vx_form: int = 0):
+    """(orb_lm (n_mo, Nlm, Nr), rho_lm (Nlm, Nr)), and vx_lm (Nlm, Nr) when
+    vx_form is 1 (Slater) or 2 (Kohn-Sham): the single-centre expansions of
+    the molecular orbitals, the density and the local exchange of a
+    contracted spherical-Gaussian basis on the device (scatt_sce_basis).
+    shells: a list of (center (3,), l, exponents, raw coefficients); C_mo:
+    (n_mo, nbf) in molden AO order; occ: (n_mo,)."""
     sl = np.array([int(s[1]) for s in shells], dtype=np.int32)
     sn = np.array([len(s[2]) for s in shells], dtype=np.int32)
     sc = np.ascontiguousarray([np.asarray(s[0], dtype=np.float64) for s in shells])
@@ -242,7 +243,9 @@ def sce_basis(shells, C_mo, occ, Lmax: int, Nr: int, r0: float, dr: float, origi
     n_lm = (Lmax + 1) ** 2
     orb = np.zeros((Cm.shape[0], n_lm, Nr))
     rho = np.zeros((n_lm, Nr))
+    vx = np.zeros((n_lm, Nr)) if vx_form else None
     check(lib().scatt_sce_basis(int(Lmax), int(Nr), float(r0), float(dr), as_dptr(o), len(shells), as_iptr(sl),
                                 as_iptr(sn), as_dptr(sc), as_dptr(ex), as_dptr(cf), Cm.shape[0], as_dptr(Cm),
-                                as_dptr(oc), int(chunk), as_dptr(orb), as_dptr(rho)))
-    return orb, rho
+                                as_dptr(oc), int(vx_form), int(chunk), as_dptr(orb), as_dptr(rho),
+                                as_dptr(vx) if vx is not None else None))
+    return (orb, rho, vx) if vx_form else (orb, rho)

@@ -1,6 +1,7 @@
 """The device basis-to-expansion path (scatt_sce_basis: the AO values of
 preprocessing/src/basis/MoldenBasis.hpp, the orbitals and the density, each
-projected as preprocessing/src/sce/SCE.hpp does) against the oracle
+and the local exchange of potential/LocalExchange.hpp, each projected as
+preprocessing/src/sce/SCE.hpp does) against the oracle
 (oracle/basis.py with oracle/sce.py, pinned in tests/test_oracle_basis.py
 and tests/test_oracle_sce.py).  Same arithmetic up to summation order and
 the angles (the device forms cos / sin of theta and phi algebraically, the
@@ -29,15 +30,18 @@ def _molecule(seed=11):
     return shells, C, occ
 
 
-@pytest.mark.parametrize("Lmax,Nr,chunk,r0", [(6, 9, 0, 0.0), (10, 13, 4, 0.02), (16, 5, 1, 0.0)])
-def test_basis_expansions_match_oracle(Lmax, Nr, chunk, r0):
+@pytest.mark.parametrize("Lmax,Nr,chunk,r0,vx", [(6, 9, 0, 0.0, 0), (10, 13, 4, 0.02, 1), (16, 5, 1, 0.0, 2)])
+def test_basis_expansions_match_oracle(Lmax, Nr, chunk, r0, vx):
+    """Orbitals, density and (Slater or Kohn-Sham) local exchange."""
     shells, C, occ = _molecule()
     dr = 0.3
     origin = np.array([0.0, 0.0, 0.35])
-    orb, rho = _lib.sce_basis(shells, C, occ, Lmax, Nr, r0, dr, origin, chunk)
+    got = _lib.sce_basis(shells, C, occ, Lmax, Nr, r0, dr, origin, chunk, vx_form=vx)
     r = r0 + np.arange(Nr) * dr
-    orb_ref, rho_ref = B.sce_of_basis(shells, C, occ, Lmax, r, origin)
+    ref = B.sce_of_basis(shells, C, occ, Lmax, r, origin, vx_form=vx)
+    assert len(got) == len(ref) == (3 if vx else 2)
     for i in range(C.shape[0]):
-        scale = np.max(np.abs(orb_ref[i]))
-        assert np.max(np.abs(orb[i] - orb_ref[i])) <= 1e-12 * scale, i
-    assert np.max(np.abs(rho - rho_ref)) <= 1e-12 * np.max(np.abs(rho_ref))
+        scale = np.max(np.abs(ref[0][i]))
+        assert np.max(np.abs(got[0][i] - ref[0][i])) <= 1e-12 * scale, i
+    for g, f in zip(got[1:], ref[1:]):
+        assert np.max(np.abs(g - f)) <= 1e-12 * np.max(np.abs(f))
