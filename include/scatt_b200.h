@@ -458,6 +458,26 @@ int scatt_sce_basis(int Lmax, int Nr, double r0, double dr, const double* origin
                     int n_mo, const double* C, const double* occ, int vx_form, int chunk, double* orb_lm,
                     double* rho_lm, double* vx_lm);
 
+/* Molden reader (preprocessing/src/molden/Molden.hpp), host-only: the
+ * [Atoms] (bohr; Angs or unmarked blocks converted), [GTO] and [MO]
+ * sections and the [5D] / [5D7F] / [5D10F] / [7F] / [9G] flags, kept as
+ * written.  scatt_molden_info: out7 = n_atoms, n_shell, nbf, alpha MOs,
+ * beta MOs, primitives in all, Cartesian shells of l >= 2.
+ * scatt_molden_atoms: n_atoms x (Z, x, y, z).  scatt_molden_shells: the
+ * arrays scatt_sce_basis takes (l, primitives, centre, exponents and raw
+ * coefficients in file order); a Cartesian shell of l >= 2 is an error, as
+ * in the reference's build_basis.  scatt_molden_mos: n_mo x nbf
+ * coefficients (row-major, AO order), occupations and energies of the alpha
+ * (beta = 0) or beta orbitals.  Malformed files return SCATT_ERR_IO with
+ * the offending line. */
+typedef struct scatt_molden scatt_molden;
+int scatt_molden_open(const char* path, scatt_molden** out);
+int scatt_molden_info(scatt_molden* m, int* out7);
+int scatt_molden_atoms(scatt_molden* m, double* zxyz);
+int scatt_molden_shells(scatt_molden* m, int* l, int* nprim, double* center, double* exps, double* coefs);
+int scatt_molden_mos(scatt_molden* m, int beta, double* C, double* occ, double* energy);
+int scatt_molden_close(scatt_molden* m);
+
 /* ------------------------------------------------------ file formats
  * Host-only entry points (no device work, no GPU needed) for the files
  * around the path, on an HDF5 subset written from the public file-format
