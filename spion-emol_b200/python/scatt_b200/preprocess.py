@@ -1,0 +1,79 @@
+"""The preprocessing chain of the reference (preprocessing/src/
+main_preprocess.cpp: Molden file -> single-centre expansion of the
+orbitals and the density -> Hartree potential -> the schema-v2 file the
+scattering solve reads), on the library's device steps:
+
+    read_molden (scatt_molden_*)  ->  sce_basis (scatt_sce_basis: orbitals,
+    density, local exchange)  ->  hartree (scatt_hartree)  ->
+    h5io.write_preproc
+
+The SCE origin is placed at (0, 0, 0) and the atoms are translated so that
+the chosen centre sits there (main_preprocess.cpp:278-303): 'atoms' (their
+geometric mean, the default), 'com' (the Z-weighted mean) or
+'origin_of_file'.  The radial grid is r_k = k dr, k = 0 .. round(rmax / dr)
+(rmin = 0, as the solver's grid).  The occupied orbitals are the alpha
+orbitals with a non-zero occupation, in file order.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import _lib, h5io
+from .molden import read_molden
+from .synth import ScanInputs
+
+
+def centre_of(atoms: np.ndarray, choice: str) -> np.ndarray:
+    """main_preprocess.cpp:283-299."""
+    if choice in ("atoms", "auto"):
+        return atoms[:, 1:].mean(axis=0)
+    if choice == "com":
+        return (atoms[:, :1] * atoms[:, 1:]).sum(axis=0) / atoms[:, 0].sum()
+    if choice == "origin_of_file":
+        return np.zeros(3)
+    raise ValueError(f"unknown origin choice {choice!r}")
+
+
+def preprocess(molden_path, Lmax: int, dr: float, rmax: float, origin: str = "atoms", l_cont: int = 0,
+               chunk: int = 0, exchange: str = "none"):
+    """(ScanInputs, extras): the scan's energy-independent inputs from a
+    Molden file -- psi_lm the SCE coefficients of every alpha orbital
+    (Lmax channels), V_H from the SCE density by the radial Poisson
+    integrals -- and extras {'rho_lm', 'V_x' (with exchange 'slater' or
+    'ks'), 'centre', 'N_e'}.  N_e = sqrt(4 pi) int r^2 rho_00 dr by
+    Simpson's rule, the reference's density check (SCE.hpp:278-285)."""
+    m = read_molden(molden_path)
+    atoms = m["atoms"].copy()
+    c = centre_of(atoms, origin)
+    atoms[:, 1:] -= c
+    shells = [(cen - c, l, e, k) for cen, l, e, k in m["shells"]]
+    Nr = int(round(rmax / dr)) + 1
+    a = m["alpha"]
+    vx_form = {"none": 0, "slater": 1, "ks": 2}[exchange]
+    out = _lib.sce_basis(shells, a["C"], a["occ"], Lmax, Nr, 0.0, dr, (0.0, 0.0, 0.0), chunk, vx_form=vx_form)
+    orb, rho = out[0], out[1]
+    if m["beta"]["C"].shape[0]:
+        # the beta orbitals' density adds to the alpha one (evaluate_density)
+        b = m["beta"]
+        rho = rho + _lib.sce_basis(shells, b["C"], b["occ"], Lmax, Nr, 0.0, dr, (0.0, 0.0, 0.0), chunk)[1]
+    V_H = _lib.hartree(rho, dr, Lmax)
+    r = np.arange(Nr) * dr
+    w = np.full(Nr, 2.0 * dr / 3.0)
+    w[1::2] = 4.0 * dr / 3.0
+    w[0] = w[-1] = dr / 3.0
+    extras = {"rho_lm": rho, "centre": c, "N_e": math.sqrt(4.0 * math.pi) * float(np.sum(w * r * r * rho[0]))}
+    if vx_form:
+        extras["V_x"] = out[2]
+    n_occ = int(np.count_nonzero(a["occ"]))
+    inp = ScanInputs(name=str(molden_path), dr=float(dr), Nr=Nr, l_cont=int(l_cont or min(Lmax, 10)),
+                     atoms=atoms, psi_lm=orb, orb_energies=a["energy"].copy(), n_occ=n_occ, V_H=V_H)
+    return inp, extras
+
+
+def preprocess_to_file(molden_path, path, Lmax: int, dr: float, rmax: float, split: bool = False, **kw):
+    """preprocess() written in the reference's schema (h5io.write_preproc);
+    returns the path to open (ScanSolver.from_preproc)."""
+    inp, _ = preprocess(molden_path, Lmax, dr, rmax, **kw)
+    return h5io.write_preproc(path, inp, split=split)
