@@ -64,6 +64,17 @@ def test_every_compute_entry_point_reports_no_device():
                                              _lib.as_dptr(C), 4),
         "scatt_bench_inverse": lambda: L.scatt_bench_inverse(8, 1, 1, _lib.as_dptr(ms)),
         "scatt_ctx_create": lambda: L.scatt_ctx_create(0, ctypes.byref(ctypes.c_void_p())),
+        "scatt_hartree": lambda: L.scatt_hartree(1, 4, 8, 0.0, 0.1, _lib.as_dptr(np.ones((4, 8))),
+                                                 _lib.as_dptr(np.zeros((4, 8)))),
+        "scatt_sce_project": lambda: L.scatt_sce_project(1, 2, 0, _lib.as_dptr(np.ones((2, 2, 4))),
+                                                         _lib.as_dptr(np.zeros((4, 2)))),
+        "scatt_cc_dipole": lambda: L.scatt_cc_dipole(4, 4, 6, 0, 0.1, 0, _lib.as_dptr(np.ones((6, 4, 4))), 1,
+                                                     _lib.as_dptr(np.ones((6, 4, 4))), _lib.as_dptr(np.zeros((4, 4)))),
+        "scatt_sce_basis": lambda: L.scatt_sce_basis(
+            1, 2, 0.0, 0.1, _lib.as_dptr(np.zeros(3)), 1, _lib.as_iptr(np.zeros(1, dtype=np.int32)),
+            _lib.as_iptr(np.ones(1, dtype=np.int32)), _lib.as_dptr(np.zeros(3)), _lib.as_dptr(np.ones(1)),
+            _lib.as_dptr(np.ones(1)), 1, _lib.as_dptr(np.ones((1, 1))), _lib.as_dptr(np.ones(1)), 0, 0,
+            _lib.as_dptr(np.zeros((1, 4, 2))), _lib.as_dptr(np.zeros((4, 2))), None),
     }
     for name, call in calls.items():
         assert call() == 7, name

@@ -106,3 +106,15 @@ def test_missing_file_is_an_io_error(tmp_path):
     with pytest.raises(ScattError) as ei:
         molden.read_molden(tmp_path / "none.molden")
     assert ei.value.code == 11
+
+
+def test_sce_centre_choices():
+    """main_preprocess.cpp:283-299: the geometric mean of the atoms, the
+    Z-weighted mean, or the file's own origin."""
+    from scatt_b200 import preprocess
+    atoms = np.array([[8.0, 0.0, 0.0, 0.0], [1.0, 0.0, 1.43, 1.1], [1.0, 0.0, -1.43, 1.1]])
+    np.testing.assert_allclose(preprocess.centre_of(atoms, "atoms"), [0.0, 0.0, 2.2 / 3.0], atol=1e-15)
+    np.testing.assert_allclose(preprocess.centre_of(atoms, "com"), [0.0, 0.0, 2.2 / 10.0], atol=1e-15)
+    assert np.array_equal(preprocess.centre_of(atoms, "origin_of_file"), np.zeros(3))
+    with pytest.raises(ValueError):
+        preprocess.centre_of(atoms, "elsewhere")
