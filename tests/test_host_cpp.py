@@ -161,3 +161,19 @@ def test_psi_and_cc_dipole_calls_compile(tmp_path):
     assert r.returncode == 0, r.stderr
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+
+
+def test_preprocessing_interface_compiles_and_reads_molden(tmp_path):
+    """tests/host_preproc_check.cpp uses host/scatt_preproc.hpp as the
+    reference's preprocessing driver would: warning-free; the Molden reader
+    runs on the host; the device steps report a missing device."""
+    _driver()
+    exe = tmp_path / "preproc_check"
+    cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror",
+           "-I", os.path.join(ROOT, "include"), "-I", os.path.join(PKG, "host"),
+           os.path.join(ROOT, "tests", "host_preproc_check.cpp"),
+           "-L", PKG, "-lscatt_b200", f"-Wl,-rpath,{PKG}", "-o", str(exe)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
