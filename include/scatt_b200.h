@@ -391,6 +391,40 @@ int scatt_psi_sweep(scatt_ctx* ctx, const scatt_solve_opts* opts, int n_energy, 
                     const int* l_cont, int segment, int n_lo, int n_hi, const scatt_outputs* outputs,
                     double* psi_out);
 
+/* The on-disk psi store of the reference's back-propagation, the files its
+ * continuum-continuum dipole driver reads (src/scatt/BackPropagator.cpp:
+ * 27-101, :255-283, :700-745; the full-matrix PotentialStorage layout of
+ * src/scatt/PotentialStorage.cpp:31-35, :556-631, :1542-1566): a directory
+ * of pot_chunk_<c>.bin (int32 count + count column-major N_psi x N_psi
+ * matrices), metadata.bin (size_t points, int32 N_psi, chunk_size,
+ * chunks), psi_asym.bin (the asymptotic buffer, 32-byte 'PSI_ASYM'
+ * header), manifest.txt (the reference's "kind=psi energy=... keep=lo..hi"
+ * line) and __SUCCESS__ written last.  Host-only.
+ * scatt_psi_store_write: psi holds the keep_hi - keep_lo + 1 matrices of
+ * points keep_lo .. keep_hi, ld^2 apart with leading dimension ld (as
+ * scatt_psi_sweep writes them, ld = Np_max); psi_asym likewise the n_asym
+ * matrices of points asym_offset .. asym_offset + n_asym - 1 (NULL when
+ * n_asym = 0).  scatt_psi_store_dirname: the reference's default directory
+ * name.  The reader refuses a store without __SUCCESS__;
+ * scatt_psi_store_info: out6 = points, N_psi, chunk_size, chunks, n_asym,
+ * asym_offset; scatt_psi_store_read: matrices first .. first + count - 1
+ * (counted from keep_lo), packed N_psi x N_psi. */
+typedef struct {
+    double energy, dr;
+    int n_grid, n_psi, n_f, l_cont, l_exch, n_occ, n_transition;
+    int keep_lo, keep_hi, chunk_size, n_asym, asym_offset;
+} scatt_psi_store_meta;
+typedef struct scatt_psi_store scatt_psi_store;
+int scatt_psi_store_dirname(const scatt_psi_store_meta* meta, char* buf, int cap);
+int scatt_psi_store_write(const char* dir, const scatt_psi_store_meta* meta, const double* psi, int ld,
+                          const double* psi_asym, int ld_asym);
+int scatt_psi_store_open(const char* dir, scatt_psi_store** out);
+int scatt_psi_store_info(scatt_psi_store* h, long long* out6);
+int scatt_psi_store_manifest(scatt_psi_store* h, char* buf, int cap);
+int scatt_psi_store_read(scatt_psi_store* h, long long first, long long count, double* out);
+int scatt_psi_store_read_asym(scatt_psi_store* h, double* out);
+int scatt_psi_store_close(scatt_psi_store* h);
+
 /* Continuum-continuum dipole, the consumer of the psi store
  * (postprocessing/two_photon_delay/cc_dipole/src/CCDipole.cpp:294-334 and
  * its range-accumulating API, include/CCDipole.hpp): for one final state
