@@ -334,12 +334,14 @@ def _isqrt_ceil(n):
     return r
 
 
-def write_preproc(path, inp, split=False, gzip=4, initial_state=None):
+def write_preproc(path, inp, split=False, gzip=4, initial_state=None, extra=None):
     """Writes the energy-independent inputs `inp` in the reference's
     preprocessing schema (combined file at `path`, or with split=True the
     pair <stem>.orbitals.h5 + <stem>.potentials.h5 where path is the stem).
     initial_state = (psi (Nlm, Nr_store), energy, occupation) adds the
-    /initial_state group.  Returns the path to open."""
+    /initial_state group; extra = {dataset path: array} adds datasets to
+    the potentials side (e.g. /potential/V_local_exchange and /rho/rho_lm,
+    main_preprocess.cpp:706-714).  Returns the path to open."""
     psi = np.asarray(inp.psi_lm, dtype=np.float64)
     n_orb, Nlm, Nr_store = psi.shape
     L = _isqrt_ceil(max(Nlm, inp.V_H.shape[0])) - 1
@@ -382,6 +384,8 @@ def write_preproc(path, inp, split=False, gzip=4, initial_state=None):
             w.dataset("/polarizability/alpha_tensor", np.eye(3) * inp.alpha_pol)
             w.dataset("/polarizability/alpha_iso_au", np.float64(inp.alpha_pol))
         w.dataset("/meta/schema_version", np.int64(2))
+        for name, arr in (extra or {}).items():
+            w.dataset(name, np.asarray(arr, dtype=np.float64), gzip=gzip)
 
     path = os.fspath(path)
     if not split:

@@ -77,3 +77,32 @@ def preprocess_to_file(molden_path, path, Lmax: int, dr: float, rmax: float, spl
     returns the path to open (ScanSolver.from_preproc)."""
     inp, _ = preprocess(molden_path, Lmax, dr, rmax, **kw)
     return h5io.write_preproc(path, inp, split=split)
+
+
+def main(argv=None):
+    """Command line in the manner of the reference's preprocess tool
+    (main_preprocess.cpp:60-210: --lmax, --dr, --rmax, --exchange,
+    --origin): python -m scatt_b200.preprocess MOLDEN OUT [--split]."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(prog="python -m scatt_b200.preprocess")
+    ap.add_argument("molden")
+    ap.add_argument("out", help="combined file path, or the stem of the split pair with --split")
+    ap.add_argument("--lmax", type=int, default=20)
+    ap.add_argument("--dr", type=float, default=0.01)
+    ap.add_argument("--rmax", type=float, default=40.0)
+    ap.add_argument("--exchange", default="none", choices=["none", "slater", "ks"])
+    ap.add_argument("--origin", default="atoms", choices=["atoms", "auto", "com", "origin_of_file"])
+    ap.add_argument("--split", action="store_true")
+    a = ap.parse_args(argv)
+    inp, ex = preprocess(a.molden, a.lmax, a.dr, a.rmax, origin=a.origin, exchange=a.exchange)
+    extra = {"/rho/rho_lm": ex["rho_lm"]}
+    if "V_x" in ex:
+        extra["/potential/V_local_exchange"] = ex["V_x"]
+    path = h5io.write_preproc(a.out, inp, split=a.split, extra=extra)
+    print(json.dumps({"file": path, "Nr": inp.Nr, "Lmax": a.lmax, "orbitals": int(inp.psi_lm.shape[0]),
+                      "n_occ": inp.n_occ, "N_e": ex["N_e"], "centre": [float(x) for x in ex["centre"]]}))
+
+
+if __name__ == "__main__":
+    main()

@@ -366,3 +366,18 @@ def test_cpp_interface(tmp_path):
     assert desc[1:5] == ["3", str(cut), str(inp.psi_lm.shape[2]), "-1"]
     assert float(desc[8]) == inp.psi_lm[0, 0, 1]
     assert float(desc[9]) == inp.orb_energies[inp.n_occ - 1]
+
+
+def test_preproc_extra_datasets(tmp_path):
+    """The density and the local exchange the preprocessing chain computes
+    land beside V_H (main_preprocess.cpp:706-714) and read back unchanged."""
+    inp = synth.h2_like(Nr=101, dr=0.1, l_cont=2)
+    rng = np.random.default_rng(5)
+    rho, vx = rng.standard_normal((9, 101)), rng.standard_normal((9, 101))
+    path = h5io.write_preproc(tmp_path / "x.h5", inp,
+                              extra={"/rho/rho_lm": rho, "/potential/V_local_exchange": vx})
+    with h5io.H5Reader(path) as r:
+        np.testing.assert_array_equal(r.read("/rho/rho_lm"), rho)
+        np.testing.assert_array_equal(r.read("/potential/V_local_exchange"), vx)
+    with h5io.Preproc(path) as pp:
+        assert pp.Nr == 101
