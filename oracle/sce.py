@@ -96,3 +96,33 @@ def synthesize(coef: np.ndarray, Lmax: int) -> np.ndarray:
         Y = np.stack([real_ylm(l, m, TH[i], PH[i]) for i in range(theta.size)])
         out += coef[ch][:, None, None] * Y[None]
     return out
+
+
+def synthesize_at(F_lm: np.ndarray, r0: float, dr: float, origin, Lmax: int, P) -> float:
+    """preprocessing/src/sce/Synthesize.hpp:23-97: F(P) = sum_lm F_lm(r) Y^R_lm
+    at the point P, F_lm (>= (Lmax + 1)^2 rows, Nr columns) on r_k = r0 + k dr,
+    by 4-point Lagrange interpolation in r on the stencil k - 1 .. k + 2
+    (k = floor((r - r0) / dr) clamped to 1 .. Nr - 3); 0 outside the grid."""
+    d = np.asarray(P, dtype=np.float64) - np.asarray(origin, dtype=np.float64)
+    r = float(np.sqrt(d @ d))
+    Nr = F_lm.shape[1]
+    if r < r0 - 1e-14 or r > r0 + (Nr - 1) * dr + 1e-14:
+        return 0.0
+    theta = phi = 0.0
+    if r > 1e-14:
+        theta = math.acos(min(1.0, max(-1.0, d[2] / r)))
+        phi = math.atan2(d[1], d[0])
+    k = min(max(int(math.floor((r - r0) / dr)), 1), Nr - 3)
+    s = (r - (r0 + k * dr)) / dr
+    w = np.array([-s * (s - 1.0) * (s - 2.0) / 6.0, (s + 1.0) * (s - 1.0) * (s - 2.0) * 0.5,
+                  -(s + 1.0) * s * (s - 2.0) * 0.5, (s + 1.0) * s * (s - 1.0) / 6.0])
+    n_lm = (Lmax + 1) ** 2
+    Fr = F_lm[:n_lm, k - 1:k + 3] @ w
+    S = s_table(Lmax, np.array([theta]))[:, :, 0]
+    out = 0.0
+    for l in range(Lmax + 1):
+        out += Fr[l * l + l] * S[l, 0]
+        for m in range(1, l + 1):
+            out += Fr[l * l + l + m] * math.sqrt(2.0) * S[l, m] * math.cos(m * phi)
+            out += Fr[l * l + l - m] * math.sqrt(2.0) * S[l, m] * math.sin(m * phi)
+    return float(out)
