@@ -137,6 +137,7 @@ class Setup:
     chi_init: np.ndarray           # (Nr, n_lambda) initial state (u-convention)
     phi: np.ndarray                # (n_occ, Nr, n_lambda) occupied orbitals
     spin: np.ndarray               # (n_occ,)
+    mu_idx: np.ndarray | None = None   # continuum channels kept (full (l, m) indices), None: all
 
 
 def n_transition(inp, n_occ, n_lambda):
@@ -150,7 +151,14 @@ def n_transition(inp, n_occ, n_lambda):
     return max(1, n_tr)
 
 
-def make_setup(inp, l_cont: int | None = None, vcube: VCube | None = None) -> Setup:
+def make_setup(inp, l_cont: int | None = None, vcube: VCube | None = None, channels=None) -> Setup:
+    """channels (optional): the continuum channels to keep, as full (l, m)
+    indices l^2 + l + m <= (l_cont + 1)^2 - 1 -- a symmetry block.  The
+    reference always keeps every channel; with a subset, V, the exchange
+    rows and every per-channel table are those of the kept channels, the
+    exchange channels all stay, and on a molecule whose potential and
+    orbitals respect the symmetry the result is that block of the full
+    solve (where the Johnson shifts of both agree)."""
     l_cont = inp.l_cont if l_cont is None else l_cont
     l_x = min(l_cont, 10)
     n_mu = (l_cont + 1) ** 2
@@ -174,6 +182,14 @@ def make_setup(inp, l_cont: int | None = None, vcube: VCube | None = None) -> Se
     Gc = sp.csr_matrix((vals, (rows, cols)), shape=(n_mu * n_sigma, max(nlm, 1)))
     Gc.sum_duplicates()
     Gc.sort_indices()
+    mu_idx = None
+    if channels is not None:
+        mu_idx = np.array(sorted(set(int(c) for c in channels)), dtype=np.int64)
+        if mu_idx.size == 0 or mu_idx[0] < 0 or mu_idx[-1] >= n_mu:
+            raise ValueError("channels must be non-empty full (l, m) indices below (l_cont + 1)^2")
+        Gc = Gc[(mu_idx[:, None] * n_sigma + np.arange(n_sigma)[None, :]).ravel()]
+        lm = [lm[i] for i in mu_idx]
+        n_mu = int(mu_idx.size)
     # chi[ir](i, lambda) = r * psi_lm, r = rmin + ir*dr, rmin = 0 (WavefunctionSetup.cpp:196-204)
     nl = min(n_lambda, inp.Nlm_store)
     chi_r = np.zeros((n_occ, n_lambda, n_tr))
@@ -194,10 +210,12 @@ def make_setup(inp, l_cont: int | None = None, vcube: VCube | None = None) -> Se
         vcube = VCube(inp)
     return Setup(inp, Nr, dr, l_cont, l_x, n_mu, n_sigma, n_lambda, n_occ, n_tr, Nf, n_mu + Nf,
                  np.array([a for a, b in lm]), np.array([b for a, b in lm]),
-                 np.tile(ls, n_occ), vcube, Gc, nlm, chi_r, chi_init, phi, spin)
+                 np.tile(ls, n_occ), vcube, Gc, nlm, chi_r, chi_init, phi, spin, mu_idx)
 
 
 def V_at(st: Setup, n: int) -> np.ndarray:
+    if st.mu_idx is not None:
+        return st.vcube.get(n)[np.ix_(st.mu_idx, st.mu_idx)]
     return st.vcube.get(n)[: st.n_mu, : st.n_mu]
 
 
