@@ -100,12 +100,19 @@ def min_eig_fast(M, threshold):
     return float(sla.eigvalsh(M, lower=True)[0])
 
 
-def stability_shift(M, W_min=W_MIN, margin=SHIFT_MARGIN):
-    """SchurInverter.cpp:53-59 -- returns (shifted M, shifted?)."""
+def shift_delta(M, W_min=W_MIN, margin=SHIFT_MARGIN) -> float:
+    """SchurInverter.cpp:53-59: the diagonal shift for M, 0 when none."""
     me = min_eig_fast(M, W_min)
-    if me >= W_min:
+    return 0.0 if me >= W_min else W_min - me + margin
+
+
+def stability_shift(M, W_min=W_MIN, margin=SHIFT_MARGIN, delta=None):
+    """SchurInverter.cpp:53-59 -- returns (shifted M, shifted?).  delta:
+    the shift decided elsewhere (on the whole matrix of a block solve)."""
+    if delta is None:
+        delta = shift_delta(M, W_min, margin)
+    if delta == 0.0:
         return M, False
-    delta = W_min - me + margin
     M = M.copy()
     M[np.diag_indices_from(M)] += delta
     return M, True
@@ -138,6 +145,7 @@ class Setup:
     phi: np.ndarray                # (n_occ, Nr, n_lambda) occupied orbitals
     spin: np.ndarray               # (n_occ,)
     mu_idx: np.ndarray | None = None   # continuum channels kept (full (l, m) indices), None: all
+    whole: "Setup | None" = None       # block solves: the all-channel setup the shifts are decided on
 
 
 def n_transition(inp, n_occ, n_lambda):
@@ -151,14 +159,18 @@ def n_transition(inp, n_occ, n_lambda):
     return max(1, n_tr)
 
 
-def make_setup(inp, l_cont: int | None = None, vcube: VCube | None = None, channels=None) -> Setup:
+def make_setup(inp, l_cont: int | None = None, vcube: VCube | None = None, channels=None,
+               whole_matrix_shift: bool = True) -> Setup:
     """channels (optional): the continuum channels to keep, as full (l, m)
     indices l^2 + l + m <= (l_cont + 1)^2 - 1 -- a symmetry block.  The
     reference always keeps every channel; with a subset, V, the exchange
     rows and every per-channel table are those of the kept channels, the
     exchange channels all stay, and on a molecule whose potential and
     orbitals respect the symmetry the result is that block of the full
-    solve (where the Johnson shifts of both agree)."""
+    solve.  The stability shifts (SchurInverter.cpp:53-59) are decided on
+    the all-channel A and S, block-diagonal there, so on the lowest
+    eigenvalue over every block, as a block-diagonal solve must to match the
+    reference; whole_matrix_shift=False decides them on the block alone."""
     l_cont = inp.l_cont if l_cont is None else l_cont
     l_x = min(l_cont, 10)
     n_mu = (l_cont + 1) ** 2
@@ -208,9 +220,10 @@ def make_setup(inp, l_cont: int | None = None, vcube: VCube | None = None, chann
     spin = np.full(n_occ, 2.0)
     if vcube is None:
         vcube = VCube(inp)
+    whole = make_setup(inp, l_cont, vcube) if (mu_idx is not None and whole_matrix_shift) else None
     return Setup(inp, Nr, dr, l_cont, l_x, n_mu, n_sigma, n_lambda, n_occ, n_tr, Nf, n_mu + Nf,
                  np.array([a for a, b in lm]), np.array([b for a, b in lm]),
-                 np.tile(ls, n_occ), vcube, Gc, nlm, chi_r, chi_init, phi, spin, mu_idx)
+                 np.tile(ls, n_occ), vcube, Gc, nlm, chi_r, chi_init, phi, spin, mu_idx, whole)
 
 
 def V_at(st: Setup, n: int) -> np.ndarray:
@@ -262,9 +275,12 @@ def sinv_at(st: Setup, E: float, n: int, counts=None) -> np.ndarray:
     A[np.diag_indices(st.n_mu)] += h2_6 * E
     if n < st.Nr:
         A = A - h2_6 * V_at(st, n)
+    d_A = d_S = None
+    if st.whole is not None and n < STAB_N_MAX:
+        d_A, d_S = whole_shifts(st.whole, E, n)
     if n < STAB_N_MAX:
         A = sym(A)
-        A, sh = stability_shift(A)
+        A, sh = stability_shift(A, delta=d_A)
         if counts is not None and sh:
             counts["A"] += 1
     if n < st.n_tr:
@@ -273,12 +289,29 @@ def sinv_at(st: Setup, E: float, n: int, counts=None) -> np.ndarray:
         Bs = B * Dinv[None, :]
         S = A - Bs @ B.T
         if n < STAB_N_MAX:
-            S, sh = stability_shift(S)
+            S, sh = stability_shift(S, delta=d_S)
             if counts is not None and sh:
                 counts["S"] += 1
     else:
         S = A
     return inverse_symmetric_indefinite(S)
+
+
+def whole_shifts(st: Setup, E: float, n: int):
+    """The shifts of A and S that sinv_at applies at n on the all-channel
+    setup st: (delta_A, delta_S), 0 where none."""
+    h2_6 = st.dr * st.dr / 6.0
+    A = np.eye(st.n_mu)
+    A[np.diag_indices(st.n_mu)] += h2_6 * E
+    if n < st.Nr:
+        A = A - h2_6 * V_at(st, n)
+    d_A = shift_delta(sym(A))
+    d_S = 0.0
+    if n < st.n_tr:
+        A, _ = stability_shift(sym(A), delta=d_A)
+        B = B_at(st, n)
+        d_S = shift_delta(A - (B * dinv_at(st, n)[None, :]) @ B.T)
+    return d_A, d_S
 
 
 # ------------------------------------------------------------ W^-1

@@ -7,11 +7,10 @@ On a linear molecule on the z axis the static-exchange potential couples
 keeps one block: V, the exchange rows and the per-channel tables are those
 of the kept channels.  The reference always solves every channel; the
 subset is the groundwork for a block-diagonal device solve, and this test
-pins what it must reproduce.  One limit is tested too: the stability shift
-of SchurInverter.cpp:53-59 is decided on the whole matrix, so where it
-fires on the full solve because of another block, the block's own solve
-does not shift and differs -- a block-diagonal solve has to take the
-minimum over all blocks.
+pins what it must reproduce.  The stability shift of
+SchurInverter.cpp:53-59 is decided on the whole matrix, that is on the
+lowest eigenvalue over every block; decided on the block alone
+(whole_matrix_shift=False) it can differ, and the sigma_u case shows how.
 """
 import numpy as np
 import pytest
@@ -28,12 +27,12 @@ def full():
     return inp, O.solve_energy(O.make_setup(inp), E)
 
 
-def block(inp, channels):
-    return O.solve_energy(O.make_setup(inp, channels=channels), E)
+def block(inp, channels, whole=True):
+    return O.solve_energy(O.make_setup(inp, channels=channels, whole_matrix_shift=whole), E)
 
 
-@pytest.mark.parametrize("channels", [[0, 6, 20], [1, 5, 11, 19], [3, 7, 13, 21]],
-                         ids=["sigma_g", "pi_minus", "pi_plus"])
+@pytest.mark.parametrize("channels", [[0, 6, 20], [2, 12], [1, 5, 11, 19], [3, 7, 13, 21]],
+                         ids=["sigma_g", "sigma_u", "pi_minus", "pi_plus"])
 def test_block_equals_the_full_solve(full, channels):
     inp, rf = full
     rs = block(inp, channels)
@@ -50,15 +49,15 @@ def test_block_equals_the_full_solve(full, channels):
         assert np.max(np.abs(Df[S] - Ds)) <= tol, q
 
 
-def test_shift_decided_on_the_whole_matrix(full):
+def test_shift_decided_on_the_block_alone_differs(full):
     """sigma_u (m = 0, l odd): the full solve shifts A once (at n = 1, by
-    another block's lowest eigenvalue); the block alone does not.  n = 1 lies
-    in the analytic start of the forward recurrence, so K still agrees, but
-    the back-propagation runs through S^-1(1), so psi near the origin and
-    the dipoles that see it differ."""
+    another block's lowest eigenvalue); the block decided alone does not.
+    n = 1 lies in the analytic start of the forward recurrence, so K still
+    agrees, but the back-propagation runs through S^-1(1), so psi near the
+    origin and the dipoles that see it differ."""
     inp, rf = full
     S = [2, 12]
-    rs = block(inp, S)
+    rs = block(inp, S, whole=False)
     assert rf.shifts == {"A": 1, "S": 0} and rs.shifts == {"A": 0, "S": 0}
     assert np.max(np.abs(rf.K_kme[np.ix_(S, S)] - rs.K_kme)) <= 1e-11 * np.max(np.abs(rs.K_kme))
     rel = [np.max(np.abs(rf.slices[q]["D"][S] - rs.slices[q]["D"])) / np.max(np.abs(rs.slices[q]["D"]))
