@@ -1,0 +1,127 @@
+"""The preprocessing command line's input-convention gate
+(main_preprocess.cpp:557-632): every occupied orbital's ||psi||^2 in
+[0.50, 1.10], N_e of the SCE density within 10% of the occupations, a
+failed gate writes nothing and exits 3, --no-validate-input skips it.
+Host logic only: the device steps are replaced by fixed results."""
+import json
+import math
+import types
+
+import numpy as np
+import pytest
+
+from scatt_b200 import preprocess as P
+
+
+def test_norm_squared_of_hydrogen_1s():
+    dr, Nr = 0.01, 4001
+    r = np.arange(Nr) * dr
+    F = np.zeros((4, Nr))
+    F[0] = 2.0 * np.exp(-r)                 # R_10, channel (0, 0)
+    assert abs(P.norm_squared(F, dr) - 1.0) < 1e-8      # Simpson at dr = 0.01: 2.7e-9
+    F[2] = F[0]                             # a second channel adds its own norm
+    assert abs(P.norm_squared(F, dr) - 2.0) < 2e-8
+
+
+def test_simpson_weights_integrate_a_cubic_exactly():
+    dr, Nr = 0.1, 21
+    r = np.arange(Nr) * dr
+    assert abs(np.sum(P.simpson_weights(Nr, dr) * r**3) - 2.0**4 / 4) < 1e-12
+
+
+def test_gate_passes_and_counts_advisories():
+    ok = P.validate([0.999, 0.995], 9.98, 10.0)
+    assert ok["ok"] and not ok["failures"] and ok["advisory"] == 0
+    assert ok["worst_norm"] == (0.995, 0.999) and abs(ok["ne_rel"] - 0.002) < 1e-12
+    adv = P.validate([0.95, 1.0], 10.0, 10.0)
+    assert adv["ok"] and adv["advisory"] == 1
+
+
+@pytest.mark.parametrize("norms,N_e,what", [([0.4, 1.0], 10.0, "orbital 1"), ([1.0, 1.2], 10.0, "orbital 2"),
+                                            ([1.0, 1.0], 8.5, "N_e")])
+def test_gate_fails(norms, N_e, what):
+    out = P.validate(norms, N_e, 10.0)
+    assert not out["ok"] and len(out["failures"]) == 1 and what in out["failures"][0]
+
+
+def test_gate_thresholds_are_the_callers():
+    assert P.validate([0.4], 10.0, 10.0, norm_lo=0.3)["ok"]
+    assert P.validate([1.0], 8.5, 10.0, ne_tol=0.2)["ok"]
+    assert P.validate([1.0], 3.0, 0.0)["ne_rel"] == 0.0          # no occupations: no N_e check
+
+
+@pytest.fixture
+def fake_chain(monkeypatch):
+    """preprocess() and the writer replaced by fixed results."""
+    state = {"norms": [0.999, 0.997], "N_e": 4.0, "written": []}
+
+    def fake_preprocess(path, Lmax, dr, rmax, origin="atoms", exchange="none", **kw):
+        inp = types.SimpleNamespace(Nr=11, psi_lm=np.zeros((3, 4, 11)), n_occ=2)
+        ex = {"rho_lm": np.zeros((4, 11)), "centre": np.zeros(3), "N_e": state["N_e"], "N_e_expected": 4.0,
+              "orb_norm_sq": state["norms"]}
+        return inp, ex
+
+    def fake_write(path, inp, split=False, extra=None):
+        state["written"].append(path)
+        return path
+
+    monkeypatch.setattr(P, "preprocess", fake_preprocess)
+    monkeypatch.setattr(P.h5io, "write_preproc", fake_write)
+    return state
+
+
+def test_command_line_writes_when_the_gate_passes(fake_chain, capsys):
+    assert P.main(["mol.molden", "out.h5"]) == 0
+    assert fake_chain["written"] == ["out.h5"]
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["validate"]["advisory"] == 0 and line["orb_norm_sq"] == [0.999, 0.997]
+    assert math.isclose(line["N_e"], 4.0) and line["N_e_expected"] == 4.0
+
+
+def test_command_line_failed_gate_writes_nothing(fake_chain, capsys):
+    fake_chain["norms"] = [0.999, 2.0]              # a doubly normalised orbital
+    assert P.main(["mol.molden", "out.h5"]) == 3
+    assert fake_chain["written"] == []
+    err = capsys.readouterr().err
+    assert "FAIL orbital 2" in err and "--no-validate-input" in err
+
+
+def test_command_line_gate_can_be_skipped_or_loosened(fake_chain, capsys):
+    fake_chain["N_e"] = 3.0                         # 25% off
+    assert P.main(["mol.molden", "out.h5"]) == 3
+    assert P.main(["mol.molden", "out.h5", "--validate-ne-tol", "0.3"]) == 0
+    assert P.main(["mol.molden", "out2.h5", "--no-validate-input"]) == 0
+    assert fake_chain["written"] == ["out.h5", "out2.h5"]
+    assert json.loads(capsys.readouterr().out.strip().splitlines()[-1])["validate"] is None
+
+
+def test_gate_on_the_reference_water_molden(tmp_path):
+    """The reference's H2O cc-pVDZ Molden file (preprocessing/reference_data,
+    via tests/golden/preproc_reference.json) through the oracle's SCE at
+    Lmax 16: the gate passes with one advisory (the O 1s, off the SCE
+    centre, needs higher l: ||psi||^2 0.964 here, 0.996 at Lmax 30), and
+    the same orbitals doubly normalised fail it on every orbital and on N_e."""
+    import os
+    from oracle import basis as B
+    from scatt_b200 import molden
+    gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "preproc_reference.json")
+    with open(gold) as f:
+        text = json.load(f)["h2o_ccpvdz_sph"]["molden"]
+    p = tmp_path / "h2o.molden"
+    p.write_text(text)
+    m = molden.read_molden(p)
+    a = m["alpha"]
+    occ = a["occ"][a["occ"] > 0]
+    dr, r = 0.02, np.arange(601) * 0.02
+    origin = m["atoms"][:, 1:].mean(axis=0)
+    for scale, ok in ((1.0, True), (math.sqrt(2.0), False)):
+        orb, rho = B.sce_of_basis(m["shells"], scale * a["C"][a["occ"] > 0], occ, 16, r, origin)
+        norms = [P.norm_squared(o, dr) for o in orb]
+        N_e = math.sqrt(4.0 * math.pi) * float(np.sum(P.simpson_weights(r.size, dr) * r * r * rho[0]))
+        out = P.validate(norms, N_e, float(occ.sum()))
+        assert out["ok"] is ok
+        if ok:
+            assert out["advisory"] == 1 and 0.95 < norms[0] < 0.99 and min(norms[1:]) > 0.99
+            assert abs(N_e - 10.0) < 0.1
+        else:
+            assert len(out["failures"]) == len(norms) + 1
