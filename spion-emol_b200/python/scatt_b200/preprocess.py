@@ -53,6 +53,16 @@ def norm_squared(F_lm: np.ndarray, dr: float) -> float:
     return float(np.sum(simpson_weights(Nr, dr) * r * r * np.sum(F_lm * F_lm, axis=0)))
 
 
+def inner_product_radial(Fa: np.ndarray, Fb: np.ndarray, dr: float) -> float:
+    """Vnuclear.hpp:210-230: <Fa|Fb> = int r^2 sum_lm Fa_lm(r) Fb_lm(r) dr,
+    the reference's Coulomb sanity sums (J = 0.5 <rho|V_H>)."""
+    if Fa.shape != Fb.shape:
+        raise ValueError("inner_product_radial: shape mismatch")
+    Nr = Fa.shape[-1]
+    r = np.arange(Nr) * dr
+    return float(np.sum(simpson_weights(Nr, dr) * r * r * np.sum(Fa * Fb, axis=0)))
+
+
 def validate(orb_norm_sq, N_e: float, N_e_expected: float, norm_lo: float = 0.50, norm_hi: float = 1.10,
              ne_tol: float = 0.10) -> dict:
     """The input-convention gate of main_preprocess.cpp:557-632: every
@@ -83,7 +93,8 @@ def preprocess(molden_path, Lmax: int, dr: float, rmax: float, origin: str = "at
     sqrt(4 pi) int r^2 rho_00 dr by Simpson's rule, the reference's density
     check (SCE.hpp:278-285); N_e_expected the sum of the alpha and beta
     occupations (main_preprocess.cpp:270-273); orb_norm_sq the ||psi||^2 of
-    each occupied alpha orbital's expansion (SCE.hpp:268-276)."""
+    each occupied alpha orbital's expansion (SCE.hpp:268-276); J the
+    Coulomb energy 0.5 <rho|V_H> (main_preprocess.cpp:505-508)."""
     m = read_molden(molden_path)
     atoms = m["atoms"].copy()
     c = centre_of(atoms, origin)
@@ -103,7 +114,8 @@ def preprocess(molden_path, Lmax: int, dr: float, rmax: float, origin: str = "at
     w = simpson_weights(Nr, dr)
     extras = {"rho_lm": rho, "centre": c, "N_e": math.sqrt(4.0 * math.pi) * float(np.sum(w * r * r * rho[0])),
               "N_e_expected": float(np.sum(a["occ"]) + np.sum(m["beta"]["occ"])),
-              "orb_norm_sq": [norm_squared(orb[j], dr) for j in np.flatnonzero(a["occ"])]}
+              "orb_norm_sq": [norm_squared(orb[j], dr) for j in np.flatnonzero(a["occ"])],
+              "J": 0.5 * inner_product_radial(rho, V_H, dr)}
     if vx_form:
         extras["V_x"] = out[2]
     n_occ = int(np.count_nonzero(a["occ"]))
@@ -158,7 +170,7 @@ def main(argv=None):
     path = h5io.write_preproc(a.out, inp, split=a.split, extra=extra)
     print(json.dumps({"file": path, "Nr": inp.Nr, "Lmax": a.lmax, "orbitals": int(inp.psi_lm.shape[0]),
                       "n_occ": inp.n_occ, "N_e": ex["N_e"], "N_e_expected": ex["N_e_expected"],
-                      "orb_norm_sq": [float(v) for v in ex["orb_norm_sq"]],
+                      "orb_norm_sq": [float(v) for v in ex["orb_norm_sq"]], "J": ex.get("J"),
                       "validate": None if check is None else {k: check[k] for k in ("worst_norm", "ne_rel", "advisory")},
                       "centre": [float(x) for x in ex["centre"]]}))
     return 0

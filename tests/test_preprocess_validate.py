@@ -125,3 +125,19 @@ def test_gate_on_the_reference_water_molden(tmp_path):
             assert abs(N_e - 10.0) < 0.1
         else:
             assert len(out["failures"]) == len(norms) + 1
+
+
+def test_coulomb_energy_of_hydrogen_1s():
+    """J = 0.5 <rho|V_H> of the hydrogen 1s density is 5/16 hartree:
+    rho = exp(-2r) / pi, V_H = 1/r - (1 + 1/r) exp(-2r), both (0, 0)
+    channels sqrt(4 pi) times the function."""
+    dr, Nr = 0.005, 6001
+    r = np.arange(Nr) * dr
+    rho = np.zeros((4, Nr))
+    V = np.zeros((4, Nr))
+    rho[0] = math.sqrt(4.0 * math.pi) * np.exp(-2.0 * r) / math.pi
+    with np.errstate(divide="ignore", invalid="ignore"):
+        V[0] = math.sqrt(4.0 * math.pi) * np.where(r > 0, (1.0 - (1.0 + r) * np.exp(-2.0 * r)) / r, 1.0)
+    assert abs(0.5 * P.inner_product_radial(rho, V, dr) - 5.0 / 16.0) < 1e-9
+    with pytest.raises(ValueError):
+        P.inner_product_radial(rho, V[:1], dr)
